@@ -1,0 +1,184 @@
+/*
+ * jfdk.h -- C ABI of the B200-native FDK reconstruction engine (libjfdk.so).
+ *
+ * This is the drop-in boundary under JEngine's Agent/Pipe surface: the C++
+ * agents in jenhine_b200/host (PreProcessingAgent, FilterAgent, BPCUDAAgent,
+ * CTNumAgent) call these entry points; nothing else in the engine is exposed.
+ *
+ * Conventions
+ *  - Plain C types only: pointers, sizes, floats.  Device pointers ("d_") are
+ *    CUDA device addresses owned by the caller; host pointers ("h_") are host
+ *    memory (pinned is faster, pageable works).
+ *  - Every call returns jfdk_status; no C++ exception crosses the ABI.  The
+ *    message of the last failure is jfdk_last_error(ctx).
+ *  - One context per CUDA stream.  A context is not thread-safe: callers
+ *    serialise on it (the reference issues all CUDA work of BPCUDAAgent from
+ *    its single WorkFlow0 thread, BPCUDAAgent/BPCUDAAgent.cpp:160-187).
+ *  - All work is enqueued on the context's stream; calls return without
+ *    synchronising unless stated.  jfdk_sync waits for the stream.
+ *  - An out-of-memory failure returns JFDK_ERR_OOM and a message starting with
+ *    "CUDA failed to malloc " -- the prefix JEngine's retry loop matches
+ *    (CUDA/DeviceMemory.cpp:60-66, JEngine/JEngine.cpp:413-421).
+ *  - Sizes beyond what the kernels index with 32-bit offsets per frame are
+ *    rejected with JFDK_ERR_INVALID; nothing is silently truncated.
+ */
+#ifndef JFDK_H
+#define JFDK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int jfdk_status;
+enum {
+    JFDK_OK = 0,
+    JFDK_ERR_INVALID = -1,      /* bad argument or size                         */
+    JFDK_ERR_CUDA = -2,         /* CUDA runtime or launch failure               */
+    JFDK_ERR_OOM = -3,          /* device allocation failed                     */
+    JFDK_ERR_UNSUPPORTED = -4,  /* valid in the reference, not implemented here */
+    JFDK_ERR_STATE = -5,        /* call out of order (e.g. finalize, no views)  */
+    JFDK_ERR_NO_DEVICE = -6     /* no usable sm_100 device                      */
+};
+
+/* Arithmetic of the filtered projections and the ramp product. */
+enum {
+    JFDK_PRECISION_FP32 = 0,  /* plain form: FP32 end to end                    */
+    JFDK_PRECISION_MIXED = 1  /* FP16 filtered projections with a per-view scale;
+                                 BF16x3 split-precision ramp product            */
+};
+
+/* Scan parameters: Config/ScanParams.h:13-40. */
+typedef struct jfdk_scan_params {
+    int num_views;             /* NumViews: views per rotation                  */
+    float dso;                 /* DSO, mm                                       */
+    float dsd;                 /* DSD, mm                                       */
+    int num_dets_u;            /* NumDetsU: raw frame columns                   */
+    int num_dets_v;            /* NumDetsV: raw frame rows                      */
+    float detector_pixel_size; /* DetectorPixelSize, mm                         */
+    int border_up, border_down, border_left, border_right; /* BorderSize*     */
+    float bright_field;        /* BrightField (scalar GainCorr divisor)         */
+    float beam_hardening[3];   /* BeamHardeningParams (a0, a1, a2)              */
+    float half_sample_rate;    /* HalfSampleRate; <= 0 derives it from the
+                                  detector as Config/ConfigHelper.cpp:52-53      */
+    int detector_on_right;     /* FilterAgent detectorAtTheRight / FilterCore
+                                  yMirroring (JEngine/JEngine.cpp:153-162)       */
+    int filter_input_width;    /* FilterAgent nInputWidth; 0 = used columns      */
+} jfdk_scan_params;
+
+/* Reconstruction parameters: Config/ReconParams.h:14-68. */
+typedef struct jfdk_recon_params {
+    int num_pixels_x, num_pixels_y, num_pixels_z; /* NumPixelsX/Y/Z              */
+    float pitch_xy, pitch_z;                      /* PitchXY, PitchZ, mm          */
+    float ct_norm0, ct_norm1;                     /* CTNumNorm0, CTNumNorm1       */
+    float mu_water;                               /* MuWater (0.02 in the
+                                                     reference, ConfigHelper.cpp:70) */
+    float filter_cutoff_start, filter_cutoff_end; /* FilterCutOffStart/End        */
+    int num_adjust;                               /* |FilterAdjustPoints|         */
+    const float* adjust_points;                   /* FilterAdjustPoints           */
+    const float* adjust_level_db;                 /* FilterAdjustLevelInDB        */
+    int z_filter;                                 /* apply ZFilterAgent's [1/4,1/2,1/4]
+                                                     row smoothing (FilterAgent/
+                                                     ZFilterAgent.cpp:49-71)       */
+} jfdk_recon_params;
+
+typedef struct jfdk_ctx jfdk_ctx;
+
+/* Create a context on the current device and the given CUDA stream (NULL =
+ * a private stream).  ptms: num_views x 12 floats, row-major 3x4 projection
+ * matrices (TransformMatrix/ProjectionMatrix.h:11-19) already adjusted the
+ * way JEngine/JEngine.cpp:139-150 does.  Replaces the constructors of
+ * PreProcessingCore, FilterCore + PreFilterWeightGenerator, BPCUDACore and
+ * CTNumCore (PreProcessingAgent/PreProcessingCore.cpp:15-65,
+ * FilterAgent/FilterCore.cpp:13-61, FilterAgent/PreFilterWeightGenerator.cpp:
+ * 10-50, BPCUDAAgent/BPCUDACore.cpp:17-127, CTNumAgent/CTNumCore.cpp:8-20). */
+jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan,
+                        const jfdk_recon_params* recon, const float* h_ptms,
+                        int precision, void* cuda_stream);
+void jfdk_destroy(jfdk_ctx* ctx);
+const char* jfdk_last_error(const jfdk_ctx* ctx);
+jfdk_status jfdk_sync(jfdk_ctx* ctx);
+/* Geometry-derived sizes: filter input/output width, FFT length, rows. */
+jfdk_status jfdk_get_dims(const jfdk_ctx* ctx, int* filter_in_w, int* filter_out_w,
+                          int* fft_length, int* rows);
+
+/* ---- stage entry points (the agents' Cores) ------------------------------ */
+
+/* PreProcessingCore::Process for nv frames
+ * (PreProcessingAgent/PreProcessingCore.cpp:67-86): uint16 -> float, clamp at
+ * 1, border crop, / BrightField, -ln, beam hardening.  d_raw: nv x NumDetsV x
+ * NumDetsU uint16; d_out: nv x NumUsedDetsV x NumUsedDetsU float. */
+jfdk_status jfdk_preprocess_frames(jfdk_ctx* ctx, const uint16_t* d_raw, int nv, float* d_out);
+
+/* FilterAgent::ProcessTask + FilterCore::ProcessRow for views [v0, v0+nv) of
+ * the rotation (FilterAgent/FilterAgent.cpp:99-192, FilterCore.cpp:189-222):
+ * cosine pre-weight of the view's 9-view group, truncation ramp, ramp filter.
+ * d_in: nv x rows x filter_in_w float; d_out: nv x rows x filter_out_w float. */
+jfdk_status jfdk_filter_frames(jfdk_ctx* ctx, const float* d_in, int v0, int nv, float* d_out);
+
+/* ZFilterAgent::ProcessTask (FilterAgent/ZFilterAgent.cpp:49-71) in place on
+ * nv frames of rows x width. */
+jfdk_status jfdk_zfilter_frames(jfdk_ctx* ctx, float* d_frames, int nv);
+
+/* BPCUDACore::DeployBackProj for views [v0, v0+nv) of filtered frames
+ * (BPCUDAAgent/BPCUDACore.cu:25-66, with BPCore's edge semantics,
+ * BPAgent/BPCore.cpp:115-196): u-taper, voxel-driven bilinear backprojection,
+ * accumulated into the context's sum and weight volumes.  d_proj: nv x rows
+ * x filter_out_w float.  A view with IsShotStart first calls jfdk_bp_reset. */
+jfdk_status jfdk_bp_reset(jfdk_ctx* ctx);
+jfdk_status jfdk_bp_accumulate(jfdk_ctx* ctx, const float* d_proj, int v0, int nv);
+
+/* BPCore::DoneSlice + CTNumCore::Process for slices [z0, z0+nz)
+ * (BPAgent/BPCore.cpp:198-205, CTNumAgent/CTNumCore.cpp:22-36): voxel =
+ * sum / weight, then HU.  Either output may be NULL.  apply_ctnum = 0 gives
+ * the raw normalised backprojection (the reference's "Slice" pipe before
+ * CTNumAgent). d_out: nz x Y x X float; d_out16: int16 HU rounded toward zero
+ * with saturation (Performance/BasicMathIPP.cpp:224-227). */
+jfdk_status jfdk_finalize(jfdk_ctx* ctx, int z0, int nz, int apply_ctnum, float* d_out,
+                          int16_t* d_out16);
+
+/* CTNumCore::Process on n floats in place. */
+jfdk_status jfdk_ctnum(jfdk_ctx* ctx, float* d_inout, size_t n);
+
+/* ---- whole-volume path -------------------------------------------------- */
+
+/* All stages for one rotation: raw frames (device) -> HU volume (device).
+ * Views are preprocessed, weighted and filtered in chunks into the filtered
+ * projection store, then backprojected in one pass with CT numbers fused into
+ * the final store.  d_hu and/or d_hu16 may be NULL (not both). */
+jfdk_status jfdk_reconstruct(jfdk_ctx* ctx, const uint16_t* d_raw, float* d_hu, int16_t* d_hu16);
+
+/* Same with host buffers: h_raw (num_views x NumDetsV x NumDetsU uint16) is
+ * copied in, h_hu (Z x Y x X float) copied out; synchronous. */
+jfdk_status jfdk_reconstruct_host(jfdk_ctx* ctx, const uint16_t* h_raw, float* h_hu);
+
+/* ---- options --------------------------------------------------------------- */
+enum {
+    JFDK_OPT_BP_EXACT = 1,    /* 1: backprojection rounds every step like BPCore
+                                 (IEEE division, no contraction); 0 (default):
+                                 one reciprocal per sample point, FMA lerps     */
+    JFDK_OPT_VIEW_CHUNK = 2   /* views preprocessed + filtered per launch in
+                                 jfdk_reconstruct (default 32)                   */
+};
+jfdk_status jfdk_set_option(jfdk_ctx* ctx, int key, long long value);
+
+/* ---- introspection (tests, autotuner) ------------------------------------ */
+
+/* The per-view BP u-taper (num_views x filter_out_w floats, host), computed as
+ * BPCore.cpp:68-100. */
+jfdk_status jfdk_get_uweights(const jfdk_ctx* ctx, float* h_out);
+/* The ramp operator: h_T is filter_out_w x filter_in_w (row j = output
+ * column j), h_c the edge-ramp response (filter_out_w). */
+jfdk_status jfdk_get_ramp_operator(const jfdk_ctx* ctx, float* h_T, float* h_c);
+/* Number of kernels this context has launched (a counter, for benchmarks). */
+long long jfdk_kernel_launches(const jfdk_ctx* ctx);
+
+/* Library build / device check: 0 when an sm_100 device is current. */
+jfdk_status jfdk_device_check(char* msg, int msg_len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JFDK_H */

@@ -1,0 +1,458 @@
+// jfdk_api.cpp -- the C ABI (include/jfdk.h): context setup, device memory,
+// and the stage / whole-volume entry points.  No exception leaves this file.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "jfdk_internal.h"
+
+using namespace jfdk;
+
+namespace {
+
+inline size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
+
+// A failed CUDA call sets the context's message and returns a status.
+jfdk_status fail(jfdk_ctx* c, jfdk_status st, const std::string& msg) {
+    if (c) c->err = msg;
+    return st;
+}
+
+jfdk_status cuda_fail(jfdk_ctx* c, cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation)
+        return fail(c, JFDK_ERR_OOM, std::string("CUDA failed to malloc ") + what);
+    return fail(c, JFDK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define JFDK_CUDA(ctx, call, what)                          \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+    } while (0)
+
+#define JFDK_LAUNCH(ctx, call, what)                        \
+    do {                                                    \
+        cudaError_t e_ = (call);                            \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+        ++(ctx)->launches;                                  \
+    } while (0)
+
+template <class T>
+jfdk_status dev_alloc(jfdk_ctx* c, T** p, size_t count, const char* what) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, e == cudaErrorMemoryAllocation ? JFDK_ERR_OOM : JFDK_ERR_CUDA,
+                    std::string("CUDA failed to malloc ") + std::to_string(count * sizeof(T)) +
+                        " bytes for " + what);
+    }
+    *p = static_cast<T*>(q);
+    return JFDK_OK;
+}
+
+template <class T>
+void dev_free(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+int a_pitch(const jfdk_ctx* c) { return (int)round_up(c->in_w, 16); }
+long long q_frame(const jfdk_ctx* c) { return (long long)(c->rows + 1) * c->q_pitch; }
+
+jfdk_status ensure_A(jfdk_ctx* c, size_t rows) {
+    if (c->a_rows >= rows) return JFDK_OK;
+    dev_free(c->d_A);
+    dev_free(c->d_e);
+    c->a_rows = 0;
+    jfdk_status st = dev_alloc(c, &c->d_A, rows * a_pitch(c), "the weighted rows");
+    if (st) return st;
+    st = dev_alloc(c, &c->d_e, rows, "the edge means");
+    if (st) return st;
+    c->a_rows = rows;
+    return JFDK_OK;
+}
+
+jfdk_status ensure_Q(jfdk_ctx* c, int views) {
+    if (c->q_views >= views) return JFDK_OK;
+    dev_free(c->d_q);
+    c->q_views = 0;
+    const size_t n = (size_t)views * q_frame(c);
+    jfdk_status st = dev_alloc(c, &c->d_q, n, "the filtered projection store");
+    if (st) return st;
+    JFDK_CUDA(c, cudaMemsetAsync(c->d_q, 0, n * sizeof(float), c->stream), "clearing the projection store");
+    c->q_views = views;
+    return JFDK_OK;
+}
+
+jfdk_status ensure_acc(jfdk_ctx* c) {
+    if (c->d_sum) return JFDK_OK;
+    const size_t n = (size_t)c->X * c->Y * c->Z;
+    jfdk_status st = dev_alloc(c, &c->d_sum, n, "the backprojection sum volume");
+    if (st) return st;
+    return dev_alloc(c, &c->d_cnt, n, "the backprojection weight volume");
+}
+
+WeightParams weight_params(const jfdk_ctx* c) {
+    WeightParams w{};
+    w.tinv = c->d_tinv;
+    w.dmin = c->d_dmin;
+    w.num_views = c->nviews;
+    w.L = c->L;
+    w.det_right = c->mirror;
+    w.mirror = c->mirror;
+    return w;
+}
+
+PrepParams prep_params(const jfdk_ctx* c, const uint16_t* raw) {
+    PrepParams p{};
+    p.raw = raw;
+    p.in_w = c->scan.num_dets_u;
+    p.in_h = c->scan.num_dets_v;
+    p.crop_x = c->scan.border_left;
+    p.crop_y = c->scan.border_up;
+    p.width = c->used_u;
+    p.rows = c->used_v;
+    p.bright_field = c->scan.bright_field;
+    p.bhc0 = c->scan.beam_hardening[0];
+    p.bhc1 = c->scan.beam_hardening[1];
+    p.bhc2 = c->scan.beam_hardening[2];
+    // PreProcessingCore.cpp:56 -- skipped when the parameters are (1, 0, 0)
+    p.do_bhc = !(p.bhc0 == 1.0f && p.bhc1 == 0.0f && p.bhc2 == 0.0f);
+    return p;
+}
+
+BPParams bp_params(const jfdk_ctx* c) {
+    BPParams b{};
+    b.q = c->d_q;
+    b.uw = c->d_uw;
+    b.ptm = c->d_ptm;
+    b.frame_stride = q_frame(c);
+    b.U = c->out_w;
+    b.V = c->rows;
+    b.pitch = c->q_pitch;
+    b.X = c->X; b.Y = c->Y; b.Z = c->Z;
+    b.pxy = c->pxy; b.pz = c->pz;
+    b.z_begin = 0; b.z_end = c->Z;
+    b.ct_scale = c->ct_scale;
+    b.ct_norm1 = c->recon.ct_norm1;
+    return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+jfdk_status jfdk_device_check(char* msg, int msg_len) {
+    int dev = 0, n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    std::string m;
+    jfdk_status st = JFDK_OK;
+    if (e != cudaSuccess || n == 0) {
+        m = std::string("no CUDA device: ") + cudaGetErrorString(e);
+        st = JFDK_ERR_NO_DEVICE;
+        cudaGetLastError();
+    } else {
+        cudaGetDevice(&dev);
+        cudaDeviceProp prop{};
+        cudaGetDeviceProperties(&prop, dev);
+        m = std::string(prop.name) + " sm_" + std::to_string(prop.major) + std::to_string(prop.minor);
+        if (prop.major != 10) st = JFDK_ERR_NO_DEVICE;
+    }
+    if (msg && msg_len > 0) {
+        std::strncpy(msg, m.c_str(), msg_len - 1);
+        msg[msg_len - 1] = 0;
+    }
+    return st;
+}
+
+const char* jfdk_last_error(const jfdk_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+long long jfdk_kernel_launches(const jfdk_ctx* c) { return c ? c->launches : 0; }
+
+void jfdk_destroy(jfdk_ctx* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    dev_free(c->d_ptm); dev_free(c->d_uw); dev_free(c->d_tinv); dev_free(c->d_dmin);
+    dev_free(c->d_T); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_q);
+    dev_free(c->d_sum); dev_free(c->d_cnt); dev_free(c->d_raw_stage); dev_free(c->d_hu_stage);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk_recon_params* recon,
+                        const float* h_ptms, int precision, void* cuda_stream) {
+    if (!out || !scan || !recon || !h_ptms) return JFDK_ERR_INVALID;
+    *out = nullptr;
+    jfdk_ctx* c = new (std::nothrow) jfdk_ctx();
+    if (!c) return JFDK_ERR_OOM;
+    auto bail = [&](jfdk_status st) { *out = c; return st; };  // caller reads the message, then destroys
+    c->scan = *scan;
+    c->recon = *recon;
+    if (recon->num_adjust > 0) {
+        if (!recon->adjust_points || !recon->adjust_level_db)
+            return bail(fail(c, JFDK_ERR_INVALID, "adjust points without values"));
+        c->adj_pts.assign(recon->adjust_points, recon->adjust_points + recon->num_adjust);
+        c->adj_db.assign(recon->adjust_level_db, recon->adjust_level_db + recon->num_adjust);
+    }
+    c->recon.adjust_points = nullptr;
+    c->recon.adjust_level_db = nullptr;
+    c->precision = precision;
+    if (precision != JFDK_PRECISION_FP32)
+        return bail(fail(c, JFDK_ERR_UNSUPPORTED, "precision mode not available in this build"));
+    c->nviews = scan->num_views;
+    c->used_u = scan->num_dets_u - scan->border_left - scan->border_right;
+    c->used_v = scan->num_dets_v - scan->border_up - scan->border_down;
+    c->in_w = scan->filter_input_width > 0 ? scan->filter_input_width : c->used_u;
+    c->out_w = c->used_u;
+    c->rows = c->used_v;
+    c->mirror = scan->detector_on_right ? 1 : 0;
+    c->X = recon->num_pixels_x; c->Y = recon->num_pixels_y; c->Z = recon->num_pixels_z;
+    c->pxy = recon->pitch_xy; c->pz = recon->pitch_z;
+    if (c->nviews < 1 || c->used_u < 3 || c->used_v < 1 || c->in_w < 3 || c->X < 1 || c->Y < 1 || c->Z < 1 ||
+        scan->border_left < 0 || scan->border_right < 0 || scan->border_up < 0 || scan->border_down < 0 ||
+        !(scan->dso > 1.0f) || !(scan->bright_field > 0.0f) || !(recon->mu_water != 0.0f) ||
+        (long long)c->rows * c->in_w > (1LL << 31) || (long long)c->X * c->Y > (1LL << 31))
+        return bail(fail(c, JFDK_ERR_INVALID, "invalid scan or reconstruction size"));
+    if (c->mirror && c->in_w < c->out_w)
+        return bail(fail(c, JFDK_ERR_INVALID, "mirrored filter needs input width >= output width"));
+    c->L = fft_length(c->in_w);
+    if (scan->half_sample_rate > 0.0f) {
+        c->hsr = scan->half_sample_rate;
+    } else {  // Config/ConfigHelper.cpp:52-53
+        const float det_at_iso = scan->detector_pixel_size / scan->dsd * scan->dso;
+        c->hsr = 0.5f * (1.0f / det_at_iso);
+    }
+    c->q_pitch = (int)round_up(c->out_w + 1, 4);
+    c->groups = (c->nviews + 8) / 9;
+    c->ct_scale = recon->ct_norm0 * 1000.f / recon->mu_water;  // CTNumCore.cpp:24
+    c->ptms.assign(h_ptms, h_ptms + (size_t)c->nviews * 12);
+
+    int dev = 0;
+    JFDK_CUDA(c, cudaGetDevice(&dev), "cudaGetDevice");
+    cudaDeviceProp prop{};
+    JFDK_CUDA(c, cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+    if (prop.major != 10) return bail(fail(c, JFDK_ERR_NO_DEVICE, "libjfdk needs an sm_100 (B200) device"));
+    c->device = dev;
+    if (cuda_stream) {
+        c->stream = static_cast<cudaStream_t>(cuda_stream);
+    } else {
+        JFDK_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        c->own_stream = true;
+    }
+
+    const std::string msg = build_host_operators(*scan, c->recon, c->adj_pts, c->adj_db, h_ptms, c->in_w,
+                                                 c->out_w, c->rows, c->mirror, c->hsr, c->ops);
+    if (!msg.empty()) return bail(fail(c, JFDK_ERR_INVALID, msg));
+
+    // device constants
+    jfdk_status st;
+    if ((st = dev_alloc(c, &c->d_ptm, (size_t)c->nviews * 12, "the projection matrices"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_uw, (size_t)c->nviews * c->q_pitch, "the u-tapers"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_tinv, (size_t)c->groups * 16, "the inverse transforms"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_dmin, (size_t)c->groups, "the pre-weight minima"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_T, (size_t)c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_c, (size_t)c->out_w, "the edge response"))) return bail(st);
+    std::vector<float> uwp((size_t)c->nviews * c->q_pitch, 0.0f);
+    for (int v = 0; v < c->nviews; ++v)
+        std::memcpy(&uwp[(size_t)v * c->q_pitch], &c->ops.uw[(size_t)v * c->out_w], sizeof(float) * c->out_w);
+    std::vector<float> Tp((size_t)c->out_w * a_pitch(c), 0.0f);
+    for (int j = 0; j < c->out_w; ++j)
+        std::memcpy(&Tp[(size_t)j * a_pitch(c)], &c->ops.T[(size_t)j * c->in_w], sizeof(float) * c->in_w);
+    JFDK_CUDA(c, cudaMemcpyAsync(c->d_ptm, h_ptms, sizeof(float) * c->nviews * 12, cudaMemcpyHostToDevice, c->stream), "upload");
+    JFDK_CUDA(c, cudaMemcpyAsync(c->d_uw, uwp.data(), sizeof(float) * uwp.size(), cudaMemcpyHostToDevice, c->stream), "upload");
+    JFDK_CUDA(c, cudaMemcpyAsync(c->d_tinv, c->ops.tinv.data(), sizeof(float) * c->ops.tinv.size(), cudaMemcpyHostToDevice, c->stream), "upload");
+    JFDK_CUDA(c, cudaMemcpyAsync(c->d_T, Tp.data(), sizeof(float) * Tp.size(), cudaMemcpyHostToDevice, c->stream), "upload");
+    JFDK_CUDA(c, cudaMemcpyAsync(c->d_c, c->ops.c.data(), sizeof(float) * c->out_w, cudaMemcpyHostToDevice, c->stream), "upload");
+    JFDK_LAUNCH(c, launch_preweight_dmin(c->d_tinv, c->groups, c->rows, c->L, c->in_w, c->mirror, c->d_dmin, c->stream),
+                "pre-weight minimum");
+    JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "context setup");
+    *out = c;
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_set_option(jfdk_ctx* c, int key, long long value) {
+    if (!c) return JFDK_ERR_INVALID;
+    switch (key) {
+        case JFDK_OPT_BP_EXACT: c->opt_bp_exact = value ? 1 : 0; return JFDK_OK;
+        case JFDK_OPT_VIEW_CHUNK:
+            if (value < 1 || value > 4096) return fail(c, JFDK_ERR_INVALID, "view chunk out of range");
+            c->opt_view_chunk = (int)value;
+            return JFDK_OK;
+        default: return fail(c, JFDK_ERR_INVALID, "unknown option");
+    }
+}
+
+jfdk_status jfdk_sync(jfdk_ctx* c) {
+    if (!c) return JFDK_ERR_INVALID;
+    JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "stream synchronize");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_get_dims(const jfdk_ctx* c, int* in_w, int* out_w, int* L, int* rows) {
+    if (!c) return JFDK_ERR_INVALID;
+    if (in_w) *in_w = c->in_w;
+    if (out_w) *out_w = c->out_w;
+    if (L) *L = c->L;
+    if (rows) *rows = c->rows;
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_get_uweights(const jfdk_ctx* c, float* h) {
+    if (!c || !h) return JFDK_ERR_INVALID;
+    std::memcpy(h, c->ops.uw.data(), sizeof(float) * c->ops.uw.size());
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_get_ramp_operator(const jfdk_ctx* c, float* T, float* cc) {
+    if (!c) return JFDK_ERR_INVALID;
+    if (T) std::memcpy(T, c->ops.T.data(), sizeof(float) * c->ops.T.size());
+    if (cc) std::memcpy(cc, c->ops.c.data(), sizeof(float) * c->ops.c.size());
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_preprocess_frames(jfdk_ctx* c, const uint16_t* d_raw, int nv, float* d_out) {
+    if (!c || !d_raw || !d_out || nv < 0) return fail(c, JFDK_ERR_INVALID, "preprocess: bad argument");
+    if (nv == 0) return JFDK_OK;
+    JFDK_LAUNCH(c, launch_preprocess(prep_params(c, d_raw), nv, d_out, c->stream), "preprocess");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_filter_frames(jfdk_ctx* c, const float* d_in, int v0, int nv, float* d_out) {
+    if (!c || !d_in || !d_out || nv < 0 || v0 < 0) return fail(c, JFDK_ERR_INVALID, "filter: bad argument");
+    if (nv == 0) return JFDK_OK;
+    jfdk_status st = ensure_A(c, (size_t)nv * c->rows);
+    if (st) return st;
+    JFDK_LAUNCH(c, launch_weight(d_in, nv, v0, c->in_w, c->rows, weight_params(c), c->d_A, a_pitch(c), c->d_e, c->stream),
+                "pre-weight");
+    RampParams r{};
+    r.A = c->d_A; r.e = c->d_e; r.B = c->d_T; r.c = c->d_c;
+    r.M = nv * c->rows; r.N = c->out_w; r.K = c->in_w; r.a_pitch = a_pitch(c);
+    r.rows = c->rows; r.view_base = v0; r.store_base = 0;
+    r.uw = nullptr; r.uw_pitch = c->q_pitch;
+    r.q = d_out; r.q_frame_stride = (long long)c->rows * c->out_w; r.q_pitch = c->out_w;
+    JFDK_LAUNCH(c, launch_ramp_gemm(r, c->stream), "ramp filter");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_zfilter_frames(jfdk_ctx* c, float* d, int nv) {
+    if (!c || !d || nv < 0) return fail(c, JFDK_ERR_INVALID, "zfilter: bad argument");
+    if (nv == 0) return JFDK_OK;
+    JFDK_LAUNCH(c, launch_zfilter(d, nv, c->rows, c->out_w, (long long)c->rows * c->out_w, c->out_w, c->stream),
+                "z-filter");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_bp_reset(jfdk_ctx* c) {
+    if (!c) return JFDK_ERR_INVALID;
+    jfdk_status st = ensure_acc(c);
+    if (st) return st;
+    const size_t n = (size_t)c->X * c->Y * c->Z * sizeof(float);
+    JFDK_CUDA(c, cudaMemsetAsync(c->d_sum, 0, n, c->stream), "clearing the sum volume");
+    JFDK_CUDA(c, cudaMemsetAsync(c->d_cnt, 0, n, c->stream), "clearing the weight volume");
+    c->bp_has_views = true;
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_bp_accumulate(jfdk_ctx* c, const float* d_proj, int v0, int nv) {
+    if (!c || !d_proj || nv < 0 || v0 < 0 || v0 + nv > c->nviews)
+        return fail(c, JFDK_ERR_INVALID, "bp_accumulate: bad argument");
+    if (!c->d_sum) return fail(c, JFDK_ERR_STATE, "bp_accumulate before bp_reset");
+    if (nv == 0) return JFDK_OK;
+    jfdk_status st = ensure_Q(c, nv);
+    if (st) return st;
+    // copy into the padded store (pad column and row stay zero)
+    JFDK_CUDA(c, cudaMemcpy2DAsync(c->d_q, sizeof(float) * c->q_pitch, d_proj, sizeof(float) * c->out_w,
+                                   sizeof(float) * c->out_w, c->rows, cudaMemcpyDeviceToDevice, c->stream),
+              "staging projections");
+    for (int i = 1; i < nv; ++i)
+        JFDK_CUDA(c, cudaMemcpy2DAsync(c->d_q + (size_t)i * q_frame(c), sizeof(float) * c->q_pitch,
+                                       d_proj + (size_t)i * c->rows * c->out_w, sizeof(float) * c->out_w,
+                                       sizeof(float) * c->out_w, c->rows, cudaMemcpyDeviceToDevice, c->stream),
+                  "staging projections");
+    BPParams b = bp_params(c);
+    b.view_base = v0; b.v0 = v0; b.nv = nv;
+    b.sum = c->d_sum; b.cnt = c->d_cnt; b.load_acc = 1;
+    JFDK_LAUNCH(c, launch_bp(b, false, false, c->opt_bp_exact != 0, c->stream), "backprojection");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_finalize(jfdk_ctx* c, int z0, int nz, int apply_ct, float* d_out, int16_t* d_out16) {
+    if (!c || z0 < 0 || nz < 0 || z0 + nz > c->Z || (!d_out && !d_out16))
+        return fail(c, JFDK_ERR_INVALID, "finalize: bad argument");
+    if (!c->d_sum) return fail(c, JFDK_ERR_STATE, "finalize before any backprojection");
+    const size_t plane = (size_t)c->X * c->Y;
+    JFDK_LAUNCH(c, launch_finalize(c->d_sum + z0 * plane, c->d_cnt + z0 * plane, nz * plane, apply_ct, c->ct_scale,
+                                   c->recon.ct_norm1, d_out, d_out16, c->stream),
+                "finalize");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_ctnum(jfdk_ctx* c, float* d, size_t n) {
+    if (!c || !d) return fail(c, JFDK_ERR_INVALID, "ctnum: bad argument");
+    if (n == 0) return JFDK_OK;
+    JFDK_LAUNCH(c, launch_ctnum(d, n, c->ct_scale, c->recon.ct_norm1, c->stream), "ct numbers");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, int16_t* d_hu16) {
+    if (!c || !d_raw || (!d_hu && !d_hu16)) return fail(c, JFDK_ERR_INVALID, "reconstruct: bad argument");
+    if (c->in_w != c->used_u)
+        return fail(c, JFDK_ERR_UNSUPPORTED, "reconstruct: conjugate-view compositing (filter width != frame width)");
+    jfdk_status st = ensure_Q(c, c->nviews);
+    if (st) return st;
+    const int chunk = std::min(c->opt_view_chunk, c->nviews);
+    if ((st = ensure_A(c, (size_t)chunk * c->rows))) return st;
+    const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;
+    const bool zf = c->recon.z_filter != 0;
+    for (int v0 = 0; v0 < c->nviews; v0 += chunk) {
+        const int nv = std::min(chunk, c->nviews - v0);
+        JFDK_LAUNCH(c, launch_prep_weight(prep_params(c, d_raw + (size_t)v0 * frame), nv, v0, weight_params(c), c->d_A,
+                                          a_pitch(c), c->d_e, c->stream),
+                    "preprocess + pre-weight");
+        RampParams r{};
+        r.A = c->d_A; r.e = c->d_e; r.B = c->d_T; r.c = c->d_c;
+        r.M = nv * c->rows; r.N = c->out_w; r.K = c->in_w; r.a_pitch = a_pitch(c);
+        r.rows = c->rows; r.view_base = v0; r.store_base = v0;
+        r.uw = zf ? nullptr : c->d_uw; r.uw_pitch = c->q_pitch;
+        r.q = c->d_q; r.q_frame_stride = q_frame(c); r.q_pitch = c->q_pitch;
+        JFDK_LAUNCH(c, launch_ramp_gemm(r, c->stream), "ramp filter");
+    }
+    if (zf)
+        JFDK_LAUNCH(c, launch_zfilter(c->d_q, c->nviews, c->rows, c->out_w, q_frame(c), c->q_pitch, c->stream),
+                    "z-filter");
+    BPParams b = bp_params(c);
+    b.view_base = 0; b.v0 = 0; b.nv = c->nviews;
+    b.out = d_hu; b.out16 = d_hu16; b.apply_ct = 1;
+    JFDK_LAUNCH(c, launch_bp(b, true, !zf, c->opt_bp_exact != 0, c->stream), "backprojection");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_reconstruct_host(jfdk_ctx* c, const uint16_t* h_raw, float* h_hu) {
+    if (!c || !h_raw || !h_hu) return fail(c, JFDK_ERR_INVALID, "reconstruct_host: bad argument");
+    const size_t raw_bytes = (size_t)c->nviews * c->scan.num_dets_u * c->scan.num_dets_v * sizeof(uint16_t);
+    const size_t hu_bytes = (size_t)c->X * c->Y * c->Z * sizeof(float);
+    jfdk_status st;
+    if (c->raw_stage_bytes < raw_bytes) {
+        dev_free(c->d_raw_stage);
+        c->raw_stage_bytes = 0;
+        if ((st = dev_alloc(c, &c->d_raw_stage, raw_bytes / sizeof(uint16_t), "the raw frames"))) return st;
+        c->raw_stage_bytes = raw_bytes;
+    }
+    if (c->hu_stage_bytes < hu_bytes) {
+        dev_free(c->d_hu_stage);
+        c->hu_stage_bytes = 0;
+        if ((st = dev_alloc(c, &c->d_hu_stage, hu_bytes / sizeof(float), "the output volume"))) return st;
+        c->hu_stage_bytes = hu_bytes;
+    }
+    JFDK_CUDA(c, cudaMemcpyAsync(c->d_raw_stage, h_raw, raw_bytes, cudaMemcpyHostToDevice, c->stream), "raw upload");
+    if ((st = jfdk_reconstruct(c, c->d_raw_stage, c->d_hu_stage, nullptr))) return st;
+    JFDK_CUDA(c, cudaMemcpyAsync(h_hu, c->d_hu_stage, hu_bytes, cudaMemcpyDeviceToHost, c->stream), "volume download");
+    JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "reconstruct_host");
+    return JFDK_OK;
+}
+
+}  // extern "C"

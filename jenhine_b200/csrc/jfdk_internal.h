@@ -1,0 +1,163 @@
+// jfdk_internal.h -- context layout and helpers shared by the engine's
+// translation units.  Not part of the public ABI (include/jfdk.h is).
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/jfdk.h"
+
+namespace jfdk {
+
+// Host-side operators derived from the geometry and filter parameters
+// (geometry.cpp).  All are per-context constants.
+struct HostOperators {
+    std::vector<float> uw;      // [views][out_w]   BP u-taper (BPCore.cpp:68-100)
+    std::vector<float> tinv;    // [groups][16]     inverse TM per 9-view group
+    std::vector<float> T;       // [out_w][in_w]    ramp operator (Toeplitz)
+    std::vector<float> c;       // [out_w]          edge-ramp response
+    std::vector<float> H;       // [L/2+1]          filter spectrum
+};
+
+int fft_length(int width);  // FilterCore::CalFFTLength
+// Fills ops from the context's parameters; returns "" or an error message.
+std::string build_host_operators(const jfdk_scan_params& scan, const jfdk_recon_params& recon,
+                                 const std::vector<float>& adj_pts,
+                                 const std::vector<float>& adj_db, const float* ptms,
+                                 int in_w, int out_w, int rows, int mirror, float hsr,
+                                 HostOperators& ops);
+
+// Parameters of the backprojection kernels (bp.cu).
+struct BPParams {
+    const float* q;          // filtered projections, [views][rows + 1][pitch] float
+    const __half* qh;        // same in FP16 (mixed precision), or null
+    const float* qscale;     // [views] dequantisation scale (mixed precision)
+    const float* uw;         // [views][pitch] u-taper (zero padded)
+    const float* ptm;        // [views][12]
+    long long frame_stride;  // elements between views in q / qh
+    int view_base;           // index of q's first frame in the rotation
+    int v0, nv;              // views to accumulate (rotation indices)
+    int U, V, pitch;         // columns, rows, row pitch of q
+    int X, Y, Z;
+    float pxy, pz;
+    int z_begin, z_end;      // slices handled by this launch
+    float* sum;              // [Z][Y][X] accumulators (chunked mode)
+    float* cnt;
+    int load_acc;            // add to sum/cnt already in memory
+    float* out;              // finalize: [Z][Y][X] float or null
+    int16_t* out16;          // finalize: int16 HU or null
+    int apply_ct;
+    float ct_scale, ct_norm1;
+};
+
+// Launchers (return cudaError_t of the launch).
+cudaError_t launch_bp(const BPParams& p, bool finalize, bool tapered, bool exact,
+                      cudaStream_t s);
+cudaError_t launch_finalize(const float* sum, const float* cnt, size_t n, int apply_ct,
+                            float ct_scale, float norm1, float* out, int16_t* out16,
+                            cudaStream_t s);
+cudaError_t launch_ctnum(float* d, size_t n, float ct_scale, float norm1, cudaStream_t s);
+
+struct PrepParams {
+    const uint16_t* raw;     // [nv][in_h][in_w]
+    int in_w, in_h, crop_x, crop_y;
+    int width, rows;         // used (cropped) frame size
+    float bright_field;
+    float bhc0, bhc1, bhc2;
+    int do_bhc;
+};
+struct WeightParams {
+    const float* tinv;       // [groups][16]
+    const float* dmin;       // [groups]
+    int num_views;           // views per rotation
+    int L;                   // FFT length (pre-weight row length)
+    int det_right;
+    int mirror;
+};
+cudaError_t launch_preprocess(const PrepParams& p, int nv, float* out, cudaStream_t s);
+// Pre-weight + edge mean of frames already preprocessed (agent path).
+cudaError_t launch_weight(const float* in, int nv, int v0, int width, int rows,
+                          const WeightParams& w, float* A, int a_pitch, float* e,
+                          cudaStream_t s);
+// Raw -> weighted A operand + edge means in one pass (whole-volume path).
+cudaError_t launch_prep_weight(const PrepParams& p, int nv, int v0, const WeightParams& w,
+                               float* A, int a_pitch, float* e, cudaStream_t s);
+// Frame minimum of the pre-weight distance per group.
+cudaError_t launch_preweight_dmin(const float* tinv, int groups, int rows, int L,
+                                  int in_w, int det_right, float* dmin, cudaStream_t s);
+
+struct RampParams {
+    const float* A;          // [M][a_pitch]
+    const float* e;          // [M]
+    const float* B;          // [N][K] Toeplitz operator
+    const float* c;          // [N]
+    int M, N, K, a_pitch;
+    int rows;                // rows per view (M = nv * rows)
+    int view_base;           // rotation index of A's first view
+    int store_base;          // index of A's first view in the output store
+    const float* uw;         // [views][uw_pitch] taper or null (agent path)
+    int uw_pitch;
+    float* q;                // output, [..][rows + pad][q_pitch]
+    long long q_frame_stride;
+    int q_pitch;
+};
+cudaError_t launch_ramp_gemm(const RampParams& p, cudaStream_t s);
+
+cudaError_t launch_zfilter(float* frames, int nv, int rows, int width, long long frame_stride,
+                           int pitch, cudaStream_t s);
+
+}  // namespace jfdk
+
+struct jfdk_ctx {
+    jfdk_scan_params scan{};
+    jfdk_recon_params recon{};
+    std::vector<float> adj_pts, adj_db;
+    int precision = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // sizes
+    int nviews = 0;
+    int used_u = 0, used_v = 0;   // cropped frame
+    int in_w = 0, out_w = 0;      // filter input / output widths
+    int rows = 0, L = 0, mirror = 0;
+    float hsr = 0.f;
+    int X = 0, Y = 0, Z = 0;
+    float pxy = 0.f, pz = 0.f;
+    int q_pitch = 0;              // filtered store row pitch (floats), >= out_w + 1
+    int groups = 0;
+    float ct_scale = 0.f;
+
+    std::vector<float> ptms;
+    jfdk::HostOperators ops;
+
+    // device constants
+    float* d_ptm = nullptr;
+    float* d_uw = nullptr;       // [views][q_pitch]
+    float* d_tinv = nullptr;
+    float* d_dmin = nullptr;
+    float* d_T = nullptr;
+    float* d_c = nullptr;
+
+    // device working storage (allocated on demand)
+    float* d_A = nullptr;  size_t a_rows = 0;   // weighted rows, pitch in_w
+    float* d_e = nullptr;
+    float* d_q = nullptr;  int q_views = 0;     // filtered store
+    float* d_sum = nullptr;
+    float* d_cnt = nullptr;
+    uint16_t* d_raw_stage = nullptr; size_t raw_stage_bytes = 0;
+    float* d_hu_stage = nullptr; size_t hu_stage_bytes = 0;
+    bool bp_has_views = false;
+
+    // JFDK_OPT_* settings
+    int opt_bp_exact = 0;
+    int opt_view_chunk = 32;
+
+    long long launches = 0;
+    std::string err;
+};

@@ -1,0 +1,219 @@
+"""Python host API over libjfdk.so.
+
+``FDKEngine`` mirrors the per-stage interface of the reference's agents:
+
+=====================  ===========================================  ==============================
+method                 reference                                    C ABI
+=====================  ===========================================  ==============================
+``preprocess``         PreProcessingCore::Process                   jfdk_preprocess_frames
+``filter``             FilterAgent::ProcessTask / FilterCore         jfdk_filter_frames
+``zfilter``            ZFilterAgent::ProcessTask                    jfdk_zfilter_frames
+``bp_reset``           BPCUDACore::InitShot_Synced / BPCore::InitShot jfdk_bp_reset
+``bp_accumulate``      BPCUDACore::DeployBackProj (BPCore semantics) jfdk_bp_accumulate
+``finalize``           BPCore::DoneSlice (+ CTNumCore::Process)     jfdk_finalize
+``ctnum``              CTNumCore::Process                           jfdk_ctnum
+``reconstruct``        the whole Proj -> Slice pipeline             jfdk_reconstruct
+=====================  ===========================================  ==============================
+
+Device buffers are torch CUDA tensors (torch provides allocation and streams
+only); every computation runs in libjfdk.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+
+
+@dataclasses.dataclass
+class ScanConfig:
+    """Config/ScanParams.h fields (snake case)."""
+    num_views: int
+    dso: float
+    dsd: float
+    num_dets_u: int
+    num_dets_v: int
+    detector_pixel_size: float
+    border_up: int = 0
+    border_down: int = 0
+    border_left: int = 0
+    border_right: int = 0
+    bright_field: float = 50000.0
+    beam_hardening: Sequence[float] = (1.0, 0.0, 0.0)
+    half_sample_rate: float = 0.0       # 0: derived as Config/ConfigHelper.cpp:52-53
+    detector_on_right: bool = False
+    filter_input_width: int = 0          # 0: the used detector width
+
+
+@dataclasses.dataclass
+class ReconConfig:
+    """Config/ReconParams.h fields (snake case)."""
+    num_pixels_x: int
+    num_pixels_y: int
+    num_pixels_z: int
+    pitch_xy: float
+    pitch_z: float
+    ct_norm0: float = 1.0
+    ct_norm1: float = 1.0
+    mu_water: float = 0.02
+    filter_cutoff_start: float = 0.0
+    filter_cutoff_end: float = 0.0
+    adjust_points: Sequence[float] = ()
+    adjust_level_db: Sequence[float] = ()
+    z_filter: bool = False
+
+
+def _ptr(t) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+class FDKEngine:
+    """One reconstruction context (one CUDA stream) on the current device."""
+
+    def __init__(self, scan: ScanConfig, recon: ReconConfig, ptms, precision: str = "fp32",
+                 stream=None, bp_exact: bool = False, view_chunk: Optional[int] = None):
+        self.lib = _lib.load()
+        self.scan, self.recon = scan, recon
+        self.ptms = np.ascontiguousarray(np.asarray(ptms, np.float32).reshape(-1, 12))
+        if self.ptms.shape[0] != scan.num_views:
+            raise ValueError("need one 3x4 projection matrix per view")
+        sp = _lib.ScanParams()
+        for f in ("num_views", "dso", "dsd", "num_dets_u", "num_dets_v", "detector_pixel_size",
+                  "border_up", "border_down", "border_left", "border_right", "bright_field",
+                  "half_sample_rate", "filter_input_width"):
+            setattr(sp, f, getattr(scan, f))
+        sp.beam_hardening[:] = [float(x) for x in scan.beam_hardening]
+        sp.detector_on_right = int(bool(scan.detector_on_right))
+        self._adj = (np.ascontiguousarray(recon.adjust_points, np.float32),
+                     np.ascontiguousarray(recon.adjust_level_db, np.float32))
+        if self._adj[0].size != self._adj[1].size:
+            raise ValueError("adjust points and levels differ in length")
+        rp = _lib.ReconParams()
+        for f in ("num_pixels_x", "num_pixels_y", "num_pixels_z", "pitch_xy", "pitch_z", "ct_norm0",
+                  "ct_norm1", "mu_water", "filter_cutoff_start", "filter_cutoff_end"):
+            setattr(rp, f, getattr(recon, f))
+        rp.num_adjust = self._adj[0].size
+        fp = C.POINTER(C.c_float)
+        rp.adjust_points = self._adj[0].ctypes.data_as(fp)
+        rp.adjust_level_db = self._adj[1].ctypes.data_as(fp)
+        rp.z_filter = int(bool(recon.z_filter))
+        prec = {"fp32": _lib.PRECISION_FP32, "mixed": _lib.PRECISION_MIXED}[precision]
+        ctx = C.c_void_p()
+        st = self.lib.jfdk_create(C.byref(ctx), C.byref(sp), C.byref(rp),
+                                  self.ptms.ctypes.data_as(C.c_void_p), prec,
+                                  C.c_void_p(stream) if stream else None)
+        if st != _lib.JFDK_OK:
+            msg = self.lib.jfdk_last_error(ctx).decode() if ctx.value else ""
+            if ctx.value:
+                self.lib.jfdk_destroy(ctx)
+            raise _lib.JfdkError(st, msg)
+        self.ctx = ctx
+        if bp_exact:
+            self._check(self.lib.jfdk_set_option(ctx, _lib.OPT_BP_EXACT, 1))
+        if view_chunk:
+            self._check(self.lib.jfdk_set_option(ctx, _lib.OPT_VIEW_CHUNK, int(view_chunk)))
+        dims = [C.c_int() for _ in range(4)]
+        self._check(self.lib.jfdk_get_dims(ctx, *[C.byref(d) for d in dims]))
+        self.filter_in_w, self.filter_out_w, self.fft_length, self.rows = [d.value for d in dims]
+
+    # -- plumbing -------------------------------------------------------------
+    def _check(self, st):
+        _lib.check(self.ctx, st)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.jfdk_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def sync(self):
+        self._check(self.lib.jfdk_sync(self.ctx))
+
+    @property
+    def kernel_launches(self) -> int:
+        return self.lib.jfdk_kernel_launches(self.ctx)
+
+    def uweights(self) -> np.ndarray:
+        w = np.empty((self.scan.num_views, self.filter_out_w), np.float32)
+        self._check(self.lib.jfdk_get_uweights(self.ctx, w.ctypes.data_as(C.c_void_p)))
+        return w
+
+    def ramp_operator(self):
+        T = np.empty((self.filter_out_w, self.filter_in_w), np.float32)
+        c = np.empty(self.filter_out_w, np.float32)
+        self._check(self.lib.jfdk_get_ramp_operator(self.ctx, T.ctypes.data_as(C.c_void_p),
+                                                    c.ctypes.data_as(C.c_void_p)))
+        return T, c
+
+    # -- stages (torch CUDA tensors in and out) ----------------------------------
+    def preprocess(self, raw, out=None):
+        import torch
+        nv = raw.shape[0]
+        used_v = self.scan.num_dets_v - self.scan.border_up - self.scan.border_down
+        used_u = self.scan.num_dets_u - self.scan.border_left - self.scan.border_right
+        out = out if out is not None else torch.empty((nv, used_v, used_u), dtype=torch.float32, device=raw.device)
+        self._check(self.lib.jfdk_preprocess_frames(self.ctx, _ptr(raw), nv, _ptr(out)))
+        return out
+
+    def filter(self, frames, v0: int = 0, out=None):
+        import torch
+        nv = frames.shape[0]
+        out = out if out is not None else torch.empty((nv, self.rows, self.filter_out_w), dtype=torch.float32,
+                                                      device=frames.device)
+        self._check(self.lib.jfdk_filter_frames(self.ctx, _ptr(frames), v0, nv, _ptr(out)))
+        return out
+
+    def zfilter(self, frames):
+        self._check(self.lib.jfdk_zfilter_frames(self.ctx, _ptr(frames), frames.shape[0]))
+        return frames
+
+    def bp_reset(self):
+        self._check(self.lib.jfdk_bp_reset(self.ctx))
+
+    def bp_accumulate(self, frames, v0: int):
+        self._check(self.lib.jfdk_bp_accumulate(self.ctx, _ptr(frames), v0, frames.shape[0]))
+
+    def finalize(self, apply_ctnum: bool = True, z0: int = 0, nz: Optional[int] = None, out=None,
+                 out16=None, device="cuda"):
+        import torch
+        nz = self.recon.num_pixels_z - z0 if nz is None else nz
+        shape = (nz, self.recon.num_pixels_y, self.recon.num_pixels_x)
+        if out is None and out16 is None:
+            out = torch.empty(shape, dtype=torch.float32, device=device)
+        self._check(self.lib.jfdk_finalize(self.ctx, z0, nz, int(apply_ctnum), _ptr(out), _ptr(out16)))
+        return out if out is not None else out16
+
+    def ctnum(self, vol):
+        self._check(self.lib.jfdk_ctnum(self.ctx, _ptr(vol), vol.numel()))
+        return vol
+
+    def reconstruct(self, raw, out=None, out16=None):
+        import torch
+        shape = (self.recon.num_pixels_z, self.recon.num_pixels_y, self.recon.num_pixels_x)
+        if out is None and out16 is None:
+            out = torch.empty(shape, dtype=torch.float32, device=raw.device)
+        self._check(self.lib.jfdk_reconstruct(self.ctx, _ptr(raw), _ptr(out), _ptr(out16)))
+        return out if out is not None else out16
+
+    def reconstruct_host(self, raw: np.ndarray, out: Optional[np.ndarray] = None) -> np.ndarray:
+        raw = np.ascontiguousarray(raw, np.uint16)
+        shape = (self.recon.num_pixels_z, self.recon.num_pixels_y, self.recon.num_pixels_x)
+        out = out if out is not None else np.empty(shape, np.float32)
+        self._check(self.lib.jfdk_reconstruct_host(self.ctx, raw.ctypes.data_as(C.c_void_p),
+                                                   out.ctypes.data_as(C.c_void_p)))
+        return out

@@ -1,0 +1,92 @@
+"""The benchmark workloads, each a seeded synthetic scan.
+
+c1  plain FDK, CPU-runnable: 360 views over 360 deg, SID 500 mm, SDD 800 mm,
+    256 x 256 detector at 0.5 mm, 10-ellipsoid phantom (mu 0-0.05 /mm),
+    I0 = 1e5 Poisson noise, per-pixel gain 1 +/- 0.05 and offset 0-50 in the
+    raw data, 128^3 volume at 0.5 mm.
+c2  dental-CBCT size, plain FP32: 600 views over 360 deg, 768 x 768 detector
+    at 0.2 mm, 640 x 640 x 480 volume at 0.125 mm, per-view flexmap
+    (+/- 0.5 px detector shift, +/- 0.2 deg tilt), 20 ellipsoids plus 3
+    metal inserts (mu 0.5 /mm), I0 = 5e4.  The orbit is not given for this
+    case; it uses c1's SID 500 mm / SDD 800 mm.
+mini_*  reduced versions of c1 / c2 for parity tests.
+
+The reference corrects gain with one scalar bright field
+(PreProcessingAgent/GainCorr.cpp:10-13); the per-pixel gain and offset are
+properties of the synthetic detector, left in the raw frames.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+from .fdk import ReconConfig, ScanConfig
+from .phantom import ScanGeometry, random_phantom
+
+
+@dataclasses.dataclass
+class Workload:
+    name: str
+    geom: ScanGeometry
+    recon: ReconConfig
+    n_ellipsoids: int
+    n_metal: int
+    i0: float
+    bright_field: float = 50000.0
+    gain_spread: float = 0.05
+    offset_max: float = 50.0
+    beam_hardening: tuple = (1.0, 0.0, 0.0)
+
+    @property
+    def scan(self) -> ScanConfig:
+        g = self.geom
+        return ScanConfig(num_views=g.n_views, dso=g.sid, dsd=g.sdd, num_dets_u=g.det_u,
+                          num_dets_v=g.det_v, detector_pixel_size=g.pixel_u,
+                          bright_field=self.bright_field, beam_hardening=self.beam_hardening)
+
+    def phantom(self):
+        r = self.recon
+        extent = (r.num_pixels_x * r.pitch_xy, r.num_pixels_y * r.pitch_xy, r.num_pixels_z * r.pitch_z)
+        return random_phantom(self.geom.seed + 1, extent, self.n_ellipsoids, n_metal=self.n_metal)
+
+    @property
+    def updates(self) -> int:
+        """Voxel-view updates of one reconstruction (the GUPS numerator)."""
+        r = self.recon
+        return r.num_pixels_x * r.num_pixels_y * r.num_pixels_z * self.geom.n_views
+
+    def raw_numpy(self):
+        from .phantom import line_integrals, raw_frames
+        return raw_frames(line_integrals(self.geom, self.phantom()), self.geom.seed + 2, i0=self.i0,
+                          bright_field=self.bright_field, gain_spread=self.gain_spread,
+                          offset_max=self.offset_max)
+
+    def raw_torch(self, device="cuda"):
+        from .phantom import raw_frames_torch
+        return raw_frames_torch(self.geom, self.phantom(), self.geom.seed + 2, self.i0, self.bright_field,
+                                self.gain_spread, self.offset_max, device=device)
+
+
+def c1() -> Workload:
+    return Workload("c1", ScanGeometry(360, 500.0, 800.0, 256, 256, 0.5, 0.5, seed=101),
+                    ReconConfig(128, 128, 128, 0.5, 0.5, ct_norm0=1.0, ct_norm1=1.0), 10, 0, 1e5)
+
+
+def c2() -> Workload:
+    return Workload("c2", ScanGeometry(600, 500.0, 800.0, 768, 768, 0.2, 0.2, flex_shift_px=0.5,
+                                       flex_tilt_deg=0.2, seed=202),
+                    ReconConfig(640, 640, 480, 0.125, 0.125, ct_norm0=1.0, ct_norm1=1.0), 20, 3, 5e4)
+
+
+def mini_c1() -> Workload:
+    return Workload("mini_c1", ScanGeometry(48, 500.0, 800.0, 64, 56, 2.0, 2.0, seed=5),
+                    ReconConfig(40, 40, 32, 1.6, 1.6, ct_norm0=1.2, ct_norm1=1.0), 10, 0, 1e5)
+
+
+def mini_c2() -> Workload:
+    return Workload("mini_c2", ScanGeometry(60, 500.0, 800.0, 96, 80, 1.6, 1.6, flex_shift_px=0.5,
+                                            flex_tilt_deg=0.2, seed=6),
+                    ReconConfig(64, 64, 48, 1.25, 1.25, ct_norm0=1.2, ct_norm1=0.9), 20, 3, 5e4,
+                    beam_hardening=(1.0, 0.05, 0.01))
+
+
+WORKLOADS = {"c1": c1, "c2": c2, "mini_c1": mini_c1, "mini_c2": mini_c2}

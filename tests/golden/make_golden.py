@@ -1,0 +1,75 @@
+"""Generate tests/golden/*.npz from the reference's own Core classes.
+
+Runs the JEngine PreProcessingCore / PreFilterWeightGenerator / FilterCore /
+BPCore / CTNumCore compiled from source (oracle/_ref, built by
+oracle/build.py with the project's IPP/MKL shims) on small seeded inputs and
+stores inputs and outputs.  The GPU parity tests and the CPU oracle tests read
+these files; nothing at test time needs the reference tree.
+
+Usage:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from jenhine_b200.phantom import ScanGeometry, line_integrals, random_phantom, raw_frames  # noqa: E402
+from oracle.pyoracle import RefCores  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# Small cases of the two benchmark geometries (same orbit and magnification,
+# fewer views, coarser detector and volume so each file stays small).
+CASES = {
+    "mini_c1": dict(geom=dict(n_views=36, sid=500.0, sdd=800.0, det_u=48, det_v=40, pixel_u=2.0,
+                              pixel_v=2.0, seed=11),
+                    vol=(24, 24, 20, 2.5, 2.5), phantom=dict(n=10), i0=1e5, bf=50000.0,
+                    bhc=(1.0, 0.0, 0.0), norm=(1.2, 1.0)),
+    "mini_c2": dict(geom=dict(n_views=40, sid=500.0, sdd=800.0, det_u=56, det_v=44, pixel_u=2.6,
+                              pixel_v=2.6, flex_shift_px=0.5, flex_tilt_deg=0.2, seed=22),
+                    vol=(32, 32, 24, 2.5, 2.5), phantom=dict(n=20, n_metal=3), i0=5e4,
+                    bf=50000.0, bhc=(1.0, 0.05, 0.01), norm=(1.2, 0.9),
+                    filt=dict(cut_start=0.0, cut_end=0.0, adj_pts=(0.05, 0.1), adj_db=(1.0, -1.0))),
+}
+
+
+def make(name: str, c: dict, ref: RefCores) -> str:
+    g = ScanGeometry(**c["geom"])
+    X, Y, Z, pxy, pz = c["vol"]
+    ph = random_phantom(c["geom"]["seed"] + 1, (X * pxy, Y * pxy, Z * pz), **c["phantom"])
+    raw = raw_frames(line_integrals(g, ph), c["geom"]["seed"] + 2, i0=c["i0"], bright_field=c["bf"])
+    ptms = g.ptms()
+    dso = np.float32(g.sid)
+    hsr = g.half_sample_rate
+    f = c.get("filt", {})
+    prep = ref.preprocess(raw, c["bf"], c["bhc"])
+    filt = ref.filter(prep, ptms, hsr, float(dso), f.get("cut_start", 0.0), f.get("cut_end", 0.0),
+                      f.get("adj_pts", ()), f.get("adj_db", ()), nthreads=4)
+    bp = ref.bp(filt, ptms, X, Y, Z, pxy, pz, nthreads=4)
+    hu = ref.ctnum(bp, *c["norm"])
+    pw0 = ref.preweight(ptms, g.det_u, g.det_v, float(dso), 4)
+    path = os.path.join(OUT, f"{name}.npz")
+    np.savez_compressed(
+        path, raw=raw, ptms=ptms, dso=dso, hsr=np.float32(hsr), bright_field=np.float32(c["bf"]),
+        bhc=np.asarray(c["bhc"], np.float32), vol=np.asarray([X, Y, Z], np.int32),
+        pitch=np.asarray([pxy, pz], np.float32), norm=np.asarray(c["norm"], np.float32),
+        cut=np.asarray([f.get("cut_start", 0.0), f.get("cut_end", 0.0)], np.float32),
+        adj_pts=np.asarray(f.get("adj_pts", ()), np.float32),
+        adj_db=np.asarray(f.get("adj_db", ()), np.float32),
+        prep=prep, preweight_v4=pw0, filt=filt, bp=bp, hu=hu)
+    return path
+
+
+def main() -> None:
+    ref = RefCores()
+    for name, c in CASES.items():
+        print(make(name, c, ref))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,178 @@
+"""Pin the CPU oracle (oracle/fdk_oracle.c) before trusting it.
+
+1. The golden values of the reference's own unit tests:
+   UTFilterAgent/UTPreFilterWeightGenerator.cpp:46-48, UTTransformMatrix/
+   UTTransformMatrix.cpp:40-68, UTPerformance/UTRealFFT.cpp:13-142,
+   UTTransformMatrix/UTProjectionMatrixModifier.cpp:14-219.
+2. The reference's Core classes compiled from source (oracle/_ref), on the
+   committed golden fixtures and on fresh seeded inputs.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_l2
+
+# UTPreFilterWeightGenerator.cpp:8-20
+PW_PTM = np.array([-1.33108, -7.78814, -0.01779, 573.81219, -0.96645, -0.02576, 7.50237, 344.55353,
+                   -0.00225, 0.00000, 0.00000, 1.00000], np.float32)
+# UTTransformMatrix.cpp:42-50
+TM_PTM = np.array([-1.31600, -7.78872, -0.02526, 573.39276, -0.95473, -0.03864, 7.52651, 344.78983,
+                   -0.00225, -0.00000, 0.00000, 1.00000], np.float32)
+TM_GOLD = np.array([-1.31600, -7.78872, -0.02526, 573.39276, -0.95473, -0.03864, 7.52651, 344.78983,
+                    -0.99675, -0.0, 0.0, 5.0977446e-06, -0.00225, -0.00000, 0.00000, 1.00000], np.float32)
+
+
+def ulps(a, b):
+    a = np.float32(a); b = np.float32(b)
+    return abs(int(a.view(np.int32)) - int(b.view(np.int32)))
+
+
+def test_preweight_golden(oracle):
+    w = oracle.preweight_for_view(PW_PTM, 443.0, 686, 644, False)
+    assert w.shape == (644, 2048)
+    # The frame minimum sits where the reference's float computation put it.
+    assert w[429, 591] == 1.0
+    # MKL's sgesv operation order is not public; the restated LAPACK order
+    # lands within 7 float ULPs (4.2e-7) of the two non-trivial goldens, whose
+    # own error against the FP64 value is ~2e-6.
+    assert abs(w[0, 0] - np.float32(0.977879)) <= 5e-7
+    assert abs(w[-1, -1] - np.float32(0.9202493)) <= 5e-7
+    assert w.min() > 0.9 and w.max() == 1.0
+
+
+def test_ptm2tm_golden(oracle):
+    tm = oracle.ptm2tm(TM_PTM, 443.0)
+    for i in range(16):
+        assert ulps(tm[i], TM_GOLD[i]) <= 4, (i, tm[i], TM_GOLD[i])  # EXPECT_FLOAT_EQ
+
+
+def test_rfft_golden(oracle):
+    x = np.arange(1, 8, dtype=np.float32)
+    f = oracle.rfft_forward(x)
+    gold = np.array([28.0, 0.0, -3.49999976, 7.26782513, -3.5, 2.79115677, -3.5, 0.798852026], np.float32)
+    np.testing.assert_allclose(f, gold, rtol=0, atol=2e-6)  # MKL's floats, our double FFT
+    back = oracle.rfft_backward(f, 7)
+    for i in range(7):
+        assert ulps(back[i], x[i]) <= 4
+
+
+@pytest.mark.parametrize("n", [100, 101])
+def test_ramlak_spectrum(oracle, n):
+    # UTRealFFT.cpp:70-142: the Ram-Lak kernel's spectrum is ~ i / n, imag ~ 0
+    rl = np.zeros(n, np.float32)
+    rl[0] = 0.25
+    pipi = np.float32(np.pi) * np.float32(np.pi)
+    for i in range(1, n // 2 + 1, 2):
+        rl[i] = rl[n - i] = np.float32(-1.0) / (pipi * np.float32(i) * np.float32(i))
+    f = oracle.rfft_forward(rl)
+    re, im = f[0::2], f[1::2]
+    assert np.all(np.abs(im[1:]) < 1e-7)
+    np.testing.assert_allclose(re, np.arange(n // 2 + 1) / np.float32(n), atol=0.003)
+
+
+CUBE = [(x, y, z) for x in (-1.0, 1.0) for y in (-1.0, 1.0) for z in (-1.0, 1.0)]
+
+
+def _uv(p, x, y, z):
+    p = p.astype(np.float32).reshape(3, 4)
+    h = p @ np.array([x, y, z, 1.0], np.float32)
+    return h[0] / h[2], h[1] / h[2]
+
+
+@pytest.mark.parametrize("op", ["move_u", "move_v", "reverse_x", "reverse_y", "move_z"])
+def test_ptm_modifier_properties(oracle, op):
+    # UTProjectionMatrixModifier.cpp: moving the detector axis shifts (u, v)
+    # by the distance; reversing an axis mirrors that world coordinate;
+    # moving z translates the volume.
+    d = 2.0
+    p1 = oracle.ptm_modify(TM_PTM, op, d)
+    for x, y, z in CUBE:
+        if op == "reverse_x":
+            a, b = _uv(TM_PTM, x, y, z), _uv(p1, -x, y, z)
+        elif op == "reverse_y":
+            a, b = _uv(TM_PTM, x, y, z), _uv(p1, x, -y, z)
+        elif op == "move_z":
+            a, b = _uv(TM_PTM, x, y, z + d), _uv(p1, x, y, z)
+        else:
+            a, b = _uv(TM_PTM, x, y, z), _uv(p1, x, y, z)
+            b = (b[0] + d, b[1]) if op == "move_u" else (b[0], b[1] + d)
+        np.testing.assert_allclose(a, b, rtol=2e-6, atol=1e-4)
+
+
+def test_preweight_grouping(oracle):
+    # FilterAgent.cpp:101-126: weight of views 9g..9g+8 comes from view min(9g+4, N-1)
+    assert [oracle.preweight_source_view(v, 40) for v in (0, 8, 9, 17, 35, 36, 39)] == [4, 4, 13, 13, 31, 39, 39]
+
+
+def test_uweights_centred_detector(oracle):
+    from jenhine_b200.phantom import ScanGeometry
+    g = ScanGeometry(4, 500.0, 800.0, 64, 32, 2.0, 2.0)
+    w = oracle.bp_uweights(g.ptms(), 64)
+    # isocentre column 31 -> taper over the first 62 columns, ones after
+    assert np.all(w[:, 62:] == 1.0) and w[0, 0] == 0.0
+    assert np.all(np.diff(w[0, :62]) > 0)
+
+
+def test_ctnum_values(oracle):
+    v = np.array([0.0, 0.02, 0.026, 0.05, 1.0, np.nan], np.float32)
+    h = oracle.ctnum(v, 1.0, 0.5)
+    assert h[0] == -1000.0 and h[1] == 0.0
+    assert h[2] == np.float32(300.0) or abs(h[2] - 300.0) < 1e-3
+    s = np.float32(1.0) * np.float32(1000.0) / np.float32(0.02)
+    hh = np.float32(np.float32(0.05) * s) - np.float32(1000.0)
+    assert h[3] == np.float32(np.float32(np.float32(hh - np.float32(300.0)) * np.float32(0.5)) + np.float32(300.0))
+    assert h[4] == 8191.0 or h[4] < 8191.0
+    assert np.isnan(h[5])
+
+
+# ---- restatement vs the reference Cores ------------------------------------
+
+def test_golden_fixtures_vs_restatement(oracle, golden):
+    name, g = golden
+    X, Y, Z = (int(v) for v in g["vol"])
+    pxy, pz = (float(v) for v in g["pitch"])
+    prep = oracle.preprocess(g["raw"], float(g["bright_field"]), g["bhc"])
+    np.testing.assert_array_equal(prep, g["prep"])
+    H = oracle.filter_spectrum(oracle.fft_length(prep.shape[2]), float(g["hsr"]), *g["cut"],
+                               g["adj_pts"], g["adj_db"])
+    filt = oracle.filter_projections(g["prep"], g["ptms"], H, float(g["dso"]))
+    assert rel_l2(filt, g["filt"]) < 1e-6
+    pw = oracle.preweight_for_view(g["ptms"][4], float(g["dso"]), prep.shape[2], prep.shape[1])
+    np.testing.assert_allclose(pw, g["preweight_v4"], rtol=0, atol=2e-6)
+    bp = oracle.bp(g["filt"], g["ptms"], X, Y, Z, pxy, pz)
+    np.testing.assert_array_equal(bp, g["bp"])      # same float order as BPCore
+    hu = oracle.ctnum(g["bp"], *g["norm"])
+    np.testing.assert_array_equal(hu, g["hu"])      # CTNumCore bit for bit
+
+
+def test_restatement_vs_refcores_fresh(oracle, refcores):
+    from jenhine_b200.phantom import ScanGeometry, line_integrals, random_phantom, raw_frames
+    g = ScanGeometry(27, 450.0, 700.0, 40, 36, 2.4, 2.4, flex_shift_px=0.3, flex_tilt_deg=0.1, seed=77)
+    ph = random_phantom(78, (48, 48, 40), 6)
+    raw = raw_frames(line_integrals(g, ph), 79, i0=2e4, bright_field=30000.0, gain_spread=0.02, offset_max=20)
+    P = g.ptms()
+    bhc = (1.0, 0.1, 0.02)
+    prep_o = oracle.preprocess(raw, 30000.0, bhc, borders=(2, 1, 3, 1))
+    prep_r = refcores.preprocess(raw, 30000.0, bhc, borders=(2, 1, 3, 1))
+    np.testing.assert_array_equal(prep_o, prep_r)
+    W = prep_o.shape[2]
+    H = oracle.filter_spectrum(oracle.fft_length(W), g.half_sample_rate, 0.05, 0.2, (0.1,), (2.0,))
+    f_o = oracle.filter_projections(prep_o, P, H, 450.0)
+    f_r = refcores.filter(prep_r, P, g.half_sample_rate, 450.0, 0.05, 0.2, (0.1,), (2.0,))
+    assert rel_l2(f_o, f_r) < 1e-6
+    # mirrored (detector on the right), output narrower than input
+    f_om = oracle.filter_rows(prep_o[0], H, oracle.fft_length(W), W - 6, True)
+    f_rm = refcores.filter_rows_noweight(prep_o[0], g.half_sample_rate, 0.05, 0.2, (0.1,), (2.0,), True, W - 6)
+    assert rel_l2(f_om, f_rm) < 1e-6
+    vol_o = oracle.bp(f_r[:, :, :W], P, 20, 18, 14, 2.0, 2.5)
+    vol_r = refcores.bp(f_r, P, 20, 18, 14, 2.0, 2.5)
+    np.testing.assert_array_equal(vol_o, vol_r)
+    np.testing.assert_array_equal(oracle.ctnum(vol_o, 1.1, 0.8), refcores.ctnum(vol_r, 1.1, 0.8))
+
+
+def test_fp64_oracle_close_to_fp32(oracle):
+    g = load_golden("mini_c1")
+    X, Y, Z = (int(v) for v in g["vol"])
+    v32 = oracle.bp(g["filt"], g["ptms"], X, Y, Z, *map(float, g["pitch"]))
+    v64 = oracle.bp(g["filt"], g["ptms"], X, Y, Z, *map(float, g["pitch"]), f64=True)
+    assert rel_l2(v32, v64) < 1e-5
