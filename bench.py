@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""FDK reconstruction throughput on B200: GUPS (voxel-view updates / s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+                    [--workload c2] [--precision fp32] [--no-cpu-baseline]
+
+A step is one full reconstruction of the workload (raw uint16 frames ->
+preprocess -> cosine pre-weight -> ramp filter -> backprojection -> CT
+numbers) with the raw frames already resident in HBM.  Under torchrun each
+rank reconstructs its own seeded scan (independent objects, no data-path
+collective): weak scaling.  value = updates of all ranks / max over ranks of
+the device-timed K steps.
+
+e2e: the same metric through the C ABI's host-buffer call
+(jfdk_reconstruct_host): every step copies the raw frames in from pinned
+host memory and the HU volume back out.
+
+--impl reference times the reference's own CPU Cores (PreProcessingCore,
+FilterAgent/FilterCore + PreFilterWeightGenerator, BPAgent/BPCore,
+CTNumCore compiled from source into oracle/_ref) on the host cores, each step
+a bounded sample of the same workload extrapolated to one volume.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GUPS (voxel·view/s) & s/volume, 640²×480 from 600 views: mixed vs plain FP32"
+DATA = "synthetic: seeded ellipsoid phantom, analytic line integrals, Poisson noise, per-pixel gain/offset"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed"])
+    ap.add_argument("--exact", action="store_true", help="BPCore-exact backprojection rounding")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(w):
+    r, g = w.recon, w.geom
+    return {"workload": f"{w.name}: {r.num_pixels_x}x{r.num_pixels_y}x{r.num_pixels_z} from {g.n_views} views "
+                        f"of {g.det_u}x{g.det_v}",
+            "views": g.n_views, "detector": [g.det_u, g.det_v], "volume": [r.num_pixels_x, r.num_pixels_y,
+                                                                          r.num_pixels_z],
+            "voxel_mm": [r.pitch_xy, r.pitch_z], "sid_sdd_mm": [g.sid, g.sdd],
+            "updates_per_volume": w.updates,
+            "l2": "inputs larger than L2 (raw frames, filtered store and volume each > 126 MB)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.idx = gpu_index
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [l.strip().split(", ") for l in self.f.read().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic(name: str):
+    """dram bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/<name>.md, line 'dram_bytes_per_launch: N')."""
+    path = os.path.join(ROOT, "profiles", f"{name}.md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_sample(w, raw_np, filt_np, ptms, bounded=True):
+    """Reference CPU Cores on a bounded sample, extrapolated to one volume.
+    Returns (GUPS, cores, kind, sample description, seconds spent)."""
+    import numpy as np
+    try:
+        from oracle.pyoracle import RefCores
+        impl, kind = RefCores(), "reference"
+    except (OSError, FileNotFoundError, RuntimeError):
+        from oracle.pyoracle import Oracle
+        impl, kind = Oracle(), "port"
+    cores = os.cpu_count() or 1
+    r, g = w.recon, w.geom
+    nv_f = min(12, g.n_views)
+    nv_b = min(60, g.n_views)
+    nz = min(16, r.num_pixels_z)
+    t0 = time.perf_counter()
+    if kind == "reference":
+        prep = impl.preprocess(raw_np[:nv_f], w.bright_field, w.beam_hardening, nthreads=cores)
+        t1 = time.perf_counter()
+        impl.filter(prep, ptms, g.half_sample_rate, g.sid, nthreads=cores)
+        t2 = time.perf_counter()
+        # BPCore over a z-slab: the reference backprojects the whole volume,
+        # whose cost is linear in slices; the slab is the first nz slices.
+        zmid = r.num_pixels_z // 2 - nz // 2
+        slab = _ref_bp_slab(impl, filt_np[:nv_b], ptms[:nv_b], r, nz, zmid, cores)
+        t3 = time.perf_counter()
+        impl.ctnum(slab, r.ct_norm0, r.ct_norm1)
+        t4 = time.perf_counter()
+    else:
+        prep = impl.preprocess(raw_np[:nv_f], w.bright_field, w.beam_hardening)
+        t1 = time.perf_counter()
+        H = impl.filter_spectrum(impl.fft_length(g.det_u), g.half_sample_rate)
+        for v in range(nv_f):
+            impl.filter_rows(prep[v], H, impl.fft_length(g.det_u))
+        t2 = time.perf_counter()
+        slab = impl.bp(filt_np[:nv_b], ptms[:nv_b], r.num_pixels_x, r.num_pixels_y, r.num_pixels_z,
+                       r.pitch_xy, r.pitch_z, z0=r.num_pixels_z // 2 - nz // 2, nz=nz, nthreads=cores)
+        t3 = time.perf_counter()
+        impl.ctnum(slab, r.ct_norm0, r.ct_norm1)
+        t4 = time.perf_counter()
+    per_volume = ((t1 - t0) + (t2 - t1)) * g.n_views / nv_f + (t3 - t2) * (g.n_views / nv_b) * (
+        r.num_pixels_z / nz) + (t4 - t3) * r.num_pixels_z / nz
+    sample = (f"preprocess+filter of {nv_f} views (x{g.n_views / nv_f:g}) and BP of {nv_b} views into "
+              f"{nz} of {r.num_pixels_z} slices (x{g.n_views / nv_b * r.num_pixels_z / nz:g}), "
+              f"extrapolated to one volume: {per_volume:.1f} s/volume")
+    return w.updates / per_volume / 1e9, cores, kind, sample, t4 - t0, per_volume
+
+
+def _ref_bp_slab(ref, filt, ptms, r, nz, z0, cores):
+    """The reference BPCore on slices [z0, z0+nz): shift the volume centre with
+    the reference's own MoveZAxis PTM edit (JEngine/JEngine.cpp:149) so a
+    nz-slice BPCore reconstructs exactly that slab."""
+    import numpy as np
+    zc = (z0 + (nz - 1) / 2.0) - (r.num_pixels_z - 1) / 2.0
+    p = np.stack([ref.ptm_modify(ptms[i], "move_z", float(np.float32(zc * r.pitch_z))) for i in range(len(ptms))])
+    return ref.bp(filt, p, r.num_pixels_x, r.num_pixels_y, nz, r.pitch_xy, r.pitch_z, nthreads=cores)
+
+
+def run_reference(a, w, rank, world):
+    """--impl reference: the reference CPU implementation, rank 0 only."""
+    if rank != 0:
+        return
+    import numpy as np
+    from jenhine_b200.phantom import line_integrals, raw_frames
+    g = w.geom
+    ptms = g.ptms()
+    # inputs for the sample: raw frames of the first views and filtered views
+    nv = min(60, g.n_views)
+    lint = line_integrals(g, w.phantom(), views=range(nv))
+    raw = raw_frames(lint, g.seed + 2, i0=w.i0, bright_field=w.bright_field, gain_spread=w.gain_spread,
+                     offset_max=w.offset_max)
+    from oracle.pyoracle import Oracle
+    o = Oracle()
+    prep = o.preprocess(raw, w.bright_field, w.beam_hardening)
+    H = o.filter_spectrum(o.fft_length(g.det_u), g.half_sample_rate)
+    filt = np.stack([o.filter_rows(prep[v], H, o.fft_length(g.det_u)) for v in range(nv)])
+    vals, secs = [], []
+    for i in range(a.warmup + a.steps):
+        gups, cores, kind, sample, spent, per_volume = cpu_sample(w, raw, filt, ptms)
+        if i >= a.warmup:
+            vals.append(gups)
+            secs.append(per_volume)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": statistics.median(secs) * 1000.0,
+            "s_per_volume": statistics.median(secs), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": DATA, "config": workload_config(w),
+            "cpu_baseline": {"value": value, "unit": "GUPS", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from jenhine_b200.workloads import WORKLOADS
+    w = WORKLOADS[a.workload]()
+    if a.impl == "reference":
+        run_reference(a, w, rank, world)
+        return
+
+    import numpy as np
+    import torch
+    import datetime
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from jenhine_b200 import _lib
+    from jenhine_b200.fdk import FDKEngine
+
+    # each rank reconstructs its own scan
+    w.geom.seed += 1000 * rank
+    raw = w.raw_torch()
+    ptms = w.geom.ptms()
+    eng = FDKEngine(w.scan, w.recon, ptms, precision=a.precision, bp_exact=a.exact)
+    eng.set_option(_lib.OPT_STAGE_TIMING, 1)
+    r = w.recon
+    vol = torch.empty((r.num_pixels_z, r.num_pixels_y, r.num_pixels_x), dtype=torch.float32, device="cuda")
+    for _ in range(a.warmup):
+        eng.reconstruct(raw, vol)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.5)
+    launches0 = eng.kernel_launches
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stage_ms = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(a.steps):
+        eng.reconstruct(raw, vol)
+        stage_ms.append(eng.stage_times())   # events on the engine's stream
+    end.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = eng.kernel_launches - launches0
+    clk = clocks.stop()
+    ms = start.elapsed_time(end) / a.steps
+    ms_t = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = ms_t.item()
+    value = w.updates * world / (ms_max / 1000.0) / 1e9
+
+    # end to end through the host-buffer call, pinned memory
+    e2e = None
+    if not a.no_e2e:
+        raw_h = torch.empty(raw.shape, dtype=torch.uint16, pin_memory=True)
+        raw_h.copy_(raw.cpu())
+        out_h = torch.empty(vol.shape, dtype=torch.float32, pin_memory=True)
+        raw_np, out_np = raw_h.numpy(), out_h.numpy()
+        eng.reconstruct_host(raw_np, out_np)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s2.record()
+        for _ in range(a.steps):
+            eng.reconstruct_host(raw_np, out_np)
+        e2.record()
+        torch.cuda.synchronize()
+        ems = torch.tensor([s2.elapsed_time(e2) / a.steps], device="cuda")
+        if dist:
+            dist.all_reduce(ems, op=dist.ReduceOp.MAX)
+        e2e = {"value": w.updates * world / (ems.item() / 1000.0) / 1e9, "unit": "GUPS",
+               "h2d_bytes_per_step": int(raw.numel() * 2), "d2h_bytes_per_step": int(vol.numel() * 4),
+               "ms_per_step": ems.item()}
+
+    if rank == 0:
+        bp_ms = statistics.mean(s[2] for s in stage_ms)
+        pf_ms = statistics.mean(s[0] for s in stage_ms)
+        peak, peak_kind = measured_peaks()
+        g = w.geom
+        proj_bytes = g.n_views * g.det_v * g.det_u * 4
+        vol_bytes = r.num_pixels_x * r.num_pixels_y * r.num_pixels_z * 4
+        alg = proj_bytes + vol_bytes
+        achieved = alg / (bp_ms / 1000.0) / 1e9
+        line = {
+            "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_max, "s_per_volume": ms_max / 1000.0,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": DATA, "config": dict(workload_config(w), precision=a.precision,
+                                         bp_rounding="bpcore-exact" if a.exact else "fast",
+                                         parallelism=f"{world} independent scans, one per GPU"),
+            "stages_ms": {"preprocess_weight_filter": pf_ms, "backprojection_hu": bp_ms},
+            "roofline": {"kernel": "bp_kernel (backprojection + normalisation + CT numbers)",
+                         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                         "algorithmic_bytes_per_launch": alg,
+                         "traffic": profile_traffic(f"bp_kernel_{w.name}"),
+                         "note": "BP is issue/L1-bound, not HBM-bound: the HBM fraction shows how far the "
+                                 "kernel is from the memory floor"},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if not a.no_cpu_baseline and world == 1:
+            nvb = min(60, g.n_views)
+            raw_np = raw[:12].cpu().numpy()
+            filt = eng.filter(eng.preprocess(raw[:nvb]), 0).cpu().numpy()
+            gups, cores, kind, sample, spent, _ = cpu_sample(w, raw_np, filt, ptms)
+            line["cpu_baseline"] = {"value": gups, "unit": "GUPS", "cores": cores, "kind": kind,
+                                    "sample": sample, "seconds": spent}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -87,7 +87,9 @@ typedef struct jfdk_recon_params {
 typedef struct jfdk_ctx jfdk_ctx;
 
 /* Create a context on the current device and the given CUDA stream (NULL =
- * a private stream).  ptms: num_views x 12 floats, row-major 3x4 projection
+ * the legacy default stream; the caller keeps ownership of a stream it
+ * passes and must keep it alive until jfdk_destroy; all buffers the caller
+ * hands in must be ready on that stream).  ptms: num_views x 12 floats, row-major 3x4 projection
  * matrices (TransformMatrix/ProjectionMatrix.h:11-19) already adjusted the
  * way JEngine/JEngine.cpp:139-150 does.  Replaces the constructors of
  * PreProcessingCore, FilterCore + PreFilterWeightGenerator, BPCUDACore and
@@ -159,10 +161,16 @@ enum {
     JFDK_OPT_BP_EXACT = 1,    /* 1: backprojection rounds every step like BPCore
                                  (IEEE division, no contraction); 0 (default):
                                  one reciprocal per sample point, FMA lerps     */
-    JFDK_OPT_VIEW_CHUNK = 2   /* views preprocessed + filtered per launch in
+    JFDK_OPT_VIEW_CHUNK = 2,  /* views preprocessed + filtered per launch in
                                  jfdk_reconstruct (default 32)                   */
+    JFDK_OPT_STAGE_TIMING = 3 /* 1: jfdk_reconstruct records CUDA events on its
+                                 stream around each stage                        */
 };
 jfdk_status jfdk_set_option(jfdk_ctx* ctx, int key, long long value);
+/* Stage times (ms) of the last jfdk_reconstruct with JFDK_OPT_STAGE_TIMING:
+ * [0] preprocess + pre-weight + ramp filter, [1] z-filter, [2] backprojection
+ * with normalisation and CT numbers.  Synchronises the stream. */
+jfdk_status jfdk_stage_times(jfdk_ctx* ctx, float* ms3);
 
 /* ---- introspection (tests, autotuner) ------------------------------------ */
 

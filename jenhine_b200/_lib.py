@@ -24,6 +24,7 @@ PRECISION_MIXED = 1
 
 OPT_BP_EXACT = 1
 OPT_VIEW_CHUNK = 2
+OPT_STAGE_TIMING = 3
 
 
 class ScanParams(C.Structure):
@@ -67,6 +68,7 @@ _SIGS = {
     "jfdk_sync": ([_P], C.c_int),
     "jfdk_get_dims": ([_P, _P, _P, _P, _P], C.c_int),
     "jfdk_set_option": ([_P, C.c_int, C.c_longlong], C.c_int),
+    "jfdk_stage_times": ([_P, _P], C.c_int),
     "jfdk_preprocess_frames": ([_P, _P, C.c_int, _P], C.c_int),
     "jfdk_filter_frames": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
     "jfdk_zfilter_frames": ([_P, _P, C.c_int], C.c_int),

@@ -179,6 +179,8 @@ void jfdk_destroy(jfdk_ctx* c) {
     dev_free(c->d_ptm); dev_free(c->d_uw); dev_free(c->d_tinv); dev_free(c->d_dmin);
     dev_free(c->d_T); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_q);
     dev_free(c->d_sum); dev_free(c->d_cnt); dev_free(c->d_raw_stage); dev_free(c->d_hu_stage);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -237,12 +239,10 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     JFDK_CUDA(c, cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
     if (prop.major != 10) return bail(fail(c, JFDK_ERR_NO_DEVICE, "libjfdk needs an sm_100 (B200) device"));
     c->device = dev;
-    if (cuda_stream) {
-        c->stream = static_cast<cudaStream_t>(cuda_stream);
-    } else {
-        JFDK_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-        c->own_stream = true;
-    }
+    // NULL selects the legacy default stream, so the context's work is
+    // ordered with every other default-stream operation of the process.
+    c->stream = static_cast<cudaStream_t>(cuda_stream);
+    c->own_stream = false;
 
     const std::string msg = build_host_operators(*scan, c->recon, c->adj_pts, c->adj_db, h_ptms, c->in_w,
                                                  c->out_w, c->rows, c->mirror, c->hsr, c->ops);
@@ -282,8 +282,21 @@ jfdk_status jfdk_set_option(jfdk_ctx* c, int key, long long value) {
             if (value < 1 || value > 4096) return fail(c, JFDK_ERR_INVALID, "view chunk out of range");
             c->opt_view_chunk = (int)value;
             return JFDK_OK;
+        case JFDK_OPT_STAGE_TIMING:
+            if (value && !c->ev[0])
+                for (auto& e : c->ev) JFDK_CUDA(c, cudaEventCreate(&e), "cudaEventCreate");
+            c->opt_stage_timing = value ? 1 : 0;
+            return JFDK_OK;
         default: return fail(c, JFDK_ERR_INVALID, "unknown option");
     }
+}
+
+jfdk_status jfdk_stage_times(jfdk_ctx* c, float* ms) {
+    if (!c || !ms) return JFDK_ERR_INVALID;
+    if (!c->opt_stage_timing || !c->ev[0]) return fail(c, JFDK_ERR_STATE, "stage timing is off");
+    JFDK_CUDA(c, cudaEventSynchronize(c->ev[3]), "stage timing");
+    for (int i = 0; i < 3; ++i) JFDK_CUDA(c, cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]), "stage timing");
+    return JFDK_OK;
 }
 
 jfdk_status jfdk_sync(jfdk_ctx* c) {
@@ -408,6 +421,8 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, in
     if ((st = ensure_A(c, (size_t)chunk * c->rows))) return st;
     const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;
     const bool zf = c->recon.z_filter != 0;
+    const bool timing = c->opt_stage_timing != 0;
+    if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[0], c->stream), "event");
     for (int v0 = 0; v0 < c->nviews; v0 += chunk) {
         const int nv = std::min(chunk, c->nviews - v0);
         JFDK_LAUNCH(c, launch_prep_weight(prep_params(c, d_raw + (size_t)v0 * frame), nv, v0, weight_params(c), c->d_A,
@@ -421,13 +436,16 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, in
         r.q = c->d_q; r.q_frame_stride = q_frame(c); r.q_pitch = c->q_pitch;
         JFDK_LAUNCH(c, launch_ramp_gemm(r, c->stream), "ramp filter");
     }
+    if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[1], c->stream), "event");
     if (zf)
         JFDK_LAUNCH(c, launch_zfilter(c->d_q, c->nviews, c->rows, c->out_w, q_frame(c), c->q_pitch, c->stream),
                     "z-filter");
+    if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[2], c->stream), "event");
     BPParams b = bp_params(c);
     b.view_base = 0; b.v0 = 0; b.nv = c->nviews;
     b.out = d_hu; b.out16 = d_hu16; b.apply_ct = 1;
     JFDK_LAUNCH(c, launch_bp(b, true, !zf, c->opt_bp_exact != 0, c->stream), "backprojection");
+    if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[3], c->stream), "event");
     return JFDK_OK;
 }
 

@@ -157,6 +157,8 @@ struct jfdk_ctx {
     // JFDK_OPT_* settings
     int opt_bp_exact = 0;
     int opt_view_chunk = 32;
+    int opt_stage_timing = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
     long long launches = 0;
     std::string err;

@@ -102,10 +102,16 @@ class FDKEngine:
         rp.adjust_level_db = self._adj[1].ctypes.data_as(fp)
         rp.z_filter = int(bool(recon.z_filter))
         prec = {"fp32": _lib.PRECISION_FP32, "mixed": _lib.PRECISION_MIXED}[precision]
+        if stream is None:
+            # bind to torch's current stream so torch copies and the engine's
+            # kernels are ordered (0 is the legacy default stream)
+            import torch
+            stream = torch.cuda.current_stream().cuda_stream if torch.cuda.is_available() else 0
+        self.stream_handle = int(stream)
         ctx = C.c_void_p()
         st = self.lib.jfdk_create(C.byref(ctx), C.byref(sp), C.byref(rp),
                                   self.ptms.ctypes.data_as(C.c_void_p), prec,
-                                  C.c_void_p(stream) if stream else None)
+                                  C.c_void_p(self.stream_handle) if self.stream_handle else None)
         if st != _lib.JFDK_OK:
             msg = self.lib.jfdk_last_error(ctx).decode() if ctx.value else ""
             if ctx.value:
@@ -147,6 +153,16 @@ class FDKEngine:
     @property
     def kernel_launches(self) -> int:
         return self.lib.jfdk_kernel_launches(self.ctx)
+
+    def set_option(self, key: int, value: int):
+        self._check(self.lib.jfdk_set_option(self.ctx, key, int(value)))
+
+    def stage_times(self):
+        """ms of [prep + filter, z-filter, backprojection] of the last
+        reconstruct (needs set_option(OPT_STAGE_TIMING, 1))."""
+        ms = (C.c_float * 3)()
+        self._check(self.lib.jfdk_stage_times(self.ctx, ms))
+        return list(ms)
 
     def uweights(self) -> np.ndarray:
         w = np.empty((self.scan.num_views, self.filter_out_w), np.float32)

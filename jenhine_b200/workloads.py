@@ -77,6 +77,15 @@ def c2() -> Workload:
                     ReconConfig(640, 640, 480, 0.125, 0.125, ct_norm0=1.0, ct_norm1=1.0), 20, 3, 5e4)
 
 
+def c2_slab() -> Workload:
+    """c2's scan backprojected into a 16-slice central slab (profiling case:
+    same projections and kernels, 1/30 of the volume)."""
+    w = c2()
+    w.name = "c2_slab"
+    w.recon.num_pixels_z = 16
+    return w
+
+
 def mini_c1() -> Workload:
     return Workload("mini_c1", ScanGeometry(48, 500.0, 800.0, 64, 56, 2.0, 2.0, seed=5),
                     ReconConfig(40, 40, 32, 1.6, 1.6, ct_norm0=1.2, ct_norm1=1.0), 10, 0, 1e5)
@@ -89,4 +98,4 @@ def mini_c2() -> Workload:
                     beam_hardening=(1.0, 0.05, 0.01))
 
 
-WORKLOADS = {"c1": c1, "c2": c2, "mini_c1": mini_c1, "mini_c2": mini_c2}
+WORKLOADS = {"c1": c1, "c2": c2, "c2_slab": c2_slab, "mini_c1": mini_c1, "mini_c2": mini_c2}
