@@ -163,13 +163,16 @@ enum {
                                  one reciprocal per sample point, FMA lerps     */
     JFDK_OPT_VIEW_CHUNK = 2,  /* views preprocessed + filtered per launch in
                                  jfdk_reconstruct (default 32)                   */
-    JFDK_OPT_STAGE_TIMING = 3 /* 1: jfdk_reconstruct records CUDA events on its
+    JFDK_OPT_STAGE_TIMING = 3,/* 1: jfdk_reconstruct records CUDA events on its
                                  stream around each stage                        */
+    JFDK_OPT_BP_ZPT = 4       /* slices each backprojection thread keeps in
+                                 registers: 4 (default), 8 or 16                 */
 };
 jfdk_status jfdk_set_option(jfdk_ctx* ctx, int key, long long value);
 /* Stage times (ms) of the last jfdk_reconstruct with JFDK_OPT_STAGE_TIMING:
- * [0] preprocess + pre-weight + ramp filter, [1] z-filter, [2] backprojection
- * with normalisation and CT numbers.  Synchronises the stream. */
+ * [0] preprocess + pre-weight + ramp filter (+ z-filter) + packing for the
+ * backprojector, [1] reserved (0), [2] backprojection with normalisation and
+ * CT numbers.  Synchronises the stream. */
 jfdk_status jfdk_stage_times(jfdk_ctx* ctx, float* ms3);
 
 /* ---- introspection (tests, autotuner) ------------------------------------ */

@@ -25,6 +25,7 @@ PRECISION_MIXED = 1
 OPT_BP_EXACT = 1
 OPT_VIEW_CHUNK = 2
 OPT_STAGE_TIMING = 3
+OPT_BP_ZPT = 4
 
 
 class ScanParams(C.Structure):

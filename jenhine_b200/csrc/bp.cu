@@ -5,8 +5,9 @@
 // (BPAgent/BPCore.cpp:115-220):
 //   * per view the projection is multiplied by the view's u-taper and an
 //     image of the taper is backprojected alongside it (the weight);
-//   * for voxel (x, y, z): U = (x*P0 + (y*P1 + P3)) + z*P2, likewise V, W;
-//     u = U / W + 0.5, v = V / W + 0.5;
+//   * for voxel (x, y, z): U = (x*P0 + (y*P1 + P3)) + z*P2, likewise V, W,
+//     every product and sum rounded separately; u = U / W + 0.5,
+//     v = V / W + 0.5 with the quotient correctly rounded;
 //   * bilinear sample with pixel centres at integers, taken only when
 //     0 <= u <= cols-1 and 0 <= v <= rows-1 (ippiRemap leaves the destination
 //     untouched otherwise, so the view then adds nothing to sum or weight);
@@ -14,17 +15,25 @@
 // The reference GPU kernel (BPCUDAAgent/BPCUDACore.cu:25-66) differs: it
 // samples the taper without interpolation, checks only u and clamps v.
 //
-// Layout and work split: the volume is [z][y][x] with x fastest.  A CTA is
-// 32 x 8 threads over (x, y); each thread owns ZPT consecutive slices of its
-// (x, y) column and keeps their sums and weights in registers across all
-// views of the launch, so a launch that covers every view touches the volume
-// in HBM exactly once (the final store).  Filtered projections are read
-// through L1 from a padded store ([rows + 1][pitch] per view, zero padded) so
-// the bilinear +1 neighbours never need clamping.
+// Data layout.  The filtered, tapered projections are stored as "quads": for
+// every view, row r and column c one float4 (p[r][c], p[r+1][c], p[r][c+1],
+// p[r+1][c+1]) -- the whole bilinear footprint of a sample point in one
+// 16-byte load -- with zeros past the last row and column (pack_quads_kernel
+// writes it).  The taper is stored as pairs (w[c], w[c+1]).  The volume is
+// [z][y][x], x fastest.
 //
-// EXACT = true reproduces BPCore's rounding step for step (IEEE division,
-// every product and sum rounded separately); EXACT = false uses one
-// reciprocal per sample point and fused multiply-adds.
+// Work split.  A CTA is 32 x 8 threads over (x, y); each thread owns ZPT
+// consecutive slices of its (x, y) column and keeps (sum, weight) pairs in
+// registers across all views of the launch, so a launch covering every view
+// stores the volume once and never reads it.
+//
+// Arithmetic.  U, V are formed exactly as BPCore rounds them.  The quotients
+// are computed as a pair (packed f32x2) from one correctly
+// rounded reciprocal r = RN(1/W) and Markstein's correction q = RN(q0 + RN(U -
+// W q0) r), q0 = RN(U r), which yields RN(U / W); when P[10] == 0 for every
+// view W does not depend on z (BPCore adds z*0) and r is computed once per
+// (x, y, view).  EXACT additionally rounds the lerps step by step like
+// BPCore (every product and sum separately) instead of fusing them.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -51,7 +60,38 @@ __device__ __forceinline__ int16_t to_i16(float f) {
     return t >= 32767.0f ? (int16_t)32767 : (t <= -32768.0f ? (int16_t)-32768 : (int16_t)t);
 }
 
-template <int ZPT, bool FINALIZE, bool TAPERED, bool EXACT>
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// Packed f32x2 arithmetic.  Each lane of a single mul / add / fma rounds like
+// the scalar operation, but a packed multiply whose result feeds a packed add
+// can be fused into one fma by the compiler (measured on sm_100a with this
+// toolchain, for both the intrinsics and inline PTX with .rn), so every
+// product that BPCore rounds before adding is computed with scalar
+// __fmul_rn / __fadd_rn, which are never contracted.
+#define JFDK_PACKED_OP(name, op)                                                              \
+    __device__ __forceinline__ float2 name(float2 a, float2 b) {                              \
+        float2 d;                                                                             \
+        asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n " op \
+            " rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"                                          \
+            : "=f"(d.x), "=f"(d.y)                                                            \
+            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                        \
+        return d;                                                                             \
+    }
+JFDK_PACKED_OP(pmul, "mul.rn.f32x2")
+JFDK_PACKED_OP(padd, "add.rn.f32x2")
+#undef JFDK_PACKED_OP
+
+// a * b + c per lane, one rounding (fma.rn.f32x2).
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) {
+    float2 d;
+    asm("{\n .reg .b64 ra, rb, rc, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+        " mov.b64 rc, {%6, %7};\n fma.rn.f32x2 rd, ra, rb, rc;\n mov.b64 {%0, %1}, rd;\n}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
+template <int ZPT, bool FINALIZE, bool EXACT, bool WZ>
 __global__ void __launch_bounds__(256) bp_kernel(BPParams p) {
     const int x = blockIdx.x * 32 + threadIdx.x;
     const int y = blockIdx.y * 8 + threadIdx.y;
@@ -61,73 +101,67 @@ __global__ void __launch_bounds__(256) bp_kernel(BPParams p) {
     // Axes as BPCore builds them (BPCore.cpp:47-66): (i - (n-1)/2) * pitch.
     const float ax = __fmul_rn(__fadd_rn(-((float)p.X - 1.0f) / 2.0f, (float)x), p.pxy);
     const float ay = __fmul_rn(__fadd_rn(-((float)p.Y - 1.0f) / 2.0f, (float)y), p.pxy);
-    float az[ZPT], sum[ZPT], cnt[ZPT];
+    float az[ZPT];
+    float2 acc[ZPT];  // (sum, weight)
     const size_t plane = (size_t)p.X * p.Y;
     const size_t base = (size_t)y * p.X + x;
 #pragma unroll
     for (int k = 0; k < ZPT; ++k) {
-        az[k] = __fmul_rn(__fadd_rn(-((float)p.Z - 1.0f) / 2.0f, (float)(zb + k)), p.pz);
+        const float a = __fmul_rn(__fadd_rn(-((float)p.Z - 1.0f) / 2.0f, (float)(zb + k)), p.pz);
+        az[k] = a;
         const bool in = zb + k < p.z_end;
-        sum[k] = (p.load_acc && in) ? p.sum[(size_t)(zb + k) * plane + base] : 0.0f;
-        cnt[k] = (p.load_acc && in) ? p.cnt[(size_t)(zb + k) * plane + base] : 0.0f;
+        acc[k] = (p.load_acc && in) ? f2(p.sum[(size_t)(zb + k) * plane + base], p.cnt[(size_t)(zb + k) * plane + base])
+                                    : f2(0.0f, 0.0f);
     }
-    const float umax = (float)(p.U - 1), vmax = (float)(p.V - 1);
+    const float umax = (float)(p.U - 1), vmax = (float)(p.V - 1), fU = (float)p.U;
+    const float2 neg1 = f2(-1.0f, -1.0f);
 
     for (int view = p.v0; view < p.v0 + p.nv; ++view) {
         const float4* P4 = reinterpret_cast<const float4*>(p.ptm + (size_t)view * 12);
         const float4 r0 = __ldg(P4), r1 = __ldg(P4 + 1), r2 = __ldg(P4 + 2);
-        // XxPM0 + (YxPM1 + PM3), etc. (BPCore.cpp:120-145)
+        // (XxPM0 + (YxPM1 + PM3), XxPM4 + (YxPM5 + PM7)) and W (BPCore.cpp:120-145)
         const float Uxy = __fadd_rn(__fmul_rn(ax, r0.x), __fadd_rn(__fmul_rn(ay, r0.y), r0.w));
         const float Vxy = __fadd_rn(__fmul_rn(ax, r1.x), __fadd_rn(__fmul_rn(ay, r1.y), r1.w));
         const float Wxy = __fadd_rn(__fmul_rn(ax, r2.x), __fadd_rn(__fmul_rn(ay, r2.y), r2.w));
-        const float* __restrict__ q = p.q + (size_t)(view - p.view_base) * p.frame_stride;
-        const float* __restrict__ w = p.uw + (size_t)view * p.pitch;
+        const float rxy = WZ ? 0.0f : __frcp_rn(Wxy);
+        const float4* __restrict__ q = p.q4 + (size_t)(view - p.view_base) * p.q4_frame;
+        const float2* __restrict__ tw = p.tw + (size_t)view * p.U;
 #pragma unroll
         for (int k = 0; k < ZPT; ++k) {
-            float u, v;
+            const float2 UV = f2(__fadd_rn(Uxy, __fmul_rn(az[k], r0.z)), __fadd_rn(Vxy, __fmul_rn(az[k], r1.z)));
+            float W = Wxy, r = rxy;
+            if (WZ) {
+                W = __fadd_rn(Wxy, __fmul_rn(az[k], r2.z));
+                r = __frcp_rn(W);
+            }
+            const float2 rr = f2(r, r);
+            const float2 q0 = pmul(UV, rr);
+            const float2 rem = pfma(f2(-W, -W), q0, UV);           // exact remainder
+            float2 uv = padd(pfma(rem, rr, q0), f2(0.5f, 0.5f));
+            // Branch-free so the loads of all ZPT slices can be in flight at
+            // once: a point off the detector reads quad (0, 0) and adds nothing.
+            const bool in = (uv.x >= 0.0f) & (uv.x <= umax) & (uv.y >= 0.0f) & (uv.y <= vmax);
+            uv = in ? uv : f2(0.0f, 0.0f);
+            const float fu = floorf(uv.x), fv = floorf(uv.y);
+            const float2 fxy = pfma(f2(fu, fv), neg1, uv);            // (u - fu, v - fv), exact
+            const int idx = __float2int_rz(fmaf(fv, fU, fu));         // exact: < 2^24
+            const int ix = __float2int_rz(fu);
+            const float4 Q = __ldg(q + idx);
+            const float2 w = __ldg(tw + ix);
+            const float2 lo = f2(Q.x, Q.y), hi = f2(Q.z, Q.w);       // columns ix, ix + 1
+            const float2 d = pfma(lo, neg1, hi);                      // RN(hi - lo)
+            float val, c;
             if (EXACT) {
-                const float Uz = __fadd_rn(Uxy, __fmul_rn(az[k], r0.z));
-                const float Vz = __fadd_rn(Vxy, __fmul_rn(az[k], r1.z));
-                const float Wz = __fadd_rn(Wxy, __fmul_rn(az[k], r2.z));
-                u = __fadd_rn(__fdiv_rn(Uz, Wz), 0.5f);
-                v = __fadd_rn(__fdiv_rn(Vz, Wz), 0.5f);
+                const float t0 = __fadd_rn(lo.x, __fmul_rn(fxy.x, d.x));
+                const float t1 = __fadd_rn(lo.y, __fmul_rn(fxy.x, d.y));
+                val = __fadd_rn(t0, __fmul_rn(fxy.y, __fsub_rn(t1, t0)));
+                c = __fadd_rn(w.x, __fmul_rn(fxy.x, __fsub_rn(w.y, w.x)));
             } else {
-                const float Uz = fmaf(az[k], r0.z, Uxy);
-                const float Vz = fmaf(az[k], r1.z, Vxy);
-                const float Wz = fmaf(az[k], r2.z, Wxy);
-                const float rw = __frcp_rn(Wz);
-                u = fmaf(Uz, rw, 0.5f);
-                v = fmaf(Vz, rw, 0.5f);
+                const float2 t = pfma(f2(fxy.x, fxy.x), d, lo);
+                val = fmaf(fxy.y, t.y - t.x, t.x);
+                c = fmaf(fxy.x, w.y - w.x, w.x);
             }
-            if (u >= 0.0f && u <= umax && v >= 0.0f && v <= vmax) {
-                const float fu = floorf(u), fv = floorf(v);
-                const int ix = (int)fu, iy = (int)fv;
-                const float fx = u - fu, fy = v - fv;   // exact (Sterbenz)
-                const float* r = q + (size_t)iy * p.pitch + ix;
-                float p00 = __ldg(r), p01 = __ldg(r + 1);
-                float p10 = __ldg(r + p.pitch), p11 = __ldg(r + p.pitch + 1);
-                const float w0 = __ldg(w + ix), w1 = __ldg(w + ix + 1);
-                if (!TAPERED) {  // InitView's in-place projection *= uWeight
-                    p00 = __fmul_rn(p00, w0); p01 = __fmul_rn(p01, w1);
-                    p10 = __fmul_rn(p10, w0); p11 = __fmul_rn(p11, w1);
-                }
-                float val, c;
-                if (EXACT) {
-                    const float t0 = __fadd_rn(p00, __fmul_rn(fx, __fsub_rn(p01, p00)));
-                    const float t1 = __fadd_rn(p10, __fmul_rn(fx, __fsub_rn(p11, p10)));
-                    val = __fadd_rn(t0, __fmul_rn(fy, __fsub_rn(t1, t0)));
-                    c = __fadd_rn(w0, __fmul_rn(fx, __fsub_rn(w1, w0)));
-                    sum[k] = __fadd_rn(sum[k], val);
-                    cnt[k] = __fadd_rn(cnt[k], c);
-                } else {
-                    const float t0 = fmaf(fx, p01 - p00, p00);
-                    const float t1 = fmaf(fx, p11 - p10, p10);
-                    val = fmaf(fy, t1 - t0, t0);
-                    c = fmaf(fx, w1 - w0, w0);
-                    sum[k] += val;
-                    cnt[k] += c;
-                }
-            }
+            if (in) acc[k] = padd(acc[k], f2(val, c));
         }
     }
 
@@ -136,15 +170,37 @@ __global__ void __launch_bounds__(256) bp_kernel(BPParams p) {
         if (zb + k >= p.z_end) break;
         const size_t idx = (size_t)(zb + k) * plane + base;
         if (FINALIZE) {
-            float o = __fdiv_rn(sum[k], cnt[k]);   // BPCore::DoneSlice
+            float o = __fdiv_rn(acc[k].x, acc[k].y);   // BPCore::DoneSlice
             if (p.apply_ct) o = ct_number(o, p.ct_scale, p.ct_norm1);
             if (p.out) p.out[idx] = o;
             if (p.out16) p.out16[idx] = to_i16(o);
         } else {
-            p.sum[idx] = sum[k];
-            p.cnt[idx] = cnt[k];
+            p.sum[idx] = acc[k].x;
+            p.cnt[idx] = acc[k].y;
         }
     }
+}
+
+// Filtered frames -> tapered quads.  One thread per (row, column) of a frame:
+// (w[c] p[r][c], w[c] p[r+1][c], w[c+1] p[r][c+1], w[c+1] p[r+1][c+1]), the
+// products rounded as InitView's in-place multiply (BPCore.cpp:147-151).
+__global__ void __launch_bounds__(256) pack_quads_kernel(const float* __restrict__ plain, long long plain_frame,
+                                                         int rows, int U, const float2* __restrict__ tw,
+                                                         int view0, int num_views, int apply_taper,
+                                                         float4* __restrict__ q4, long long q4_frame, int slot0) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y, f = blockIdx.z;
+    if (c >= U) return;
+    const float* s = plain + (size_t)f * plain_frame + (size_t)r * U + c;
+    const bool right = c + 1 < U, down = r + 1 < rows;
+    float p00 = s[0], p01 = right ? s[1] : 0.0f;
+    float p10 = down ? s[U] : 0.0f, p11 = (right && down) ? s[U + 1] : 0.0f;
+    if (apply_taper) {
+        const float2 w = tw[(size_t)((view0 + f) % num_views) * U + c];
+        p00 = __fmul_rn(p00, w.x); p10 = __fmul_rn(p10, w.x);
+        p01 = __fmul_rn(p01, w.y); p11 = __fmul_rn(p11, w.y);
+    }
+    q4[(size_t)(slot0 + f) * q4_frame + (size_t)r * U + c] = make_float4(p00, p10, p01, p11);
 }
 
 __global__ void finalize_kernel(const float* __restrict__ sum, const float* __restrict__ cnt, size_t n,
@@ -183,24 +239,42 @@ __global__ void zfilter_kernel(float* frames, int nv, int rows, int width, long 
     }
 }
 
-template <int ZPT, bool F, bool T, bool E>
+template <int ZPT, bool F, bool E, bool WZ>
 cudaError_t go(const BPParams& p, cudaStream_t s) {
     const int nz = p.z_end - p.z_begin;
     dim3 grid((p.X + 31) / 32, (p.Y + 7) / 8, (nz + ZPT - 1) / ZPT);
-    bp_kernel<ZPT, F, T, E><<<grid, dim3(32, 8), 0, s>>>(p);
+    bp_kernel<ZPT, F, E, WZ><<<grid, dim3(32, 8), 0, s>>>(p);
     return cudaGetLastError();
+}
+
+template <int ZPT, bool F, bool E>
+cudaError_t go2(const BPParams& p, bool wz, cudaStream_t s) {
+    return wz ? go<ZPT, F, E, true>(p, s) : go<ZPT, F, E, false>(p, s);
+}
+
+template <bool F, bool E>
+cudaError_t go3(const BPParams& p, bool wz, int zpt, cudaStream_t s) {
+    switch (zpt) {
+        case 16: return go2<16, F, E>(p, wz, s);
+        case 8: return go2<8, F, E>(p, wz, s);
+        default: return go2<4, F, E>(p, wz, s);
+    }
 }
 
 }  // namespace
 
-cudaError_t launch_bp(const BPParams& p, bool finalize, bool tapered, bool exact, cudaStream_t s) {
-    constexpr int Z = 8;
-    if (finalize) {
-        if (tapered) return exact ? go<Z, true, true, true>(p, s) : go<Z, true, true, false>(p, s);
-        return exact ? go<Z, true, false, true>(p, s) : go<Z, true, false, false>(p, s);
-    }
-    if (tapered) return exact ? go<Z, false, true, true>(p, s) : go<Z, false, true, false>(p, s);
-    return exact ? go<Z, false, false, true>(p, s) : go<Z, false, false, false>(p, s);
+cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, cudaStream_t s) {
+    if (finalize) return exact ? go3<true, true>(p, w_depends_on_z, zpt, s) : go3<true, false>(p, w_depends_on_z, zpt, s);
+    return exact ? go3<false, true>(p, w_depends_on_z, zpt, s) : go3<false, false>(p, w_depends_on_z, zpt, s);
+}
+
+cudaError_t launch_pack_quads(const float* plain, long long plain_frame, int nv, int rows, int U, const float2* tw,
+                              int view0, int num_views, int apply_taper, float4* q4, long long q4_frame, int slot0,
+                              cudaStream_t s) {
+    dim3 grid((U + 255) / 256, rows, nv);
+    pack_quads_kernel<<<grid, 256, 0, s>>>(plain, plain_frame, rows, U, tw, view0, num_views, apply_taper, q4,
+                                           q4_frame, slot0);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_finalize(const float* sum, const float* cnt, size_t n, int apply_ct, float ct_scale,

@@ -61,7 +61,7 @@ void dev_free(T*& p) {
 }
 
 int a_pitch(const jfdk_ctx* c) { return (int)round_up(c->in_w, 16); }
-long long q_frame(const jfdk_ctx* c) { return (long long)(c->rows + 1) * c->q_pitch; }
+long long frame_px(const jfdk_ctx* c) { return (long long)c->rows * c->out_w; }
 
 jfdk_status ensure_A(jfdk_ctx* c, size_t rows) {
     if (c->a_rows >= rows) return JFDK_OK;
@@ -76,15 +76,23 @@ jfdk_status ensure_A(jfdk_ctx* c, size_t rows) {
     return JFDK_OK;
 }
 
-jfdk_status ensure_Q(jfdk_ctx* c, int views) {
-    if (c->q_views >= views) return JFDK_OK;
-    dev_free(c->d_q);
-    c->q_views = 0;
-    const size_t n = (size_t)views * q_frame(c);
-    jfdk_status st = dev_alloc(c, &c->d_q, n, "the filtered projection store");
+jfdk_status ensure_plain(jfdk_ctx* c, int views) {
+    if (c->plain_views >= views) return JFDK_OK;
+    dev_free(c->d_plain);
+    c->plain_views = 0;
+    jfdk_status st = dev_alloc(c, &c->d_plain, (size_t)views * frame_px(c), "the filtered frames");
     if (st) return st;
-    JFDK_CUDA(c, cudaMemsetAsync(c->d_q, 0, n * sizeof(float), c->stream), "clearing the projection store");
-    c->q_views = views;
+    c->plain_views = views;
+    return JFDK_OK;
+}
+
+jfdk_status ensure_Q4(jfdk_ctx* c, int views) {
+    if (c->q4_views >= views) return JFDK_OK;
+    dev_free(c->d_q4);
+    c->q4_views = 0;
+    jfdk_status st = dev_alloc(c, &c->d_q4, (size_t)views * frame_px(c), "the backprojection quad store");
+    if (st) return st;
+    c->q4_views = views;
     return JFDK_OK;
 }
 
@@ -127,19 +135,27 @@ PrepParams prep_params(const jfdk_ctx* c, const uint16_t* raw) {
 
 BPParams bp_params(const jfdk_ctx* c) {
     BPParams b{};
-    b.q = c->d_q;
-    b.uw = c->d_uw;
+    b.q4 = c->d_q4;
+    b.tw = c->d_tw;
     b.ptm = c->d_ptm;
-    b.frame_stride = q_frame(c);
+    b.q4_frame = frame_px(c);
     b.U = c->out_w;
     b.V = c->rows;
-    b.pitch = c->q_pitch;
     b.X = c->X; b.Y = c->Y; b.Z = c->Z;
     b.pxy = c->pxy; b.pz = c->pz;
     b.z_begin = 0; b.z_end = c->Z;
     b.ct_scale = c->ct_scale;
     b.ct_norm1 = c->recon.ct_norm1;
     return b;
+}
+
+RampParams ramp_params(const jfdk_ctx* c, int nv, float* out) {
+    RampParams r{};
+    r.A = c->d_A; r.e = c->d_e; r.B = c->d_T; r.c = c->d_c;
+    r.M = nv * c->rows; r.N = c->out_w; r.K = c->in_w; r.a_pitch = a_pitch(c);
+    r.rows = c->rows;
+    r.q = out; r.q_frame_stride = frame_px(c); r.q_pitch = c->out_w;
+    return r;
 }
 
 }  // namespace
@@ -176,8 +192,9 @@ long long jfdk_kernel_launches(const jfdk_ctx* c) { return c ? c->launches : 0; 
 void jfdk_destroy(jfdk_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    dev_free(c->d_ptm); dev_free(c->d_uw); dev_free(c->d_tinv); dev_free(c->d_dmin);
-    dev_free(c->d_T); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_q);
+    dev_free(c->d_ptm); dev_free(c->d_tw); dev_free(c->d_tinv); dev_free(c->d_dmin);
+    dev_free(c->d_T); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_plain);
+    dev_free(c->d_q4);
     dev_free(c->d_sum); dev_free(c->d_cnt); dev_free(c->d_raw_stage); dev_free(c->d_hu_stage);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
@@ -228,10 +245,11 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
         const float det_at_iso = scan->detector_pixel_size / scan->dsd * scan->dso;
         c->hsr = 0.5f * (1.0f / det_at_iso);
     }
-    c->q_pitch = (int)round_up(c->out_w + 1, 4);
     c->groups = (c->nviews + 8) / 9;
     c->ct_scale = recon->ct_norm0 * 1000.f / recon->mu_water;  // CTNumCore.cpp:24
     c->ptms.assign(h_ptms, h_ptms + (size_t)c->nviews * 12);
+    for (int v = 0; v < c->nviews; ++v)
+        if (c->ptms[(size_t)v * 12 + 10] != 0.0f) c->w_depends_on_z = true;
 
     int dev = 0;
     JFDK_CUDA(c, cudaGetDevice(&dev), "cudaGetDevice");
@@ -251,19 +269,22 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     // device constants
     jfdk_status st;
     if ((st = dev_alloc(c, &c->d_ptm, (size_t)c->nviews * 12, "the projection matrices"))) return bail(st);
-    if ((st = dev_alloc(c, &c->d_uw, (size_t)c->nviews * c->q_pitch, "the u-tapers"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_tw, (size_t)c->nviews * c->out_w, "the u-taper pairs"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_tinv, (size_t)c->groups * 16, "the inverse transforms"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_dmin, (size_t)c->groups, "the pre-weight minima"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_T, (size_t)c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_c, (size_t)c->out_w, "the edge response"))) return bail(st);
-    std::vector<float> uwp((size_t)c->nviews * c->q_pitch, 0.0f);
+    std::vector<float2> twp((size_t)c->nviews * c->out_w);
     for (int v = 0; v < c->nviews; ++v)
-        std::memcpy(&uwp[(size_t)v * c->q_pitch], &c->ops.uw[(size_t)v * c->out_w], sizeof(float) * c->out_w);
+        for (int i = 0; i < c->out_w; ++i) {
+            const float* w = &c->ops.uw[(size_t)v * c->out_w];
+            twp[(size_t)v * c->out_w + i] = make_float2(w[i], i + 1 < c->out_w ? w[i + 1] : 0.0f);
+        }
     std::vector<float> Tp((size_t)c->out_w * a_pitch(c), 0.0f);
     for (int j = 0; j < c->out_w; ++j)
         std::memcpy(&Tp[(size_t)j * a_pitch(c)], &c->ops.T[(size_t)j * c->in_w], sizeof(float) * c->in_w);
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_ptm, h_ptms, sizeof(float) * c->nviews * 12, cudaMemcpyHostToDevice, c->stream), "upload");
-    JFDK_CUDA(c, cudaMemcpyAsync(c->d_uw, uwp.data(), sizeof(float) * uwp.size(), cudaMemcpyHostToDevice, c->stream), "upload");
+    JFDK_CUDA(c, cudaMemcpyAsync(c->d_tw, twp.data(), sizeof(float2) * twp.size(), cudaMemcpyHostToDevice, c->stream), "upload");
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_tinv, c->ops.tinv.data(), sizeof(float) * c->ops.tinv.size(), cudaMemcpyHostToDevice, c->stream), "upload");
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_T, Tp.data(), sizeof(float) * Tp.size(), cudaMemcpyHostToDevice, c->stream), "upload");
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_c, c->ops.c.data(), sizeof(float) * c->out_w, cudaMemcpyHostToDevice, c->stream), "upload");
@@ -281,6 +302,10 @@ jfdk_status jfdk_set_option(jfdk_ctx* c, int key, long long value) {
         case JFDK_OPT_VIEW_CHUNK:
             if (value < 1 || value > 4096) return fail(c, JFDK_ERR_INVALID, "view chunk out of range");
             c->opt_view_chunk = (int)value;
+            return JFDK_OK;
+        case JFDK_OPT_BP_ZPT:
+            if (value != 4 && value != 8 && value != 16) return fail(c, JFDK_ERR_INVALID, "slices per thread must be 4, 8 or 16");
+            c->opt_bp_zpt = (int)value;
             return JFDK_OK;
         case JFDK_OPT_STAGE_TIMING:
             if (value && !c->ev[0])
@@ -341,13 +366,7 @@ jfdk_status jfdk_filter_frames(jfdk_ctx* c, const float* d_in, int v0, int nv, f
     if (st) return st;
     JFDK_LAUNCH(c, launch_weight(d_in, nv, v0, c->in_w, c->rows, weight_params(c), c->d_A, a_pitch(c), c->d_e, c->stream),
                 "pre-weight");
-    RampParams r{};
-    r.A = c->d_A; r.e = c->d_e; r.B = c->d_T; r.c = c->d_c;
-    r.M = nv * c->rows; r.N = c->out_w; r.K = c->in_w; r.a_pitch = a_pitch(c);
-    r.rows = c->rows; r.view_base = v0; r.store_base = 0;
-    r.uw = nullptr; r.uw_pitch = c->q_pitch;
-    r.q = d_out; r.q_frame_stride = (long long)c->rows * c->out_w; r.q_pitch = c->out_w;
-    JFDK_LAUNCH(c, launch_ramp_gemm(r, c->stream), "ramp filter");
+    JFDK_LAUNCH(c, launch_ramp_gemm(ramp_params(c, nv, d_out), c->stream), "ramp filter");
     return JFDK_OK;
 }
 
@@ -375,21 +394,16 @@ jfdk_status jfdk_bp_accumulate(jfdk_ctx* c, const float* d_proj, int v0, int nv)
         return fail(c, JFDK_ERR_INVALID, "bp_accumulate: bad argument");
     if (!c->d_sum) return fail(c, JFDK_ERR_STATE, "bp_accumulate before bp_reset");
     if (nv == 0) return JFDK_OK;
-    jfdk_status st = ensure_Q(c, nv);
+    jfdk_status st = ensure_Q4(c, nv);
     if (st) return st;
-    // copy into the padded store (pad column and row stay zero)
-    JFDK_CUDA(c, cudaMemcpy2DAsync(c->d_q, sizeof(float) * c->q_pitch, d_proj, sizeof(float) * c->out_w,
-                                   sizeof(float) * c->out_w, c->rows, cudaMemcpyDeviceToDevice, c->stream),
-              "staging projections");
-    for (int i = 1; i < nv; ++i)
-        JFDK_CUDA(c, cudaMemcpy2DAsync(c->d_q + (size_t)i * q_frame(c), sizeof(float) * c->q_pitch,
-                                       d_proj + (size_t)i * c->rows * c->out_w, sizeof(float) * c->out_w,
-                                       sizeof(float) * c->out_w, c->rows, cudaMemcpyDeviceToDevice, c->stream),
-                  "staging projections");
+    // InitView: taper the caller's frames while packing them into quads
+    JFDK_LAUNCH(c, launch_pack_quads(d_proj, frame_px(c), nv, c->rows, c->out_w, c->d_tw, v0, c->nviews, 1, c->d_q4,
+                                     frame_px(c), 0, c->stream),
+                "packing projections");
     BPParams b = bp_params(c);
     b.view_base = v0; b.v0 = v0; b.nv = nv;
     b.sum = c->d_sum; b.cnt = c->d_cnt; b.load_acc = 1;
-    JFDK_LAUNCH(c, launch_bp(b, false, false, c->opt_bp_exact != 0, c->stream), "backprojection");
+    JFDK_LAUNCH(c, launch_bp(b, false, c->opt_bp_exact != 0, c->w_depends_on_z, c->opt_bp_zpt, c->stream), "backprojection");
     return JFDK_OK;
 }
 
@@ -415,36 +429,35 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, in
     if (!c || !d_raw || (!d_hu && !d_hu16)) return fail(c, JFDK_ERR_INVALID, "reconstruct: bad argument");
     if (c->in_w != c->used_u)
         return fail(c, JFDK_ERR_UNSUPPORTED, "reconstruct: conjugate-view compositing (filter width != frame width)");
-    jfdk_status st = ensure_Q(c, c->nviews);
+    jfdk_status st = ensure_Q4(c, c->nviews);
     if (st) return st;
     const int chunk = std::min(c->opt_view_chunk, c->nviews);
     if ((st = ensure_A(c, (size_t)chunk * c->rows))) return st;
+    if ((st = ensure_plain(c, chunk))) return st;
     const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;
-    const bool zf = c->recon.z_filter != 0;
     const bool timing = c->opt_stage_timing != 0;
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[0], c->stream), "event");
+    // per chunk of views: raw -> weighted rows -> filtered frames (L2-sized
+    // buffers) -> [z-filter] -> tapered quads of the whole rotation
     for (int v0 = 0; v0 < c->nviews; v0 += chunk) {
         const int nv = std::min(chunk, c->nviews - v0);
         JFDK_LAUNCH(c, launch_prep_weight(prep_params(c, d_raw + (size_t)v0 * frame), nv, v0, weight_params(c), c->d_A,
                                           a_pitch(c), c->d_e, c->stream),
                     "preprocess + pre-weight");
-        RampParams r{};
-        r.A = c->d_A; r.e = c->d_e; r.B = c->d_T; r.c = c->d_c;
-        r.M = nv * c->rows; r.N = c->out_w; r.K = c->in_w; r.a_pitch = a_pitch(c);
-        r.rows = c->rows; r.view_base = v0; r.store_base = v0;
-        r.uw = zf ? nullptr : c->d_uw; r.uw_pitch = c->q_pitch;
-        r.q = c->d_q; r.q_frame_stride = q_frame(c); r.q_pitch = c->q_pitch;
-        JFDK_LAUNCH(c, launch_ramp_gemm(r, c->stream), "ramp filter");
+        JFDK_LAUNCH(c, launch_ramp_gemm(ramp_params(c, nv, c->d_plain), c->stream), "ramp filter");
+        if (c->recon.z_filter)
+            JFDK_LAUNCH(c, launch_zfilter(c->d_plain, nv, c->rows, c->out_w, frame_px(c), c->out_w, c->stream),
+                        "z-filter");
+        JFDK_LAUNCH(c, launch_pack_quads(c->d_plain, frame_px(c), nv, c->rows, c->out_w, c->d_tw, v0, c->nviews, 1,
+                                         c->d_q4, frame_px(c), v0, c->stream),
+                    "packing projections");
     }
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[1], c->stream), "event");
-    if (zf)
-        JFDK_LAUNCH(c, launch_zfilter(c->d_q, c->nviews, c->rows, c->out_w, q_frame(c), c->q_pitch, c->stream),
-                    "z-filter");
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[2], c->stream), "event");
     BPParams b = bp_params(c);
     b.view_base = 0; b.v0 = 0; b.nv = c->nviews;
     b.out = d_hu; b.out16 = d_hu16; b.apply_ct = 1;
-    JFDK_LAUNCH(c, launch_bp(b, true, !zf, c->opt_bp_exact != 0, c->stream), "backprojection");
+    JFDK_LAUNCH(c, launch_bp(b, true, c->opt_bp_exact != 0, c->w_depends_on_z, c->opt_bp_zpt, c->stream), "backprojection");
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[3], c->stream), "event");
     return JFDK_OK;
 }

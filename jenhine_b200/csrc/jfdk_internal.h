@@ -31,17 +31,15 @@ std::string build_host_operators(const jfdk_scan_params& scan, const jfdk_recon_
                                  int in_w, int out_w, int rows, int mirror, float hsr,
                                  HostOperators& ops);
 
-// Parameters of the backprojection kernels (bp.cu).
+// Parameters of the backprojection kernel (bp.cu).
 struct BPParams {
-    const float* q;          // filtered projections, [views][rows + 1][pitch] float
-    const __half* qh;        // same in FP16 (mixed precision), or null
-    const float* qscale;     // [views] dequantisation scale (mixed precision)
-    const float* uw;         // [views][pitch] u-taper (zero padded)
+    const float4* q4;        // quads, [slots][rows][U]: (p[r][c], p[r+1][c], p[r][c+1], p[r+1][c+1])
+    const float2* tw;        // [views][U] taper pairs (w[c], w[c+1]), w[U] = 0
     const float* ptm;        // [views][12]
-    long long frame_stride;  // elements between views in q / qh
-    int view_base;           // index of q's first frame in the rotation
+    long long q4_frame;      // quads per slot (rows * U)
+    int view_base;           // rotation index held by slot 0
     int v0, nv;              // views to accumulate (rotation indices)
-    int U, V, pitch;         // columns, rows, row pitch of q
+    int U, V;                // columns, rows
     int X, Y, Z;
     float pxy, pz;
     int z_begin, z_end;      // slices handled by this launch
@@ -55,8 +53,13 @@ struct BPParams {
 };
 
 // Launchers (return cudaError_t of the launch).
-cudaError_t launch_bp(const BPParams& p, bool finalize, bool tapered, bool exact,
-                      cudaStream_t s);
+// zpt: slices per thread (4, 8 or 16).
+cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, cudaStream_t s);
+// Filtered frames [nv][rows][U] -> quads in slots [slot0, slot0 + nv), tapered
+// with the taper of rotation view (view0 + f) when apply_taper.
+cudaError_t launch_pack_quads(const float* plain, long long plain_frame, int nv, int rows, int U, const float2* tw,
+                              int view0, int num_views, int apply_taper, float4* q4, long long q4_frame, int slot0,
+                              cudaStream_t s);
 cudaError_t launch_finalize(const float* sum, const float* cnt, size_t n, int apply_ct,
                             float ct_scale, float norm1, float* out, int16_t* out16,
                             cudaStream_t s);
@@ -97,11 +100,7 @@ struct RampParams {
     const float* c;          // [N]
     int M, N, K, a_pitch;
     int rows;                // rows per view (M = nv * rows)
-    int view_base;           // rotation index of A's first view
-    int store_base;          // index of A's first view in the output store
-    const float* uw;         // [views][uw_pitch] taper or null (agent path)
-    int uw_pitch;
-    float* q;                // output, [..][rows + pad][q_pitch]
+    float* q;                // output frames, row r of view f at q + f * q_frame_stride + r * q_pitch
     long long q_frame_stride;
     int q_pitch;
 };
@@ -129,25 +128,26 @@ struct jfdk_ctx {
     float hsr = 0.f;
     int X = 0, Y = 0, Z = 0;
     float pxy = 0.f, pz = 0.f;
-    int q_pitch = 0;              // filtered store row pitch (floats), >= out_w + 1
     int groups = 0;
     float ct_scale = 0.f;
 
     std::vector<float> ptms;
     jfdk::HostOperators ops;
+    bool w_depends_on_z = false;  // some view has P[10] != 0
 
     // device constants
     float* d_ptm = nullptr;
-    float* d_uw = nullptr;       // [views][q_pitch]
+    float2* d_tw = nullptr;      // [views][out_w] taper pairs
     float* d_tinv = nullptr;
     float* d_dmin = nullptr;
     float* d_T = nullptr;
     float* d_c = nullptr;
 
     // device working storage (allocated on demand)
-    float* d_A = nullptr;  size_t a_rows = 0;   // weighted rows, pitch in_w
+    float* d_A = nullptr;  size_t a_rows = 0;   // weighted rows, pitch a_pitch
     float* d_e = nullptr;
-    float* d_q = nullptr;  int q_views = 0;     // filtered store
+    float* d_plain = nullptr; int plain_views = 0;  // filtered frames of one chunk
+    float4* d_q4 = nullptr; int q4_views = 0;       // quad store
     float* d_sum = nullptr;
     float* d_cnt = nullptr;
     uint16_t* d_raw_stage = nullptr; size_t raw_stage_bytes = 0;
@@ -158,6 +158,7 @@ struct jfdk_ctx {
     int opt_bp_exact = 0;
     int opt_view_chunk = 32;
     int opt_stage_timing = 0;
+    int opt_bp_zpt = 4;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
     long long launches = 0;

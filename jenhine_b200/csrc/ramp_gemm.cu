@@ -11,9 +11,8 @@
 //     c[j]      = sum_k ramp_k * h[(off + j - pos_k) mod L],
 //
 // so the whole projection set is Q = A * T^T + e c^T with M = views * rows,
-// N = W_out, K = W.  The epilogue adds the rank-1 edge term and multiplies by
-// the BP u-taper of the row's view (BPAgent/BPCore.cpp:147-151), writing the
-// padded filtered-projection store the backprojector reads.
+// N = W_out, K = W.  The epilogue adds the rank-1 edge term and stores the
+// filtered rows (the backprojector's packer applies the u-taper).
 //
 // This file holds the FP32 CUDA-core (SIMT) form: 128 x 128 output tile per
 // CTA, K staged through shared memory in steps of 16, 8 x 8 outputs per
@@ -70,22 +69,19 @@ __global__ void __launch_bounds__(256) ramp_gemm_simt_kernel(RampParams p) {
                 for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(xa[i], yb[j], acc[i][j]);
         }
     }
-    // epilogue: + c[n] e[m], x taper, store into the padded projection store
+    // epilogue: + c[n] e[m] (the truncation ramp), store the filtered rows
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int m = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
         if (m >= p.M) continue;
         const int vl = m / p.rows, row = m - vl * p.rows;
         const float em = p.e[m];
-        const float* w = p.uw ? p.uw + (size_t)(p.view_base + vl) * p.uw_pitch : nullptr;
-        float* q = p.q + (size_t)(p.store_base + vl) * p.q_frame_stride + (size_t)row * p.q_pitch;
+        float* q = p.q + (size_t)vl * p.q_frame_stride + (size_t)row * p.q_pitch;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const int n = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4);
             if (n >= p.N) continue;
-            float o = fmaf(p.c[n], em, acc[i][j]);
-            if (w) o = __fmul_rn(o, w[n]);
-            q[n] = o;
+            q[n] = fmaf(p.c[n], em, acc[i][j]);
         }
     }
 }
