@@ -72,6 +72,7 @@ _SIGS = {
     "jfdk_stage_times": ([_P, _P], C.c_int),
     "jfdk_preprocess_frames": ([_P, _P, C.c_int, _P], C.c_int),
     "jfdk_filter_frames": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
+    "jfdk_filter_frames_noalloc": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
     "jfdk_zfilter_frames": ([_P, _P, C.c_int], C.c_int),
     "jfdk_bp_reset": ([_P], C.c_int),
     "jfdk_bp_accumulate": ([_P, _P, C.c_int, C.c_int], C.c_int),

@@ -194,6 +194,17 @@ class FDKEngine:
         self._check(self.lib.jfdk_filter_frames(self.ctx, _ptr(frames), v0, nv, _ptr(out)))
         return out
 
+    def filter_noalloc(self, frames, v0: int = 0, out=None):
+        """``filter`` through jfdk_filter_frames_noalloc: working rows in the
+        library's fixed 4 MiB device array, no allocation by the library (out
+        must be given by callers that cannot allocate)."""
+        import torch
+        nv = frames.shape[0]
+        out = out if out is not None else torch.empty((nv, self.rows, self.filter_out_w), dtype=torch.float32,
+                                                      device=frames.device)
+        self._check(self.lib.jfdk_filter_frames_noalloc(self.ctx, _ptr(frames), v0, nv, _ptr(out)))
+        return out
+
     def zfilter(self, frames):
         self._check(self.lib.jfdk_zfilter_frames(self.ctx, _ptr(frames), frames.shape[0]))
         return frames
