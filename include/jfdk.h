@@ -182,8 +182,10 @@ enum {
                                  jfdk_reconstruct (default 32)                   */
     JFDK_OPT_STAGE_TIMING = 3,/* 1: jfdk_reconstruct records CUDA events on its
                                  stream around each stage                        */
-    JFDK_OPT_BP_ZPT = 4       /* slices each backprojection thread keeps in
+    JFDK_OPT_BP_ZPT = 4,      /* slices each backprojection thread keeps in
                                  registers: 4 (default), 8 or 16                 */
+    JFDK_OPT_FILTER_SIMT = 5  /* 1: ramp product on FP32 CUDA cores; 0 (default):
+                                 tcgen05 tensor cores, 3xTF32 split              */
 };
 jfdk_status jfdk_set_option(jfdk_ctx* ctx, int key, long long value);
 /* Stage times (ms) of the last jfdk_reconstruct with JFDK_OPT_STAGE_TIMING:
@@ -202,6 +204,9 @@ jfdk_status jfdk_get_uweights(const jfdk_ctx* ctx, float* h_out);
 jfdk_status jfdk_get_ramp_operator(const jfdk_ctx* ctx, float* h_T, float* h_c);
 /* Number of kernels this context has launched (a counter, for benchmarks). */
 long long jfdk_kernel_launches(const jfdk_ctx* ctx);
+
+/* jfdk_sync also reports JFDK_ERR_CUDA when a kernel's bounded wait gave up
+ * (the device status word is then cleared). */
 
 /* Library build / device check: 0 when an sm_100 device is current. */
 jfdk_status jfdk_device_check(char* msg, int msg_len);

@@ -26,6 +26,7 @@ OPT_BP_EXACT = 1
 OPT_VIEW_CHUNK = 2
 OPT_STAGE_TIMING = 3
 OPT_BP_ZPT = 4
+OPT_FILTER_SIMT = 5
 
 
 class ScanParams(C.Structure):

@@ -60,7 +60,7 @@ void dev_free(T*& p) {
     p = nullptr;
 }
 
-int a_pitch(const jfdk_ctx* c) { return (int)round_up(c->in_w, 16); }
+int a_pitch(const jfdk_ctx* c) { return (int)round_up(c->in_w, 32); }
 long long frame_px(const jfdk_ctx* c) { return (long long)c->rows * c->out_w; }
 
 jfdk_status ensure_A(jfdk_ctx* c, size_t rows) {
@@ -149,6 +149,11 @@ BPParams bp_params(const jfdk_ctx* c) {
     return b;
 }
 
+cudaError_t launch_ramp(jfdk_ctx* c, const RampParams& r) {
+    if (c->opt_filter_simt) return launch_ramp_gemm(r, c->stream);
+    return launch_ramp_gemm_tc(r, c->d_Th, c->d_Tl, c->d_status, c->stream);
+}
+
 RampParams ramp_params(const jfdk_ctx* c, int nv, float* out) {
     RampParams r{};
     r.A = c->d_A; r.e = c->d_e; r.B = c->d_T; r.c = c->d_c;
@@ -193,7 +198,7 @@ void jfdk_destroy(jfdk_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     dev_free(c->d_ptm); dev_free(c->d_tw); dev_free(c->d_tinv); dev_free(c->d_dmin);
-    dev_free(c->d_T); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_plain);
+    dev_free(c->d_T); dev_free(c->d_Th); dev_free(c->d_Tl); dev_free(c->d_status); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_plain);
     dev_free(c->d_q4);
     dev_free(c->d_sum); dev_free(c->d_cnt); dev_free(c->d_raw_stage); dev_free(c->d_hu_stage);
     for (auto& e : c->ev)
@@ -273,7 +278,11 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     if ((st = dev_alloc(c, &c->d_tinv, (size_t)c->groups * 16, "the inverse transforms"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_dmin, (size_t)c->groups, "the pre-weight minima"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_T, (size_t)c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_Th, (size_t)c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_Tl, (size_t)c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_c, (size_t)c->out_w, "the edge response"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_status, 1, "the status word"))) return bail(st);
+    JFDK_CUDA(c, cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream), "clearing the status word");
     std::vector<float2> twp((size_t)c->nviews * c->out_w);
     for (int v = 0; v < c->nviews; ++v)
         for (int i = 0; i < c->out_w; ++i) {
@@ -287,6 +296,16 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_tw, twp.data(), sizeof(float2) * twp.size(), cudaMemcpyHostToDevice, c->stream), "upload");
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_tinv, c->ops.tinv.data(), sizeof(float) * c->ops.tinv.size(), cudaMemcpyHostToDevice, c->stream), "upload");
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_T, Tp.data(), sizeof(float) * Tp.size(), cudaMemcpyHostToDevice, c->stream), "upload");
+    {   // TF32-exact split for the tensor-core product: T = Th + Tl + O(2^-22 T)
+        std::vector<float> th(Tp.size()), tl(Tp.size());
+        for (size_t i = 0; i < Tp.size(); ++i) {
+            th[i] = tf32_round_host(Tp[i]);
+            tl[i] = tf32_round_host(Tp[i] - th[i]);
+        }
+        JFDK_CUDA(c, cudaMemcpyAsync(c->d_Th, th.data(), sizeof(float) * th.size(), cudaMemcpyHostToDevice, c->stream), "upload");
+        JFDK_CUDA(c, cudaMemcpyAsync(c->d_Tl, tl.data(), sizeof(float) * tl.size(), cudaMemcpyHostToDevice, c->stream), "upload");
+        JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "upload");
+    }
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_c, c->ops.c.data(), sizeof(float) * c->out_w, cudaMemcpyHostToDevice, c->stream), "upload");
     JFDK_LAUNCH(c, launch_preweight_dmin(c->d_tinv, c->groups, c->rows, c->L, c->in_w, c->mirror, c->d_dmin, c->stream),
                 "pre-weight minimum");
@@ -307,6 +326,7 @@ jfdk_status jfdk_set_option(jfdk_ctx* c, int key, long long value) {
             if (value != 4 && value != 8 && value != 16) return fail(c, JFDK_ERR_INVALID, "slices per thread must be 4, 8 or 16");
             c->opt_bp_zpt = (int)value;
             return JFDK_OK;
+        case JFDK_OPT_FILTER_SIMT: c->opt_filter_simt = value ? 1 : 0; return JFDK_OK;
         case JFDK_OPT_STAGE_TIMING:
             if (value && !c->ev[0])
                 for (auto& e : c->ev) JFDK_CUDA(c, cudaEventCreate(&e), "cudaEventCreate");
@@ -327,6 +347,12 @@ jfdk_status jfdk_stage_times(jfdk_ctx* c, float* ms) {
 jfdk_status jfdk_sync(jfdk_ctx* c) {
     if (!c) return JFDK_ERR_INVALID;
     JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "stream synchronize");
+    int status = 0;
+    JFDK_CUDA(c, cudaMemcpy(&status, c->d_status, sizeof(int), cudaMemcpyDeviceToHost), "reading the status word");
+    if (status) {
+        cudaMemset(c->d_status, 0, sizeof(int));
+        return fail(c, JFDK_ERR_CUDA, "a tensor-core pipeline wait timed out; results of the last calls are invalid");
+    }
     return JFDK_OK;
 }
 
@@ -366,7 +392,7 @@ jfdk_status jfdk_filter_frames(jfdk_ctx* c, const float* d_in, int v0, int nv, f
     if (st) return st;
     JFDK_LAUNCH(c, launch_weight(d_in, nv, v0, c->in_w, c->rows, weight_params(c), c->d_A, a_pitch(c), c->d_e, c->stream),
                 "pre-weight");
-    JFDK_LAUNCH(c, launch_ramp_gemm(ramp_params(c, nv, d_out), c->stream), "ramp filter");
+    JFDK_LAUNCH(c, launch_ramp(c, ramp_params(c, nv, d_out)), "ramp filter");
     return JFDK_OK;
 }
 
@@ -444,7 +470,7 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, in
         JFDK_LAUNCH(c, launch_prep_weight(prep_params(c, d_raw + (size_t)v0 * frame), nv, v0, weight_params(c), c->d_A,
                                           a_pitch(c), c->d_e, c->stream),
                     "preprocess + pre-weight");
-        JFDK_LAUNCH(c, launch_ramp_gemm(ramp_params(c, nv, c->d_plain), c->stream), "ramp filter");
+        JFDK_LAUNCH(c, launch_ramp(c, ramp_params(c, nv, c->d_plain)), "ramp filter");
         if (c->recon.z_filter)
             JFDK_LAUNCH(c, launch_zfilter(c->d_plain, nv, c->rows, c->out_w, frame_px(c), c->out_w, c->stream),
                         "z-filter");

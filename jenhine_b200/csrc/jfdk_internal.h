@@ -105,6 +105,12 @@ struct RampParams {
     int q_pitch;
 };
 cudaError_t launch_ramp_gemm(const RampParams& p, cudaStream_t s);
+// Tensor-core form (ramp_gemm_tc.cu): B split into TF32-exact parts Bh, Bl
+// ([N][a_pitch]); a_pitch must be a multiple of 32.  A timed-out pipeline wait
+// sets *status (device word) and the CTA skips the rest of its work.
+cudaError_t launch_ramp_gemm_tc(const RampParams& p, const float* Bh, const float* Bl, int* status,
+                                cudaStream_t s);
+float tf32_round_host(float x);
 
 cudaError_t launch_zfilter(float* frames, int nv, int rows, int width, long long frame_stride,
                            int pitch, cudaStream_t s);
@@ -141,7 +147,10 @@ struct jfdk_ctx {
     float* d_tinv = nullptr;
     float* d_dmin = nullptr;
     float* d_T = nullptr;
+    float* d_Th = nullptr;       // TF32-exact split of the ramp operator
+    float* d_Tl = nullptr;
     float* d_c = nullptr;
+    int* d_status = nullptr;     // nonzero: a kernel's bounded wait gave up
 
     // device working storage (allocated on demand)
     float* d_A = nullptr;  size_t a_rows = 0;   // weighted rows, pitch a_pitch
@@ -159,6 +168,7 @@ struct jfdk_ctx {
     int opt_view_chunk = 32;
     int opt_stage_timing = 0;
     int opt_bp_zpt = 4;
+    int opt_filter_simt = 0;     // 1: ramp product on FP32 CUDA cores instead of tcgen05
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
     long long launches = 0;
