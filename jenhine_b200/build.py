@@ -26,13 +26,20 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE
 CU_FLAGS = ARCH + COMMON + ["--expt-relaxed-constexpr", "-Xptxas", "-O3"]
 
 
+HOST = os.path.join(PKG, "host")   # C++ Agent/Pipe layer over the C ABI
+
+
 def sources():
-    return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp")))
+    cs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp"))]
+    hs = [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".cpp")]
+    return sorted(cs) + sorted(hs)
 
 
 def headers():
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    return hs + [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
+    inc = [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
+    jeng = os.path.join(INCLUDE, "jengine")
+    return hs + inc + [os.path.join(jeng, f) for f in os.listdir(jeng) if f.endswith(".h")]
 
 
 def _run(cmd, verbose):

@@ -1,0 +1,116 @@
+// test_agents_gpu.cpp -- the reference's GPU agent chain on libjfdk.so:
+// Source -> PreProcessingAgent -> FilterAgent -> DeviceUploadAgent ->
+// BPCUDAAgent -> DeviceMemoryDownloadAgent -> CTNumAgent -> Sink
+// (the order of JEngine/JEngine.cpp:186-314 without compositing).
+//
+// usage: test_agents_gpu <case.bin> <out.bin>
+//   case.bin: int32 header [views, detU, detV, X, Y, Z], float32 [dso, hsr,
+//   bright, bhc0, bhc1, bhc2, pitchXY, pitchZ, norm0, norm1, cutStart,
+//   cutEnd, nAdj], nAdj adjust points, nAdj levels, views*12 PTM floats,
+//   views*detV*detU uint16 frames.  out.bin: Z*Y*X float32 HU.
+#include <cstdio>
+#include <fstream>
+#include <vector>
+
+#include "jengine/Agents.h"
+
+using namespace JEngine;
+
+class FrameSource : public SequentialAgentBase {
+public:
+    FrameSource(const std::vector<UINT16Vec>& frames, size_t w, size_t h, int shots)
+        : SequentialAgentBase("InputAgent", 1), frames(frames), w(w), h(h), shots(shots) {}
+
+private:
+    void SetPipesImpl() override {
+        out = CreateNewPipe<UINT16Vec>("Proj");
+        out->SetTemplate(UINT16Vec(w * h), {w, h});
+        out->SetProducer(GetAgentName(), 1, 1);
+        MergePipeToTrunk(out);
+    }
+    void WorkFlow0() override {
+        for (int s = 0; s < shots; ++s)
+            for (size_t i = 0; i < frames.size(); ++i)
+                out->GetWriteToken(1, i + 1 == frames.size()).GetBuffer(0) = frames[i];
+        out->Close();
+    }
+    const std::vector<UINT16Vec>& frames;
+    size_t w, h;
+    int shots;
+    std::shared_ptr<Pipe<UINT16Vec>> out;
+};
+
+class SliceSink : public SequentialAgentBase {
+public:
+    explicit SliceSink(size_t n) : SequentialAgentBase("OutputAgent", 1), n(n) {}
+    std::vector<FloatVec> slices;
+
+private:
+    void SetPipesImpl() override {
+        in = BranchPipeFromTrunk<FloatVec>("Slice");
+        in->SetConsumer(GetAgentName(), 1, 1, 0);
+    }
+    void WorkFlow0() override {
+        try {
+            while (true) slices.push_back(in->GetReadToken().GetBuffer(0));
+        } catch (PipeClosedAndEmptySignal&) {
+        }
+    }
+    size_t n;
+    std::shared_ptr<Pipe<FloatVec>> in;
+};
+
+int main(int argc, char** argv) {
+    if (argc < 3) return 2;
+    std::ifstream f(argv[1], std::ios::binary);
+    int hdr[6];
+    float prm[13];
+    f.read((char*)hdr, sizeof hdr);
+    f.read((char*)prm, sizeof prm);
+    const size_t V = hdr[0], U = hdr[1], H = hdr[2], X = hdr[3], Y = hdr[4], Z = hdr[5];
+    const int nAdj = (int)prm[12];
+    FloatVec adjP(nAdj), adjL(nAdj);
+    f.read((char*)adjP.data(), 4 * nAdj);
+    f.read((char*)adjL.data(), 4 * nAdj);
+    std::vector<ProjectionMatrix> ptms(V);
+    for (auto& p : ptms) f.read((char*)p.Data(), 48);
+    std::vector<UINT16Vec> frames(V, UINT16Vec(U * H));
+    for (auto& fr : frames) f.read((char*)fr.data(), 2 * U * H);
+    if (!f) return 3;
+
+    const int shots = 2;  // two scans back to back: the second must not see the first
+    std::vector<std::shared_ptr<AgentBase>> agents;
+    agents.push_back(std::make_shared<FrameSource>(frames, U, H, shots));
+    agents.push_back(std::make_shared<PreProcessingAgent>(2, 1, U, H, 0, 0, 0, 0, U, H, prm[2],
+                                                          FloatVec{prm[3], prm[4], prm[5]}));
+    agents.push_back(std::make_shared<FilterAgent>(2, 240, U, H, U, false, prm[1], prm[10], prm[11], adjP, adjL,
+                                                   ptms, prm[0]));
+    agents.push_back(std::make_shared<DeviceUploadAgent>("Proj", U, H));
+    agents.push_back(std::make_shared<BPCUDAAgent>(ptms, U, H, X, Y, Z, prm[6], prm[7], Z, 1, "", 7));
+    agents.push_back(std::make_shared<DeviceMemoryDownloadAgent>("Slice", X, Y));
+    agents.push_back(std::make_shared<CTNumAgent>(2, X, Y, prm[8], prm[9], 0.02f));
+    auto sink = std::make_shared<SliceSink>(Z);
+    agents.push_back(sink);
+
+    std::vector<std::shared_ptr<PipeBase>> trunk;
+    try {
+        for (auto& a : agents) a->SetPipes(trunk);
+        for (auto& a : agents) a->GetReady();
+        for (auto& a : agents) a->Start();
+        for (auto& a : agents) a->Join();
+    } catch (std::exception& e) {
+        std::printf("exception: %s\n", e.what());
+        return 4;
+    }
+    std::printf("slices received: %zu (expected %zu)\n", sink->slices.size(), shots * Z);
+    if (sink->slices.size() != shots * Z) return 5;
+    std::ofstream o(argv[2], std::ios::binary);
+    for (size_t s = (shots - 1) * Z; s < shots * Z; ++s) o.write((const char*)sink->slices[s].data(), 4 * X * Y);
+    // both scans identical -> identical volumes
+    for (size_t z = 0; z < Z; ++z)
+        if (sink->slices[z] != sink->slices[Z + z]) {
+            std::printf("scan 2 differs from scan 1 at slice %zu\n", z);
+            return 6;
+        }
+    return 0;
+}

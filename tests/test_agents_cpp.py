@@ -1,0 +1,66 @@
+"""The C++ Agent/Pipe layer (include/jengine, jenhine_b200/host).
+
+CPU: the runtime (pipes, tokens, agent bases) compiled on its own and run as a
+native test program.  GPU: the reference's agent chain on libjfdk.so, two
+identical scans back to back, against the reference cores' HU volume."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_golden, rel_l2
+
+CPP = os.path.join(ROOT, "tests", "cpp")
+
+
+def _build(out, sources, extra=()):
+    cmd = ["g++", "-std=c++17", "-O2", "-pthread", "-I", os.path.join(ROOT, "include")] + sources + ["-o", out]
+    cmd += list(extra)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]
+
+
+def test_pipeline_runtime_cpu(tmp_path):
+    exe = str(tmp_path / "test_pipeline")
+    host = os.path.join(ROOT, "jenhine_b200", "host")
+    _build(exe, [os.path.join(CPP, "test_pipeline.cpp"), os.path.join(host, "Pipe.cpp"),
+                 os.path.join(host, "Agent.cpp")])
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "OK (0 failures)" in r.stdout
+
+
+def _write_case(path, g):
+    raw = g["raw"]
+    V, H, U = raw.shape
+    X, Y, Z = (int(v) for v in g["vol"])
+    hdr = np.array([V, U, H, X, Y, Z], np.int32)
+    adj_p, adj_l = g["adj_pts"].astype(np.float32), g["adj_db"].astype(np.float32)
+    prm = np.array([g["dso"], g["hsr"], g["bright_field"], *g["bhc"], *g["pitch"], *g["norm"], *g["cut"],
+                    adj_p.size], np.float32)
+    with open(path, "wb") as f:
+        for a in (hdr, prm, adj_p, adj_l, g["ptms"].astype(np.float32), raw.astype(np.uint16)):
+            f.write(np.ascontiguousarray(a).tobytes())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["mini_c1", "mini_c2"])
+def test_agent_chain_gpu(tmp_path, name):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from jenhine_b200 import build
+    lib = build.build()
+    exe = str(tmp_path / "test_agents_gpu")
+    _build(exe, [os.path.join(CPP, "test_agents_gpu.cpp")],
+           ["-L", os.path.dirname(lib), "-ljfdk", f"-Wl,-rpath,{os.path.dirname(lib)}"])
+    g = load_golden(name)
+    case, out = str(tmp_path / "case.bin"), str(tmp_path / "out.bin")
+    _write_case(case, g)
+    r = subprocess.run([exe, case, out], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    X, Y, Z = (int(v) for v in g["vol"])
+    hu = np.fromfile(out, np.float32).reshape(Z, Y, X)
+    assert rel_l2(hu + 1000.0, g["hu"] + 1000.0) <= 1e-5
+    assert np.max(np.abs(hu - g["hu"])) < 0.5
