@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed"])
     ap.add_argument("--exact", action="store_true", help="BPCore-exact backprojection rounding")
+    ap.add_argument("--zpt", type=int, default=0, help="slices per backprojection thread (0: form default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -255,6 +256,8 @@ def main():
     ptms = w.geom.ptms()
     eng = FDKEngine(w.scan, w.recon, ptms, precision=a.precision, bp_exact=a.exact)
     eng.set_option(_lib.OPT_STAGE_TIMING, 1)
+    if a.zpt:
+        eng.set_option(_lib.OPT_BP_ZPT, a.zpt)
     r = w.recon
     vol = torch.empty((r.num_pixels_z, r.num_pixels_y, r.num_pixels_x), dtype=torch.float32, device="cuda")
     for _ in range(a.warmup):

@@ -175,15 +175,17 @@ jfdk_status jfdk_reconstruct_host(jfdk_ctx* ctx, const uint16_t* h_raw, float* h
 
 /* ---- options --------------------------------------------------------------- */
 enum {
-    JFDK_OPT_BP_EXACT = 1,    /* 1: backprojection rounds every step like BPCore
-                                 (IEEE division, no contraction); 0 (default):
-                                 one reciprocal per sample point, FMA lerps     */
+    JFDK_OPT_BP_EXACT = 1,    /* FP32 form.  1: backprojection rounds every
+                                 step like BPCore (bit-identical sums);
+                                 0 (default): the same sample coordinates
+                                 (correctly rounded quotients), lerps fused
+                                 into FMAs                                      */
     JFDK_OPT_VIEW_CHUNK = 2,  /* views preprocessed + filtered per launch in
                                  jfdk_reconstruct (default 32)                   */
     JFDK_OPT_STAGE_TIMING = 3,/* 1: jfdk_reconstruct records CUDA events on its
                                  stream around each stage                        */
     JFDK_OPT_BP_ZPT = 4,      /* slices each backprojection thread keeps in
-                                 registers: 4 (default), 8 or 16                 */
+                                 registers: 4, 8 or 16; 0 (default): 8         */
     JFDK_OPT_FILTER_SIMT = 5  /* 1: ramp product on FP32 CUDA cores; 0 (default):
                                  tcgen05 tensor cores, 3xTF32 split              */
 };

@@ -36,6 +36,7 @@
 // BPCore (every product and sum separately) instead of fusing them.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "jfdk_internal.h"
@@ -79,6 +80,7 @@ __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b
     }
 JFDK_PACKED_OP(pmul, "mul.rn.f32x2")
 JFDK_PACKED_OP(padd, "add.rn.f32x2")
+JFDK_PACKED_OP(psub, "sub.rn.f32x2")
 #undef JFDK_PACKED_OP
 
 // a * b + c per lane, one rounding (fma.rn.f32x2).
@@ -91,8 +93,30 @@ __device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) {
     return d;
 }
 
+// add.rm.f32x2: the lanewise sum rounded toward -infinity.
+__device__ __forceinline__ float2 padd_rm(float2 a, float2 b) {
+    float2 d;
+    asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+        " add.rm.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+// Floor without the conversion unit: for 0 <= x < 2^23 the sum 2^23 + x has
+// a unit in the last place of 1, so rounding it toward -infinity gives
+// 2^23 + floor(x) exactly; its bit pattern minus that of 2^23 is floor(x) as
+// an integer, and subtracting 2^23 back gives floor(x) as a float.
+constexpr float kMagic = 8388608.0f;   // 2^23
+constexpr int kMagicBits = 0x4B000000;  // bit pattern of 2^23
+
+// Resident CTAs per SM the compiler must allow for: 8 slices per thread fit
+// in 64 registers at 4 CTAs (32 warps) per SM, which measured faster than the
+// 80-register, 3-CTA allocation the compiler picks unconstrained.
+constexpr int bp_min_blocks(int zpt) { return zpt == 8 ? 4 : 1; }
+
 template <int ZPT, bool FINALIZE, bool EXACT, bool WZ>
-__global__ void __launch_bounds__(256) bp_kernel(BPParams p) {
+__global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_kernel(BPParams p) {
     const int x = blockIdx.x * 32 + threadIdx.x;
     const int y = blockIdx.y * 8 + threadIdx.y;
     const int zb = p.z_begin + blockIdx.z * ZPT;
@@ -110,22 +134,26 @@ __global__ void __launch_bounds__(256) bp_kernel(BPParams p) {
         const float a = __fmul_rn(__fadd_rn(-((float)p.Z - 1.0f) / 2.0f, (float)(zb + k)), p.pz);
         az[k] = a;
         const bool in = zb + k < p.z_end;
-        acc[k] = (p.load_acc && in) ? f2(p.sum[(size_t)(zb + k) * plane + base], p.cnt[(size_t)(zb + k) * plane + base])
-                                    : f2(0.0f, 0.0f);
+        acc[k] = (!FINALIZE && p.load_acc && in)
+                     ? f2(p.sum[(size_t)(zb + k) * plane + base], p.cnt[(size_t)(zb + k) * plane + base])
+                     : f2(0.0f, 0.0f);
     }
-    const float umax = (float)(p.U - 1), vmax = (float)(p.V - 1), fU = (float)p.U;
+    const float umax = (float)(p.U - 1), vmax = (float)(p.V - 1);
     const float2 neg1 = f2(-1.0f, -1.0f);
 
-    for (int view = p.v0; view < p.v0 + p.nv; ++view) {
-        const float4* P4 = reinterpret_cast<const float4*>(p.ptm + (size_t)view * 12);
+    // Pointers step from view to view (index arithmetic on v0 and view_base
+    // inside the loop measured over 10% slower at the 64-register bound).
+    const float4* P4 = reinterpret_cast<const float4*>(p.ptm + (size_t)p.v0 * 12);
+    const float4* __restrict__ q = p.q4 + (size_t)(p.v0 - p.view_base) * p.q4_frame;
+    const float2* __restrict__ tw = p.tw + (size_t)p.v0 * p.U;
+#pragma unroll 1
+    for (int n = 0; n < p.nv; ++n, P4 += 3, q += p.q4_frame, tw += p.U) {
         const float4 r0 = __ldg(P4), r1 = __ldg(P4 + 1), r2 = __ldg(P4 + 2);
         // (XxPM0 + (YxPM1 + PM3), XxPM4 + (YxPM5 + PM7)) and W (BPCore.cpp:120-145)
         const float Uxy = __fadd_rn(__fmul_rn(ax, r0.x), __fadd_rn(__fmul_rn(ay, r0.y), r0.w));
         const float Vxy = __fadd_rn(__fmul_rn(ax, r1.x), __fadd_rn(__fmul_rn(ay, r1.y), r1.w));
         const float Wxy = __fadd_rn(__fmul_rn(ax, r2.x), __fadd_rn(__fmul_rn(ay, r2.y), r2.w));
         const float rxy = WZ ? 0.0f : __frcp_rn(Wxy);
-        const float4* __restrict__ q = p.q4 + (size_t)(view - p.view_base) * p.q4_frame;
-        const float2* __restrict__ tw = p.tw + (size_t)view * p.U;
 #pragma unroll
         for (int k = 0; k < ZPT; ++k) {
             const float2 UV = f2(__fadd_rn(Uxy, __fmul_rn(az[k], r0.z)), __fadd_rn(Vxy, __fmul_rn(az[k], r1.z)));
@@ -142,10 +170,10 @@ __global__ void __launch_bounds__(256) bp_kernel(BPParams p) {
             // once: a point off the detector reads quad (0, 0) and adds nothing.
             const bool in = (uv.x >= 0.0f) & (uv.x <= umax) & (uv.y >= 0.0f) & (uv.y <= vmax);
             uv = in ? uv : f2(0.0f, 0.0f);
-            const float fu = floorf(uv.x), fv = floorf(uv.y);
-            const float2 fxy = pfma(f2(fu, fv), neg1, uv);            // (u - fu, v - fv), exact
-            const int idx = __float2int_rz(fmaf(fv, fU, fu));         // exact: < 2^24
-            const int ix = __float2int_rz(fu);
+            const float2 t = padd_rm(uv, f2(kMagic, kMagic));         // 2^23 + floor(uv)
+            const float2 fxy = psub(uv, psub(t, f2(kMagic, kMagic)));  // (u - fu, v - fv), exact
+            const int ix = __float_as_int(t.x) - kMagicBits;
+            const int idx = (__float_as_int(t.y) - kMagicBits) * p.U + ix;
             const float4 Q = __ldg(q + idx);
             const float2 w = __ldg(tw + ix);
             const float2 lo = f2(Q.x, Q.y), hi = f2(Q.z, Q.w);       // columns ix, ix + 1
@@ -179,6 +207,162 @@ __global__ void __launch_bounds__(256) bp_kernel(BPParams p) {
             p.cnt[idx] = acc[k].y;
         }
     }
+}
+
+// ---- mixed precision ---------------------------------------------------------
+// Record per (slot, row r, column c), 16 bytes:
+//   .x  half2 (p[r][c], p[r+1][c]) / s       the tapered footprint, divided by
+//   .y  half2 (p[r][c+1], p[r+1][c+1]) / s   the view's power-of-two scale s
+//   .z  float w[c]                           the taper at c
+//   .w  float w[c+1] - w[c]                  and its step to c+1
+// so one 16-byte load per sample fetches everything the sample needs.
+// The coordinates use an approximate reciprocal of W and fused
+// multiply-adds; when W does not depend on z the slices of a thread are
+// equally spaced on the detector and u, v advance by a constant per slice.
+// A sample is taken when floor(u) <= cols-2 and floor(v) <= rows-2 (the
+// same set as 0 <= u <= cols-1, 0 <= v <= rows-1 up to the measure-zero
+// points u = cols-1, v = rows-1), tested on the integer parts.  The lerps,
+// the rescale by s and the (sum, weight) accumulation are FP32.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+template <int ZPT, bool FINALIZE, bool WZ>
+__global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_mixed_kernel(BPParams p) {
+    const int x = blockIdx.x * 32 + threadIdx.x;
+    const int y = blockIdx.y * 8 + threadIdx.y;
+    const int zb = p.z_begin + blockIdx.z * ZPT;
+    if (x >= p.X || y >= p.Y) return;
+    const float ax = (x - 0.5f * (p.X - 1)) * p.pxy;
+    const float ay = (y - 0.5f * (p.Y - 1)) * p.pxy;
+    const float az0 = (zb - 0.5f * (p.Z - 1)) * p.pz;
+    float2 acc[ZPT];  // (sum, weight)
+    const size_t plane = (size_t)p.X * p.Y;
+    const size_t base = (size_t)y * p.X + x;
+#pragma unroll
+    for (int k = 0; k < ZPT; ++k) {
+        const bool in = zb + k < p.z_end;
+        acc[k] = (!FINALIZE && p.load_acc && in)
+                     ? f2(p.sum[(size_t)(zb + k) * plane + base], p.cnt[(size_t)(zb + k) * plane + base])
+                     : f2(0.0f, 0.0f);
+    }
+    const unsigned um1 = (unsigned)(p.U - 1), vm1 = (unsigned)(p.V - 1), uu = (unsigned)p.U;
+    const float2 neg1 = f2(-1.0f, -1.0f), magic = f2(kMagic, kMagic);
+
+    const float4* P4 = reinterpret_cast<const float4*>(p.ptm + (size_t)p.v0 * 12);
+    const float* sc = p.qscale + p.v0;
+    const uint4* __restrict__ q = p.qh + (size_t)(p.v0 - p.view_base) * p.q4_frame;
+#pragma unroll 1
+    for (int n = 0; n < p.nv; ++n, P4 += 3, ++sc, q += p.q4_frame) {
+        const float4 r0 = __ldg(P4), r1 = __ldg(P4 + 1), r2 = __ldg(P4 + 2);
+        const float2 P26 = f2(r0.z, r1.z);
+        // U, V, W at slice zb
+        const float2 UV0 = pfma(f2(az0, az0), P26,
+                                pfma(f2(ax, ax), f2(r0.x, r1.x), pfma(f2(ay, ay), f2(r0.y, r1.y), f2(r0.w, r1.w))));
+        const float W0 = fmaf(az0, r2.z, fmaf(ax, r2.x, fmaf(ay, r2.y, r2.w)));
+        float2 uv = f2(0.f, 0.f), duv = f2(0.f, 0.f);
+        if (!WZ) {
+            const float r = rcp_approx(W0);
+            uv = pfma(UV0, f2(r, r), f2(0.5f, 0.5f));
+            const float rz = r * p.pz;
+            duv = pmul(P26, f2(rz, rz));
+        }
+        const float s = __ldg(sc);
+#pragma unroll
+        for (int k = 0; k < ZPT; ++k) {
+            float2 cuv;
+            if (WZ) {
+                const float dz = k * p.pz;
+                const float r = rcp_approx(fmaf(dz, r2.z, W0));
+                cuv = pfma(pfma(f2(dz, dz), P26, UV0), f2(r, r), f2(0.5f, 0.5f));
+            } else {
+                cuv = uv;              // slice k: uv0 + k duv, stepped
+                uv = padd(uv, duv);
+            }
+            const float2 t = padd_rm(cuv, magic);                     // 2^23 + floor(uv)
+            const float2 f = psub(cuv, psub(t, magic));               // fractions
+            const unsigned iu = __float_as_uint(t.x) - (unsigned)kMagicBits;
+            const unsigned iv = __float_as_uint(t.y) - (unsigned)kMagicBits;
+            const bool in = (iu < um1) & (iv < vm1);                  // negative / NaN wrap to large
+            const unsigned idx = in ? iv * uu + iu : 0u;
+            const uint4 rec = __ldg(q + idx);
+            const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&rec.x));  // column c, rows r, r+1
+            const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&rec.y));  // column c+1
+            const float2 tb = pfma(f2(f.x, f.x), pfma(lo, neg1, hi), lo);
+            const float val = fmaf(f.y, tb.y - tb.x, tb.x);
+            const float c = fmaf(f.x, __uint_as_float(rec.w), __uint_as_float(rec.z));
+            if (in) acc[k] = pfma(f2(s, 1.0f), f2(val, c), acc[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < ZPT; ++k) {
+        if (zb + k >= p.z_end) break;
+        const size_t idx = (size_t)(zb + k) * plane + base;
+        if (FINALIZE) {
+            float o = __fdiv_rn(acc[k].x, acc[k].y);
+            if (p.apply_ct) o = ct_number(o, p.ct_scale, p.ct_norm1);
+            if (p.out) p.out[idx] = o;
+            if (p.out16) p.out16[idx] = to_i16(o);
+        } else {
+            p.sum[idx] = acc[k].x;
+            p.cnt[idx] = acc[k].y;
+        }
+    }
+}
+
+// Largest |value| of each frame as float bits; for non-negative floats the
+// bit patterns order like the values, so an integer atomicMax reduces them.
+// out[] must be zero before the launch.
+__global__ void __launch_bounds__(256) frame_absmax_kernel(const float* __restrict__ plain, long long frame,
+                                                           unsigned* __restrict__ out) {
+    const float* fr = plain + (size_t)blockIdx.y * frame;
+    float m = 0.0f;
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < frame; i += (long long)gridDim.x * 256)
+        m = fmaxf(m, fabsf(__ldg(fr + i)));   // fmaxf drops NaN operands
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out + blockIdx.y, __float_as_uint(m));
+}
+
+// Power-of-two scale of a view: max |q| / s lies in [2^13, 2^14), so a
+// stored value and the difference of two (below 2^15) stay inside the FP16
+// range, and dividing by s is exact.  An all-zero (or non-finite) view gets 1.
+__device__ __forceinline__ float view_scale(unsigned maxbits) {
+    const float m = __uint_as_float(maxbits);
+    if (!(m > 0.0f) || !(m <= 3.0e38f)) return 1.0f;
+    return ldexpf(1.0f, ilogbf(m) - 13);
+}
+
+// Filtered frames -> mixed-precision records in slots [slot0, slot0 + nv),
+// tapered with the taper of rotation view (view0 + f) mod num_views; writes
+// that view's scale to scale[view].
+__global__ void __launch_bounds__(256) pack_mixed_kernel(const float* __restrict__ plain, long long plain_frame,
+                                                         int rows, int U, const float2* __restrict__ tw, int view0,
+                                                         int num_views, const unsigned* __restrict__ absmax,
+                                                         float* __restrict__ scale, uint4* __restrict__ qh,
+                                                         long long q_frame, int slot0) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y, f = blockIdx.z;
+    if (c >= U) return;
+    const int view = (view0 + f) % num_views;
+    const float s = view_scale(absmax[f]);
+    const float inv = __fdiv_rn(1.0f, s);
+    if (r == 0 && c == 0) scale[view] = s;
+    const float* src = plain + (size_t)f * plain_frame + (size_t)r * U + c;
+    const bool right = c + 1 < U, down = r + 1 < rows;
+    const float2 w = tw[(size_t)view * U + c];
+    const float p00 = src[0] * w.x, p10 = down ? src[U] * w.x : 0.0f;
+    const float p01 = right ? src[1] * w.y : 0.0f, p11 = (right && down) ? src[U + 1] * w.y : 0.0f;
+    const __half2 lo = __floats2half2_rn(p00 * inv, p10 * inv);
+    const __half2 hi = __floats2half2_rn(p01 * inv, p11 * inv);
+    uint4 rec;
+    rec.x = *reinterpret_cast<const unsigned*>(&lo);
+    rec.y = *reinterpret_cast<const unsigned*>(&hi);
+    rec.z = __float_as_uint(w.x);
+    rec.w = __float_as_uint(w.y - w.x);
+    qh[(size_t)(slot0 + f) * q_frame + (size_t)r * U + c] = rec;
 }
 
 // Filtered frames -> tapered quads.  One thread per (row, column) of a frame:
@@ -252,6 +436,23 @@ cudaError_t go2(const BPParams& p, bool wz, cudaStream_t s) {
     return wz ? go<ZPT, F, E, true>(p, s) : go<ZPT, F, E, false>(p, s);
 }
 
+template <int ZPT, bool F, bool WZ>
+cudaError_t go_mixed(const BPParams& p, cudaStream_t s) {
+    const int nz = p.z_end - p.z_begin;
+    dim3 grid((p.X + 31) / 32, (p.Y + 7) / 8, (nz + ZPT - 1) / ZPT);
+    bp_mixed_kernel<ZPT, F, WZ><<<grid, dim3(32, 8), 0, s>>>(p);
+    return cudaGetLastError();
+}
+
+template <bool F, bool WZ>
+cudaError_t go_mixed2(const BPParams& p, int zpt, cudaStream_t s) {
+    switch (zpt) {
+        case 16: return go_mixed<16, F, WZ>(p, s);
+        case 8: return go_mixed<8, F, WZ>(p, s);
+        default: return go_mixed<4, F, WZ>(p, s);
+    }
+}
+
 template <bool F, bool E>
 cudaError_t go3(const BPParams& p, bool wz, int zpt, cudaStream_t s) {
     switch (zpt) {
@@ -266,6 +467,28 @@ cudaError_t go3(const BPParams& p, bool wz, int zpt, cudaStream_t s) {
 cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, cudaStream_t s) {
     if (finalize) return exact ? go3<true, true>(p, w_depends_on_z, zpt, s) : go3<true, false>(p, w_depends_on_z, zpt, s);
     return exact ? go3<false, true>(p, w_depends_on_z, zpt, s) : go3<false, false>(p, w_depends_on_z, zpt, s);
+}
+
+cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, cudaStream_t s) {
+    if (finalize) return w_depends_on_z ? go_mixed2<true, true>(p, zpt, s) : go_mixed2<true, false>(p, zpt, s);
+    return w_depends_on_z ? go_mixed2<false, true>(p, zpt, s) : go_mixed2<false, false>(p, zpt, s);
+}
+
+cudaError_t launch_frame_absmax(const float* plain, long long frame, int nv, unsigned* absmax, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(absmax, 0, sizeof(unsigned) * nv, s);
+    if (e != cudaSuccess) return e;
+    const int bx = (int)std::min<long long>((frame + 255) / 256, 64);
+    frame_absmax_kernel<<<dim3(bx, nv), 256, 0, s>>>(plain, frame, absmax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_mixed(const float* plain, long long plain_frame, int nv, int rows, int U, const float2* tw,
+                              int view0, int num_views, const unsigned* absmax, float* scale, uint4* qh,
+                              long long q_frame, int slot0, cudaStream_t s) {
+    dim3 grid((U + 255) / 256, rows, nv);
+    pack_mixed_kernel<<<grid, 256, 0, s>>>(plain, plain_frame, rows, U, tw, view0, num_views, absmax, scale, qh,
+                                           q_frame, slot0);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_pack_quads(const float* plain, long long plain_frame, int nv, int rows, int U, const float2* tw,

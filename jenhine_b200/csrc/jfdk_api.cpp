@@ -96,6 +96,16 @@ jfdk_status ensure_Q4(jfdk_ctx* c, int views) {
     return JFDK_OK;
 }
 
+jfdk_status ensure_absmax(jfdk_ctx* c, int n) {
+    if (c->absmax_n >= n) return JFDK_OK;
+    dev_free(c->d_absmax);
+    c->absmax_n = 0;
+    jfdk_status st = dev_alloc(c, &c->d_absmax, (size_t)n, "the per-view maxima");
+    if (st) return st;
+    c->absmax_n = n;
+    return JFDK_OK;
+}
+
 jfdk_status ensure_acc(jfdk_ctx* c) {
     if (c->d_sum) return JFDK_OK;
     const size_t n = (size_t)c->X * c->Y * c->Z;
@@ -149,6 +159,43 @@ BPParams bp_params(const jfdk_ctx* c) {
     return b;
 }
 
+bool mixed(const jfdk_ctx* c) { return c->precision == JFDK_PRECISION_MIXED; }
+
+// Slices per thread: the option, else 8 (measured fastest in both forms).
+int bp_zpt(const jfdk_ctx* c) { return c->opt_bp_zpt ? c->opt_bp_zpt : 8; }
+
+// Filtered frames [nv][rows][out_w] of rotation views view0.. -> the BP store,
+// slots slot0..: tapered FP32 quads, or in the mixed form FP16 records with
+// the views' scales.
+jfdk_status pack_frames(jfdk_ctx* c, const float* plain, int nv, int view0, int slot0) {
+    if (mixed(c)) {
+        jfdk_status st = ensure_absmax(c, nv);
+        if (st) return st;
+        JFDK_LAUNCH(c, launch_frame_absmax(plain, frame_px(c), nv, c->d_absmax, c->stream), "per-view maxima");
+        JFDK_LAUNCH(c, launch_pack_mixed(plain, frame_px(c), nv, c->rows, c->out_w, c->d_tw, view0, c->nviews,
+                                         c->d_absmax, c->d_qscale, reinterpret_cast<uint4*>(c->d_q4), frame_px(c),
+                                         slot0, c->stream),
+                    "packing projections");
+        return JFDK_OK;
+    }
+    JFDK_LAUNCH(c, launch_pack_quads(plain, frame_px(c), nv, c->rows, c->out_w, c->d_tw, view0, c->nviews, 1, c->d_q4,
+                                     frame_px(c), slot0, c->stream),
+                "packing projections");
+    return JFDK_OK;
+}
+
+jfdk_status run_bp(jfdk_ctx* c, BPParams b, bool finalize) {
+    if (mixed(c)) {
+        b.qh = reinterpret_cast<const uint4*>(c->d_q4);
+        b.qscale = c->d_qscale;
+        JFDK_LAUNCH(c, launch_bp_mixed(b, finalize, c->w_depends_on_z, bp_zpt(c), c->stream), "backprojection");
+        return JFDK_OK;
+    }
+    JFDK_LAUNCH(c, launch_bp(b, finalize, c->opt_bp_exact != 0, c->w_depends_on_z, bp_zpt(c), c->stream),
+                "backprojection");
+    return JFDK_OK;
+}
+
 cudaError_t launch_ramp(jfdk_ctx* c, const RampParams& r) {
     if (c->opt_filter_simt) return launch_ramp_gemm(r, c->stream);
     return launch_ramp_gemm_tc(r, c->d_Th, c->d_Tl, c->d_status, c->stream);
@@ -199,7 +246,7 @@ void jfdk_destroy(jfdk_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     dev_free(c->d_ptm); dev_free(c->d_tw); dev_free(c->d_tinv); dev_free(c->d_dmin);
     dev_free(c->d_T); dev_free(c->d_Th); dev_free(c->d_Tl); dev_free(c->d_status); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_plain);
-    dev_free(c->d_q4);
+    dev_free(c->d_q4); dev_free(c->d_qscale); dev_free(c->d_absmax);
     dev_free(c->d_sum); dev_free(c->d_cnt); dev_free(c->d_raw_stage); dev_free(c->d_hu_stage);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
@@ -225,8 +272,8 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     c->recon.adjust_points = nullptr;
     c->recon.adjust_level_db = nullptr;
     c->precision = precision;
-    if (precision != JFDK_PRECISION_FP32)
-        return bail(fail(c, JFDK_ERR_UNSUPPORTED, "precision mode not available in this build"));
+    if (precision != JFDK_PRECISION_FP32 && precision != JFDK_PRECISION_MIXED)
+        return bail(fail(c, JFDK_ERR_INVALID, "unknown precision mode"));
     c->nviews = scan->num_views;
     c->used_u = scan->num_dets_u - scan->border_left - scan->border_right;
     c->used_v = scan->num_dets_v - scan->border_up - scan->border_down;
@@ -282,6 +329,7 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     if ((st = dev_alloc(c, &c->d_Tl, (size_t)c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_c, (size_t)c->out_w, "the edge response"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_status, 1, "the status word"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_qscale, (size_t)c->nviews, "the view scales"))) return bail(st);
     JFDK_CUDA(c, cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream), "clearing the status word");
     std::vector<float2> twp((size_t)c->nviews * c->out_w);
     for (int v = 0; v < c->nviews; ++v)
@@ -323,7 +371,8 @@ jfdk_status jfdk_set_option(jfdk_ctx* c, int key, long long value) {
             c->opt_view_chunk = (int)value;
             return JFDK_OK;
         case JFDK_OPT_BP_ZPT:
-            if (value != 4 && value != 8 && value != 16) return fail(c, JFDK_ERR_INVALID, "slices per thread must be 4, 8 or 16");
+            if (value != 0 && value != 4 && value != 8 && value != 16)
+                return fail(c, JFDK_ERR_INVALID, "slices per thread must be 0 (default), 4, 8 or 16");
             c->opt_bp_zpt = (int)value;
             return JFDK_OK;
         case JFDK_OPT_FILTER_SIMT: c->opt_filter_simt = value ? 1 : 0; return JFDK_OK;
@@ -422,15 +471,12 @@ jfdk_status jfdk_bp_accumulate(jfdk_ctx* c, const float* d_proj, int v0, int nv)
     if (nv == 0) return JFDK_OK;
     jfdk_status st = ensure_Q4(c, nv);
     if (st) return st;
-    // InitView: taper the caller's frames while packing them into quads
-    JFDK_LAUNCH(c, launch_pack_quads(d_proj, frame_px(c), nv, c->rows, c->out_w, c->d_tw, v0, c->nviews, 1, c->d_q4,
-                                     frame_px(c), 0, c->stream),
-                "packing projections");
+    // InitView: taper the caller's frames while packing them
+    if ((st = pack_frames(c, d_proj, nv, v0, 0))) return st;
     BPParams b = bp_params(c);
     b.view_base = v0; b.v0 = v0; b.nv = nv;
     b.sum = c->d_sum; b.cnt = c->d_cnt; b.load_acc = 1;
-    JFDK_LAUNCH(c, launch_bp(b, false, c->opt_bp_exact != 0, c->w_depends_on_z, c->opt_bp_zpt, c->stream), "backprojection");
-    return JFDK_OK;
+    return run_bp(c, b, false);
 }
 
 jfdk_status jfdk_finalize(jfdk_ctx* c, int z0, int nz, int apply_ct, float* d_out, int16_t* d_out16) {
@@ -474,16 +520,14 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, in
         if (c->recon.z_filter)
             JFDK_LAUNCH(c, launch_zfilter(c->d_plain, nv, c->rows, c->out_w, frame_px(c), c->out_w, c->stream),
                         "z-filter");
-        JFDK_LAUNCH(c, launch_pack_quads(c->d_plain, frame_px(c), nv, c->rows, c->out_w, c->d_tw, v0, c->nviews, 1,
-                                         c->d_q4, frame_px(c), v0, c->stream),
-                    "packing projections");
+        if ((st = pack_frames(c, c->d_plain, nv, v0, v0))) return st;
     }
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[1], c->stream), "event");
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[2], c->stream), "event");
     BPParams b = bp_params(c);
     b.view_base = 0; b.v0 = 0; b.nv = c->nviews;
     b.out = d_hu; b.out16 = d_hu16; b.apply_ct = 1;
-    JFDK_LAUNCH(c, launch_bp(b, true, c->opt_bp_exact != 0, c->w_depends_on_z, c->opt_bp_zpt, c->stream), "backprojection");
+    if ((st = run_bp(c, b, true))) return st;
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[3], c->stream), "event");
     return JFDK_OK;
 }

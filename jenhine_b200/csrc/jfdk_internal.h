@@ -35,6 +35,8 @@ std::string build_host_operators(const jfdk_scan_params& scan, const jfdk_recon_
 struct BPParams {
     const float4* q4;        // quads, [slots][rows][U]: (p[r][c], p[r+1][c], p[r][c+1], p[r+1][c+1])
     const float2* tw;        // [views][U] taper pairs (w[c], w[c+1]), w[U] = 0
+    const uint4* qh;         // mixed precision: records [slots][rows][U] (bp.cu)
+    const float* qscale;     // mixed precision: [views] power-of-two scale of each view
     const float* ptm;        // [views][12]
     long long q4_frame;      // quads per slot (rows * U)
     int view_base;           // rotation index held by slot 0
@@ -55,6 +57,15 @@ struct BPParams {
 // Launchers (return cudaError_t of the launch).
 // zpt: slices per thread (4, 8 or 16).
 cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, cudaStream_t s);
+// Mixed-precision form: FP16 footprints with a per-view scale (qh, qscale).
+cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, cudaStream_t s);
+// absmax[f] = bit pattern of max |plain[f][...]| over each of nv frames.
+cudaError_t launch_frame_absmax(const float* plain, long long frame, int nv, unsigned* absmax, cudaStream_t s);
+// Filtered frames -> mixed-precision records in slots [slot0, slot0 + nv);
+// writes the scale of rotation view (view0 + f) mod num_views to scale[].
+cudaError_t launch_pack_mixed(const float* plain, long long plain_frame, int nv, int rows, int U, const float2* tw,
+                              int view0, int num_views, const unsigned* absmax, float* scale, uint4* qh,
+                              long long q_frame, int slot0, cudaStream_t s);
 // Filtered frames [nv][rows][U] -> quads in slots [slot0, slot0 + nv), tapered
 // with the taper of rotation view (view0 + f) when apply_taper.
 cudaError_t launch_pack_quads(const float* plain, long long plain_frame, int nv, int rows, int U, const float2* tw,
@@ -156,7 +167,9 @@ struct jfdk_ctx {
     float* d_A = nullptr;  size_t a_rows = 0;   // weighted rows, pitch a_pitch
     float* d_e = nullptr;
     float* d_plain = nullptr; int plain_views = 0;  // filtered frames of one chunk
-    float4* d_q4 = nullptr; int q4_views = 0;       // quad store
+    float4* d_q4 = nullptr; int q4_views = 0;       // quad store (mixed: uint4 records)
+    float* d_qscale = nullptr;                      // mixed: [views] scales
+    unsigned* d_absmax = nullptr; int absmax_n = 0; // mixed: per-frame maxima
     float* d_sum = nullptr;
     float* d_cnt = nullptr;
     uint16_t* d_raw_stage = nullptr; size_t raw_stage_bytes = 0;
@@ -167,7 +180,7 @@ struct jfdk_ctx {
     int opt_bp_exact = 0;
     int opt_view_chunk = 32;
     int opt_stage_timing = 0;
-    int opt_bp_zpt = 4;
+    int opt_bp_zpt = 0;          // 0: default (bp_zpt() in jfdk_api.cpp)
     int opt_filter_simt = 0;     // 1: ramp product on FP32 CUDA cores instead of tcgen05
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 

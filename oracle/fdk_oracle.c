@@ -486,6 +486,42 @@ void jo_filter_rows(float* out, const float* in, const float* preweight,
     free(ramp); free(buf); free(re); free(im);
 }
 
+/* FP64 oracle of FilterCore::ProcessRow: the same steps as jo_filter_rows
+ * (pre-weight product, truncation ramp of the edge mean, filtering by H over
+ * L points, crop) with every buffer and operation in double. */
+void jo_filter_rows_f64(double* out, const float* in, const float* preweight,
+                        int rows, int W, int Wout, int mirror, const float* H, int L) {
+    const int R = (L - W) / 2;
+    const int off = mirror ? Wout : 0;
+    double* re = (double*)malloc(sizeof(double) * L);
+    double* im = (double*)malloc(sizeof(double) * L);
+    for (int r = 0; r < rows; ++r) {
+        const float* x = in + (size_t)r * W;
+        for (int i = 0; i < L; ++i) {
+            double v = i < W ? (double)x[i] : 0.0;
+            if (preweight) v *= (double)preweight[(size_t)r * L + i];
+            re[i] = v;
+            im[i] = 0.0;
+        }
+        if (mirror) {
+            const double edge = ((double)x[W - 1] + x[W - 2] + x[W - 3]) / 3.0;
+            for (int k = 0; k < R; ++k) re[W + k] = (double)(R - 1 - k) / R * edge;
+        } else {
+            const double edge = ((double)x[0] + x[1] + x[2]) / 3.0;
+            for (int k = 0; k < R; ++k) re[L - R + k] = (double)k / R * edge;
+        }
+        fft_c2c_pow2(re, im, L, -1);
+        for (int k = 0; k < L; ++k) {
+            const double h = (k <= L / 2) ? H[k] : H[L - k];
+            re[k] *= h; im[k] *= h;
+        }
+        fft_c2c_pow2(re, im, L, +1);
+        double* y = out + (size_t)r * Wout;
+        for (int j = 0; j < Wout; ++j) y[j] = re[off + j] / L;
+    }
+    free(re); free(im);
+}
+
 /* ======================================================================
  * Backprojection -- BPAgent/BPCore.cpp
  * ==================================================================== */
@@ -623,6 +659,66 @@ void jo_bp_accumulate_f64(double* sum, double* cnt, const float* proj, const flo
                           float pitchXY, float pitchZ, int z0, int nz, int nthreads) {
     bp_run(NULL, NULL, sum, cnt, proj, ptms, uw, v0, nv, U, V, X, Y, Z, pitchXY, pitchZ,
            z0, nz, nthreads);
+}
+
+/* FP64 oracle of BPCore for a list of voxels: the same rule as bp_worker
+ * (taper product, u = U/W + 0.5, v = V/W + 0.5, sample only when
+ * 0 <= u <= U-1 and 0 <= v <= V-1, bilinear lerps, sum and weight) with the
+ * axes, coordinates, projections and arithmetic in double. */
+typedef struct {
+    double* sum; double* cnt; const double* proj; const float* ptms; const float* uw;
+    int v0, nv, U, V, X, Y, Z; double pitchXY, pitchZ; const int* pts; int p0, p1;
+} bpp_job;
+
+static void* bpp_worker(void* arg) {
+    bpp_job* j = (bpp_job*)arg;
+    const int U = j->U, V = j->V;
+    for (int i = j->p0; i < j->p1; ++i) {
+        const double x = ((double)j->pts[3 * i] - (j->X - 1) / 2.0) * j->pitchXY;
+        const double y = ((double)j->pts[3 * i + 1] - (j->Y - 1) / 2.0) * j->pitchXY;
+        const double z = ((double)j->pts[3 * i + 2] - (j->Z - 1) / 2.0) * j->pitchZ;
+        double s = 0.0, c = 0.0;
+        for (int iv = 0; iv < j->nv; ++iv) {
+            const int view = j->v0 + iv;
+            const float* P = j->ptms + (size_t)view * 12;
+            const double Uc = x * P[0] + y * P[1] + z * P[2] + P[3];
+            const double Vc = x * P[4] + y * P[5] + z * P[6] + P[7];
+            const double Wc = x * P[8] + y * P[9] + z * P[10] + P[11];
+            const double u = Uc / Wc + 0.5, v = Vc / Wc + 0.5;
+            if (!(u >= 0.0 && u <= U - 1 && v >= 0.0 && v <= V - 1)) continue;
+            const int ix = (int)floor(u), iy = (int)floor(v);
+            const int ix1 = ix + 1 < U ? ix + 1 : U - 1;
+            const int iy1 = iy + 1 < V ? iy + 1 : V - 1;
+            const double fx = u - ix, fy = v - iy;
+            const double* p = j->proj + (size_t)iv * U * V;
+            const float* w = j->uw + (size_t)view * U;
+            const double p00 = p[(size_t)iy * U + ix] * w[ix], p01 = p[(size_t)iy * U + ix1] * w[ix1];
+            const double p10 = p[(size_t)iy1 * U + ix] * w[ix], p11 = p[(size_t)iy1 * U + ix1] * w[ix1];
+            const double t0 = p00 + fx * (p01 - p00), t1 = p10 + fx * (p11 - p10);
+            s += t0 + fy * (t1 - t0);
+            c += (double)w[ix] + fx * ((double)w[ix1] - w[ix]);
+        }
+        j->sum[i] += s;
+        j->cnt[i] += c;
+    }
+    return NULL;
+}
+
+void jo_bp_points_f64(double* sum, double* cnt, const double* proj, const float* ptms,
+                      const float* uw, int v0, int nv, int U, int V, const int* pts, int npts,
+                      int X, int Y, int Z, float pitchXY, float pitchZ, int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > npts) nthreads = npts > 0 ? npts : 1;
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * nthreads);
+    bpp_job* jobs = (bpp_job*)malloc(sizeof(bpp_job) * nthreads);
+    for (int t = 0; t < nthreads; ++t) {
+        bpp_job jb = {sum, cnt, proj, ptms, uw, v0, nv, U, V, X, Y, Z, pitchXY, pitchZ, pts,
+                      (int)((long)npts * t / nthreads), (int)((long)npts * (t + 1) / nthreads)};
+        jobs[t] = jb;
+        pthread_create(&th[t], NULL, bpp_worker, &jobs[t]);
+    }
+    for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+    free(th); free(jobs);
 }
 
 /* BPCore::DoneSlice (BPCore.cpp:198-205): out = sum / cnt. */

@@ -74,6 +74,9 @@ void jo_filter_spectrum(float* H, int L, float halfSampleRate,
 void jo_filter_rows(float* out, const float* in, const float* preweight,
                     int rows, int W, int Wout, int mirror,
                     const float* H, int L);
+/* The same in double throughout (FP64 oracle); out is double. */
+void jo_filter_rows_f64(double* out, const float* in, const float* preweight,
+                        int rows, int W, int Wout, int mirror, const float* H, int L);
 /* Equivalent real, even space kernel h_eff[L] = IDFT_L(H) (double). */
 void jo_filter_kernel_f64(double* h, const float* H, int L);
 
@@ -92,6 +95,12 @@ void jo_bp_accumulate_f64(double* sum, double* cnt, const float* proj,
                           const float* ptms, const float* uw, int v0, int nv,
                           int U, int V, int X, int Y, int Z, float pitchXY,
                           float pitchZ, int z0, int nz, int nthreads);
+/* FP64 oracle for a list of voxels pts[npts][3] = (x, y, z) indices:
+ * coordinates, taper product, lerps and sums in double; projections proj
+ * [nv][V][U] in double, NOT yet tapered.  Adds into sum[npts], cnt[npts]. */
+void jo_bp_points_f64(double* sum, double* cnt, const double* proj, const float* ptms,
+                      const float* uw, int v0, int nv, int U, int V, const int* pts, int npts,
+                      int X, int Y, int Z, float pitchXY, float pitchZ, int nthreads);
 /* out = sum / cnt (BPCore::DoneSlice). */
 void jo_bp_finalize(float* out, const float* sum, const float* cnt, size_t n);
 

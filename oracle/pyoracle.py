@@ -50,6 +50,8 @@ class Oracle:
             "jo_rfft_forward": [_P, _P, I], "jo_rfft_backward": [_P, _P, I],
             "jo_filter_spectrum": [_P, I, F, F, F, _P, _P, I],
             "jo_filter_rows": [_P, _P, _P, I, I, I, I, _P, I],
+            "jo_filter_rows_f64": [_P, _P, _P, I, I, I, I, _P, I],
+            "jo_bp_points_f64": [_P, _P, _P, _P, _P, I, I, I, I, _P, I, I, I, I, F, F, I],
             "jo_filter_kernel_f64": [_P, _P, I], "jo_bp_uweights": [_P, _P, I, I],
             "jo_bp_accumulate": [_P, _P, _P, _P, _P, I, I, I, I, I, I, I, F, F, I, I, I],
             "jo_bp_accumulate_f64": [_P, _P, _P, _P, _P, I, I, I, I, I, I, I, F, F, I, I, I],
@@ -154,6 +156,34 @@ class Oracle:
                                 w_out, int(mirror), _ptr(_c(H, _f32)), L)
         return out.reshape(rows.shape[:-1] + (w_out,))
 
+    def filter_rows_f64(self, rows, H, L, w_out=None, mirror=False, preweight=None):
+        rows = _c(rows, _f32)
+        R, W = rows.reshape(-1, rows.shape[-1]).shape
+        w_out = W if w_out is None else w_out
+        out = np.empty((R, w_out), np.float64)
+        pw = None if preweight is None else _c(preweight, _f32)
+        self.lib.jo_filter_rows_f64(_ptr(out), _ptr(rows), None if pw is None else _ptr(pw), R, W,
+                                    w_out, int(mirror), _ptr(_c(H, _f32)), L)
+        return out.reshape(rows.shape[:-1] + (w_out,))
+
+    def filter_projections_f64(self, proj, ptms, H, dso, mirror=False, rows=None):
+        """FP64 FilterAgent over views 0..N-1 (9-view pre-weight grouping, the
+        pre-weight table itself as the reference computes it), restricted to
+        detector rows [rows[0], rows[1]) when given."""
+        proj = _c(proj, _f32)
+        V, Hh, W = proj.shape
+        r0, r1 = (0, Hh) if rows is None else rows
+        L = self.fft_length(W)
+        out = np.empty((V, r1 - r0, W), np.float64)
+        cache = {}
+        for v in range(V):
+            s = self.preweight_source_view(v, V)
+            if s not in cache:
+                cache.clear()
+                cache[s] = self.preweight_for_view(ptms[s], dso, W, Hh, mirror)[r0:r1]
+            out[v] = self.filter_rows_f64(proj[v, r0:r1], H, L, W, mirror, cache[s])
+        return out
+
     def filter_projections(self, proj, ptms, H, dso, mirror=False):
         """FilterAgent over views 0..N-1: the 9-view pre-weight grouping."""
         proj = _c(proj, _f32)
@@ -197,6 +227,55 @@ class Oracle:
         out = np.empty_like(s)
         self.lib.jo_bp_finalize(_ptr(out), _ptr(s), _ptr(c), out.size)
         return out
+
+    def bp_points_f64(self, proj, ptms, pts, X, Y, Z, pitch_xy, pitch_z, row0=0, det_rows=None,
+                      nthreads=None):
+        """FP64 backprojection of voxels pts[n][3] = (x, y, z).  proj holds
+        detector rows [row0, row0 + proj.shape[1]) of a detector det_rows high
+        (default: all rows given); a voxel that samples a row outside the
+        given band raises.  Returns (sum, weight) per point."""
+        proj = _c(proj, np.float64)
+        nv, Vb, U = proj.shape
+        det_rows = Vb if det_rows is None else det_rows
+        ptms = _c(ptms, _f32).reshape(-1, 12)
+        uw = self.bp_uweights(ptms, U)
+        pts = _c(pts, np.int32).reshape(-1, 3)
+        if row0 or Vb != det_rows:
+            # embed the band in a full-height detector (zeros elsewhere) and
+            # check that every sample used lies inside the band
+            full = np.zeros((nv, det_rows, U), np.float64)
+            full[:, row0:row0 + Vb] = proj
+            self._check_band(ptms, pts, X, Y, Z, pitch_xy, pitch_z, U, det_rows, row0, row0 + Vb)
+            proj = full
+        s = np.zeros(len(pts), np.float64)
+        c = np.zeros(len(pts), np.float64)
+        self.lib.jo_bp_points_f64(_ptr(s), _ptr(c), _ptr(proj), _ptr(ptms), _ptr(uw), 0, nv, U,
+                                  det_rows, _ptr(pts), len(pts), X, Y, Z, pitch_xy, pitch_z,
+                                  nthreads or os.cpu_count() or 1)
+        return s, c
+
+    @staticmethod
+    def _check_band(ptms, pts, X, Y, Z, pitch_xy, pitch_z, U, V, r0, r1):
+        P = ptms.astype(np.float64)
+        xyz1 = np.stack([(pts[:, 0] - (X - 1) / 2.0) * pitch_xy, (pts[:, 1] - (Y - 1) / 2.0) * pitch_xy,
+                         (pts[:, 2] - (Z - 1) / 2.0) * pitch_z, np.ones(len(pts))], 1)
+        for k in range(P.shape[0]):
+            uvw = xyz1 @ P[k].reshape(3, 4).T
+            u = uvw[:, 0] / uvw[:, 2] + 0.5
+            v = uvw[:, 1] / uvw[:, 2] + 0.5
+            used = (u >= 0) & (u <= U - 1) & (v >= 0) & (v <= V - 1)
+            if used.any():
+                lo, hi = np.floor(v[used]).min(), np.floor(v[used]).max() + 1
+                if lo < r0 or hi >= r1:
+                    raise ValueError(f"view {k}: samples rows {lo:.0f}..{hi:.0f} outside [{r0}, {r1})")
+
+    @staticmethod
+    def ctnum_f64(mu, norm0, norm1, mu_water=0.02):
+        """CTNumCore::Process in double."""
+        h = np.asarray(mu, np.float64) * (norm0 * 1000.0 / mu_water) - 1000.0
+        hi = h > 300.0
+        h[hi] = np.minimum(8191.0, (h[hi] - 300.0) * norm1 + 300.0)
+        return h
 
     # -- CT numbers ---------------------------------------------------------
     def ctnum(self, vol, norm0, norm1, mu_water=0.02):

@@ -176,3 +176,49 @@ def test_fp64_oracle_close_to_fp32(oracle):
     v32 = oracle.bp(g["filt"], g["ptms"], X, Y, Z, *map(float, g["pitch"]))
     v64 = oracle.bp(g["filt"], g["ptms"], X, Y, Z, *map(float, g["pitch"]), f64=True)
     assert rel_l2(v32, v64) < 1e-5
+
+
+def test_fp64_filter_close_to_fp32(oracle, golden):
+    _, g = golden
+    W = g["prep"].shape[2]
+    L = oracle.fft_length(W)
+    H = oracle.filter_spectrum(L, float(g["hsr"]), *map(float, g["cut"]), g["adj_pts"], g["adj_db"])
+    f64 = oracle.filter_projections_f64(g["prep"][:9], g["ptms"], H, float(g["dso"]))
+    assert rel_l2(f64, g["filt"][:9]) < 1e-6
+    band = oracle.filter_projections_f64(g["prep"][:9], g["ptms"], H, float(g["dso"]), rows=(3, 11))
+    np.testing.assert_array_equal(band, f64[:, 3:11])
+
+
+def test_fp64_points_match_fp64_volume(oracle):
+    """bp_points_f64 (double coordinates) against bp(f64=True) (BPCore's float
+    coordinates, double lerps): the same up to the coordinate rounding."""
+    from fp64_fdk import all_points
+    g = load_golden("mini_c2")
+    X, Y, Z = (int(v) for v in g["vol"])
+    pxy, pz = map(float, g["pitch"])
+    s64, c64 = oracle.bp(g["filt"], g["ptms"], X, Y, Z, pxy, pz, f64=True, return_parts=True)
+    pts = all_points(X, Y, Z)
+    s, c = oracle.bp_points_f64(g["filt"].astype(np.float64), g["ptms"], pts, X, Y, Z, pxy, pz)
+    assert rel_l2(s, s64.ravel()) < 1e-5 and rel_l2(c, c64.ravel()) < 1e-5
+    # a band of rows gives the same sums as the whole detector
+    lo, hi = 0, g["filt"].shape[1]
+    s2, c2 = oracle.bp_points_f64(g["filt"][:, lo:hi].astype(np.float64), g["ptms"], pts, X, Y, Z, pxy, pz,
+                                  row0=lo, det_rows=hi)
+    np.testing.assert_array_equal(s2, s)
+
+
+def test_fp64_fdk_pinned_to_reference_outputs(oracle, golden):
+    """The FP64 FDK restates the reference's volume: its distance to the
+    reference cores' HU output (golden) is float rounding, far below the
+    1e-4 mixed-precision bar it is used to check."""
+    from fp64_fdk import all_points, fdk_f64, interior
+    _, g = golden
+    X, Y, Z = (int(v) for v in g["vol"])
+    pts = all_points(X, Y, Z)
+    hu = fdk_f64(oracle, g, pts).reshape(Z, Y, X)
+    ref = g["hu"].astype(np.float64)
+    both = np.isfinite(hu) & np.isfinite(ref)
+    assert rel_l2(hu[both] + 1000.0, ref[both] + 1000.0) < 1e-5
+    inside = interior(g, pts).reshape(Z, Y, X)
+    assert inside.any()
+    assert np.max(np.abs(hu - ref)[both & inside]) < 0.05
