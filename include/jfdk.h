@@ -186,9 +186,21 @@ enum {
                                  stream around each stage                        */
     JFDK_OPT_BP_ZPT = 4,      /* slices each backprojection thread keeps in
                                  registers: 4, 8 or 16; 0 (default): 8         */
-    JFDK_OPT_FILTER_SIMT = 5  /* 1: ramp product on FP32 CUDA cores; 0 (default):
-                                 tcgen05 tensor cores, 3xTF32 split              */
+    JFDK_OPT_FILTER_SIMT = 5, /* 1: ramp product on FP32 CUDA cores (same as
+                                 JFDK_OPT_RAMP_PRODUCT = JFDK_RAMP_FP32_SIMT);
+                                 0: the form's default                          */
+    JFDK_OPT_RAMP_PRODUCT = 6 /* how the ramp product runs, a jfdk_ramp_product */
 };
+/* Ramp products (JFDK_OPT_RAMP_PRODUCT).  The split products run on the
+ * tcgen05 tensor cores as hi*hi + hi*lo + lo*hi with FP32 accumulation. */
+typedef enum {
+    JFDK_RAMP_DEFAULT = 0,    /* TF32x3 in the FP32 form, BF16x3 in the mixed form */
+    JFDK_RAMP_TF32X3 = 1,     /* ~2^-22 relative                                    */
+    JFDK_RAMP_BF16X3 = 2,     /* ~2^-17 relative, twice the tensor rate of TF32    */
+    JFDK_RAMP_FP16X3 = 3,     /* rows and operator scaled by powers of two into the
+                                 FP16 range; ~2^-22 relative at the BF16 rate     */
+    JFDK_RAMP_FP32_SIMT = 4   /* FP32 CUDA cores                                    */
+} jfdk_ramp_product;
 jfdk_status jfdk_set_option(jfdk_ctx* ctx, int key, long long value);
 /* Stage times (ms) of the last jfdk_reconstruct with JFDK_OPT_STAGE_TIMING:
  * [0] preprocess + pre-weight + ramp filter (+ z-filter) + packing for the

@@ -27,6 +27,8 @@ OPT_VIEW_CHUNK = 2
 OPT_STAGE_TIMING = 3
 OPT_BP_ZPT = 4
 OPT_FILTER_SIMT = 5
+OPT_RAMP_PRODUCT = 6
+RAMP_DEFAULT, RAMP_TF32X3, RAMP_BF16X3, RAMP_FP16X3, RAMP_FP32_SIMT = 0, 1, 2, 3, 4
 
 
 class ScanParams(C.Structure):

@@ -7,6 +7,8 @@
 #include <new>
 #include <string>
 
+#include <cuda_bf16.h>
+
 #include "jfdk_internal.h"
 
 using namespace jfdk;
@@ -60,20 +62,46 @@ void dev_free(T*& p) {
     p = nullptr;
 }
 
-int a_pitch(const jfdk_ctx* c) { return (int)round_up(c->in_w, 32); }
+// K padded to 64 elements: whole 128-byte rows for every operand kind.
+int a_pitch(const jfdk_ctx* c) { return (int)round_up(c->in_w, 64); }
 long long frame_px(const jfdk_ctx* c) { return (long long)c->rows * c->out_w; }
 
 jfdk_status ensure_A(jfdk_ctx* c, size_t rows) {
     if (c->a_rows >= rows) return JFDK_OK;
     dev_free(c->d_A);
     dev_free(c->d_e);
+    dev_free(c->d_arow);
     c->a_rows = 0;
-    jfdk_status st = dev_alloc(c, &c->d_A, rows * a_pitch(c), "the weighted rows");
+    // room for a high and a low part of up to 4 bytes each
+    jfdk_status st = dev_alloc(c, reinterpret_cast<float**>(&c->d_A), rows * a_pitch(c) * 2, "the weighted rows");
     if (st) return st;
-    st = dev_alloc(c, &c->d_e, rows, "the edge means");
-    if (st) return st;
+    if ((st = dev_alloc(c, &c->d_e, rows, "the edge means"))) return st;
+    if ((st = dev_alloc(c, &c->d_arow, rows, "the row scales"))) return st;
     c->a_rows = rows;
     return JFDK_OK;
+}
+
+bool mixed(const jfdk_ctx* c) { return c->precision == JFDK_PRECISION_MIXED; }
+
+int ramp_kind(const jfdk_ctx* c) {
+    if (c->opt_ramp != JFDK_RAMP_DEFAULT) return c->opt_ramp;
+    return mixed(c) ? JFDK_RAMP_BF16X3 : JFDK_RAMP_TF32X3;
+}
+
+// The A operand in the layout the chosen ramp product reads: the high part
+// at d_A, the low part after a_rows rows of it.
+AOperand a_operand(const jfdk_ctx* c) {
+    AOperand a{};
+    const int k = ramp_kind(c);
+    a.kind = k == JFDK_RAMP_TF32X3 ? AOUT_TF32X2
+             : k == JFDK_RAMP_BF16X3 ? AOUT_BF16X2
+             : k == JFDK_RAMP_FP16X3 ? AOUT_FP16X2 : AOUT_F32;
+    const size_t elem = (a.kind == AOUT_BF16X2 || a.kind == AOUT_FP16X2) ? 2 : 4;
+    a.hi = c->d_A;
+    a.lo = static_cast<char*>(c->d_A) + c->a_rows * a_pitch(c) * elem;
+    a.row_scale = c->d_arow;
+    a.pitch = a_pitch(c);
+    return a;
 }
 
 jfdk_status ensure_plain(jfdk_ctx* c, int views) {
@@ -159,8 +187,6 @@ BPParams bp_params(const jfdk_ctx* c) {
     return b;
 }
 
-bool mixed(const jfdk_ctx* c) { return c->precision == JFDK_PRECISION_MIXED; }
-
 // Slices per thread: the option, else 8 (measured fastest in both forms).
 int bp_zpt(const jfdk_ctx* c) { return c->opt_bp_zpt ? c->opt_bp_zpt : 8; }
 
@@ -196,17 +222,34 @@ jfdk_status run_bp(jfdk_ctx* c, BPParams b, bool finalize) {
     return JFDK_OK;
 }
 
-cudaError_t launch_ramp(jfdk_ctx* c, const RampParams& r) {
-    if (c->opt_filter_simt) return launch_ramp_gemm(r, c->stream);
-    return launch_ramp_gemm_tc(r, c->d_Th, c->d_Tl, c->d_status, c->stream);
+cudaError_t launch_ramp(jfdk_ctx* c, RampParams r) {
+    const AOperand a = a_operand(c);
+    switch (ramp_kind(c)) {
+        case JFDK_RAMP_FP32_SIMT:
+            r.A = static_cast<const float*>(a.hi);
+            return launch_ramp_gemm(r, c->stream);
+        case JFDK_RAMP_TF32X3:
+            return launch_ramp_gemm_tc(r, RAMP_TF32X3, a.hi, a.lo, c->d_Th, c->d_Tl, c->d_status, c->stream);
+        case JFDK_RAMP_BF16X3:
+            return launch_ramp_gemm_tc(r, RAMP_BF16X3, a.hi, a.lo, c->d_Tb, c->d_Tb + (size_t)c->out_w * a_pitch(c),
+                                       c->d_status, c->stream);
+        default:
+            r.row_scale = c->d_arow;
+            r.b_scale = c->tf_inv_scale;
+            return launch_ramp_gemm_tc(r, RAMP_FP16X3, a.hi, a.lo, c->d_Tf, c->d_Tf + (size_t)c->out_w * a_pitch(c),
+                                       c->d_status, c->stream);
+    }
 }
 
 RampParams ramp_params(const jfdk_ctx* c, int nv, float* out) {
     RampParams r{};
-    r.A = c->d_A; r.e = c->d_e; r.B = c->d_T; r.c = c->d_c;
+    r.A = nullptr; r.e = c->d_e; r.B = c->d_T; r.c = c->d_c;
     r.M = nv * c->rows; r.N = c->out_w; r.K = c->in_w; r.a_pitch = a_pitch(c);
     r.rows = c->rows;
     r.q = out; r.q_frame_stride = frame_px(c); r.q_pitch = c->out_w;
+    r.row_scale = nullptr;
+    r.b_scale = 1.0f;
+    r.vec_store = (reinterpret_cast<uintptr_t>(out) % 16 == 0) && (c->out_w % 4 == 0);
     return r;
 }
 
@@ -245,7 +288,9 @@ void jfdk_destroy(jfdk_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     dev_free(c->d_ptm); dev_free(c->d_tw); dev_free(c->d_tinv); dev_free(c->d_dmin);
-    dev_free(c->d_T); dev_free(c->d_Th); dev_free(c->d_Tl); dev_free(c->d_status); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_plain);
+    dev_free(c->d_T); dev_free(c->d_Th); dev_free(c->d_Tl); dev_free(c->d_Tb); dev_free(c->d_Tf);
+    dev_free(c->d_status); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_arow);
+    dev_free(c->d_plain);
     dev_free(c->d_q4); dev_free(c->d_qscale); dev_free(c->d_absmax);
     dev_free(c->d_sum); dev_free(c->d_cnt); dev_free(c->d_raw_stage); dev_free(c->d_hu_stage);
     for (auto& e : c->ev)
@@ -327,6 +372,8 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     if ((st = dev_alloc(c, &c->d_T, (size_t)c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_Th, (size_t)c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_Tl, (size_t)c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_Tb, (size_t)2 * c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
+    if ((st = dev_alloc(c, &c->d_Tf, (size_t)2 * c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_c, (size_t)c->out_w, "the edge response"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_status, 1, "the status word"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_qscale, (size_t)c->nviews, "the view scales"))) return bail(st);
@@ -352,6 +399,27 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
         }
         JFDK_CUDA(c, cudaMemcpyAsync(c->d_Th, th.data(), sizeof(float) * th.size(), cudaMemcpyHostToDevice, c->stream), "upload");
         JFDK_CUDA(c, cudaMemcpyAsync(c->d_Tl, tl.data(), sizeof(float) * tl.size(), cudaMemcpyHostToDevice, c->stream), "upload");
+        // BF16 split, and FP16 split of the operator scaled by a power of
+        // two that puts its largest entry in [2^14, 2^15)
+        const size_t n = Tp.size();
+        std::vector<uint16_t> tb(2 * n), tf(2 * n);
+        float tmax = 0.0f;
+        for (float v : Tp) tmax = std::max(tmax, std::fabs(v));
+        const float fs = tmax > 0.0f ? std::ldexp(1.0f, 14 - std::ilogb(tmax)) : 1.0f;
+        c->tf_inv_scale = 1.0f / fs;
+        for (size_t i = 0; i < n; ++i) {
+            const __nv_bfloat16 bh = __float2bfloat16_rn(Tp[i]);
+            const __nv_bfloat16 bl = __float2bfloat16_rn(Tp[i] - __bfloat162float(bh));
+            std::memcpy(&tb[i], &bh, 2);
+            std::memcpy(&tb[n + i], &bl, 2);
+            const float v = Tp[i] * fs;
+            const __half fh = __float2half_rn(v);
+            const __half fl = __float2half_rn(v - __half2float(fh));
+            std::memcpy(&tf[i], &fh, 2);
+            std::memcpy(&tf[n + i], &fl, 2);
+        }
+        JFDK_CUDA(c, cudaMemcpyAsync(c->d_Tb, tb.data(), 2 * tb.size(), cudaMemcpyHostToDevice, c->stream), "upload");
+        JFDK_CUDA(c, cudaMemcpyAsync(c->d_Tf, tf.data(), 2 * tf.size(), cudaMemcpyHostToDevice, c->stream), "upload");
         JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "upload");
     }
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_c, c->ops.c.data(), sizeof(float) * c->out_w, cudaMemcpyHostToDevice, c->stream), "upload");
@@ -375,7 +443,12 @@ jfdk_status jfdk_set_option(jfdk_ctx* c, int key, long long value) {
                 return fail(c, JFDK_ERR_INVALID, "slices per thread must be 0 (default), 4, 8 or 16");
             c->opt_bp_zpt = (int)value;
             return JFDK_OK;
-        case JFDK_OPT_FILTER_SIMT: c->opt_filter_simt = value ? 1 : 0; return JFDK_OK;
+        case JFDK_OPT_FILTER_SIMT: c->opt_ramp = value ? JFDK_RAMP_FP32_SIMT : JFDK_RAMP_DEFAULT; return JFDK_OK;
+        case JFDK_OPT_RAMP_PRODUCT:
+            if (value < JFDK_RAMP_DEFAULT || value > JFDK_RAMP_FP32_SIMT)
+                return fail(c, JFDK_ERR_INVALID, "unknown ramp product");
+            c->opt_ramp = (int)value;
+            return JFDK_OK;
         case JFDK_OPT_STAGE_TIMING:
             if (value && !c->ev[0])
                 for (auto& e : c->ev) JFDK_CUDA(c, cudaEventCreate(&e), "cudaEventCreate");
@@ -439,7 +512,7 @@ jfdk_status jfdk_filter_frames(jfdk_ctx* c, const float* d_in, int v0, int nv, f
     if (nv == 0) return JFDK_OK;
     jfdk_status st = ensure_A(c, (size_t)nv * c->rows);
     if (st) return st;
-    JFDK_LAUNCH(c, launch_weight(d_in, nv, v0, c->in_w, c->rows, weight_params(c), c->d_A, a_pitch(c), c->d_e, c->stream),
+    JFDK_LAUNCH(c, launch_weight(d_in, nv, v0, c->in_w, c->rows, weight_params(c), a_operand(c), c->d_e, c->stream),
                 "pre-weight");
     JFDK_LAUNCH(c, launch_ramp(c, ramp_params(c, nv, d_out)), "ramp filter");
     return JFDK_OK;
@@ -513,8 +586,8 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, in
     // buffers) -> [z-filter] -> tapered quads of the whole rotation
     for (int v0 = 0; v0 < c->nviews; v0 += chunk) {
         const int nv = std::min(chunk, c->nviews - v0);
-        JFDK_LAUNCH(c, launch_prep_weight(prep_params(c, d_raw + (size_t)v0 * frame), nv, v0, weight_params(c), c->d_A,
-                                          a_pitch(c), c->d_e, c->stream),
+        JFDK_LAUNCH(c, launch_prep_weight(prep_params(c, d_raw + (size_t)v0 * frame), nv, v0, weight_params(c),
+                                          a_operand(c), c->d_e, c->stream),
                     "preprocess + pre-weight");
         JFDK_LAUNCH(c, launch_ramp(c, ramp_params(c, nv, c->d_plain)), "ramp filter");
         if (c->recon.z_filter)

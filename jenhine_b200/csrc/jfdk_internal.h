@@ -93,13 +93,22 @@ struct WeightParams {
     int mirror;
 };
 cudaError_t launch_preprocess(const PrepParams& p, int nv, float* out, cudaStream_t s);
+
+// The ramp product's A operand as the weight kernels write it.
+enum AOutKind { AOUT_F32 = 0, AOUT_TF32X2 = 1, AOUT_BF16X2 = 2, AOUT_FP16X2 = 3 };
+struct AOperand {
+    int kind;             // AOutKind
+    void* hi;             // [M][pitch]: fp32 (F32, TF32X2) or 16-bit values
+    void* lo;             // low parts (split kinds)
+    float* row_scale;     // FP16X2: [M] 1 / the row's power-of-two scale
+    int pitch;            // elements per row (K padded)
+};
 // Pre-weight + edge mean of frames already preprocessed (agent path).
-cudaError_t launch_weight(const float* in, int nv, int v0, int width, int rows,
-                          const WeightParams& w, float* A, int a_pitch, float* e,
-                          cudaStream_t s);
+cudaError_t launch_weight(const float* in, int nv, int v0, int width, int rows, const WeightParams& w,
+                          const AOperand& A, float* e, cudaStream_t s);
 // Raw -> weighted A operand + edge means in one pass (whole-volume path).
-cudaError_t launch_prep_weight(const PrepParams& p, int nv, int v0, const WeightParams& w,
-                               float* A, int a_pitch, float* e, cudaStream_t s);
+cudaError_t launch_prep_weight(const PrepParams& p, int nv, int v0, const WeightParams& w, const AOperand& A,
+                               float* e, cudaStream_t s);
 // Frame minimum of the pre-weight distance per group.
 cudaError_t launch_preweight_dmin(const float* tinv, int groups, int rows, int L,
                                   int in_w, int det_right, float* dmin, cudaStream_t s);
@@ -114,13 +123,18 @@ struct RampParams {
     float* q;                // output frames, row r of view f at q + f * q_frame_stride + r * q_pitch
     long long q_frame_stride;
     int q_pitch;
+    const float* row_scale;  // tensor-core FP16X3: [M] row factors, else null
+    float b_scale;           // tensor-core FP16X3: 1 / the operator's scale, else 1
+    int vec_store;           // q rows 16-byte aligned: store float4s
 };
 cudaError_t launch_ramp_gemm(const RampParams& p, cudaStream_t s);
-// Tensor-core form (ramp_gemm_tc.cu): B split into TF32-exact parts Bh, Bl
-// ([N][a_pitch]); a_pitch must be a multiple of 32.  A timed-out pipeline wait
-// sets *status (device word) and the CTA skips the rest of its work.
-cudaError_t launch_ramp_gemm_tc(const RampParams& p, const float* Bh, const float* Bl, int* status,
-                                cudaStream_t s);
+// Tensor-core split products (ramp_gemm_tc.cu).
+enum RampKind { RAMP_TF32X3 = 0, RAMP_BF16X3 = 1, RAMP_FP16X3 = 2 };
+// Ah, Al [M][a_pitch] and Bh, Bl [N][a_pitch] in the kind's element type;
+// a_pitch a multiple of 32 (TF32X3) or 64.  A timed-out pipeline wait sets
+// *status (device word) and the CTA skips the rest of its work.
+cudaError_t launch_ramp_gemm_tc(const RampParams& p, int kind, const void* Ah, const void* Al, const void* Bh,
+                                const void* Bl, int* status, cudaStream_t s);
 float tf32_round_host(float x);
 
 cudaError_t launch_zfilter(float* frames, int nv, int rows, int width, long long frame_stride,
@@ -160,11 +174,15 @@ struct jfdk_ctx {
     float* d_T = nullptr;
     float* d_Th = nullptr;       // TF32-exact split of the ramp operator
     float* d_Tl = nullptr;
+    uint16_t* d_Tb = nullptr;    // BF16 split: [2][out_w][a_pitch] (high, low)
+    uint16_t* d_Tf = nullptr;    // FP16 split of the scaled operator (high, low)
+    float tf_inv_scale = 1.0f;   // 1 / the FP16 operator's scale
     float* d_c = nullptr;
     int* d_status = nullptr;     // nonzero: a kernel's bounded wait gave up
 
     // device working storage (allocated on demand)
-    float* d_A = nullptr;  size_t a_rows = 0;   // weighted rows, pitch a_pitch
+    void* d_A = nullptr;  size_t a_rows = 0;    // weighted rows: high then low part, pitch a_pitch
+    float* d_arow = nullptr;                     // FP16X3: per-row factors
     float* d_e = nullptr;
     float* d_plain = nullptr; int plain_views = 0;  // filtered frames of one chunk
     float4* d_q4 = nullptr; int q4_views = 0;       // quad store (mixed: uint4 records)
@@ -181,7 +199,7 @@ struct jfdk_ctx {
     int opt_view_chunk = 32;
     int opt_stage_timing = 0;
     int opt_bp_zpt = 0;          // 0: default (bp_zpt() in jfdk_api.cpp)
-    int opt_filter_simt = 0;     // 1: ramp product on FP32 CUDA cores instead of tcgen05
+    int opt_ramp = 0;            // JFDK_OPT_RAMP_PRODUCT (0: the form's default)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
     long long launches = 0;

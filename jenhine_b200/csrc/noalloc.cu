@@ -66,7 +66,7 @@ extern "C" jfdk_status jfdk_filter_frames_noalloc(jfdk_ctx* c, const float* d_in
         return JFDK_ERR_INVALID;
     }
     if (nv == 0) return JFDK_OK;
-    const size_t pitch = (size_t)(c->in_w + 15) / 16 * 16;       // the row pitch jfdk_filter_frames uses
+    const size_t pitch = (size_t)(c->in_w + 63) / 64 * 64;       // the row pitch of the context's ramp operator
     const size_t rows = (size_t)nv * c->rows;
     const size_t edge_off = (rows * pitch + 63) / 64 * 64;          // 256-byte aligned
     if (edge_off + rows > kScratchFloats) {
@@ -94,7 +94,11 @@ extern "C" jfdk_status jfdk_filter_frames_noalloc(jfdk_ctx* c, const float* d_in
     w.L = c->L;
     w.det_right = c->mirror;
     w.mirror = c->mirror;
-    e = jfdk::launch_weight(d_in, nv, v0, c->in_w, c->rows, w, A, (int)pitch, edge, c->stream);
+    jfdk::AOperand a{};
+    a.kind = jfdk::AOUT_F32;
+    a.hi = A;
+    a.pitch = (int)pitch;
+    e = jfdk::launch_weight(d_in, nv, v0, c->in_w, c->rows, w, a, edge, c->stream);
     if (e != cudaSuccess) {
         c->err = std::string("filter_frames_noalloc: pre-weight: ") + cudaGetErrorString(e);
         return JFDK_ERR_CUDA;
@@ -106,6 +110,7 @@ extern "C" jfdk_status jfdk_filter_frames_noalloc(jfdk_ctx* c, const float* d_in
     r.M = nv * c->rows; r.N = c->out_w; r.K = c->in_w; r.a_pitch = (int)pitch;
     r.rows = c->rows;
     r.q = d_out; r.q_frame_stride = (long long)c->rows * c->out_w; r.q_pitch = c->out_w;
+    r.b_scale = 1.0f;
     e = jfdk::launch_ramp_gemm(r, c->stream);
     if (e != cudaSuccess) {
         c->err = std::string("filter_frames_noalloc: ramp filter: ") + cudaGetErrorString(e);

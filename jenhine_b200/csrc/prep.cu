@@ -17,6 +17,8 @@
 //   FilterCore::ProcessRow edge mean    FilterAgent/FilterCore.cpp:201-214
 // The float expressions are written with explicit _rn intrinsics so no FMA
 // contraction changes their rounding relative to the reference.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -114,55 +116,146 @@ __global__ void __launch_bounds__(256) preprocess_kernel(PrepParams P, float* __
 }
 
 // ---- pre-weight + edge mean of a preprocessed row --------------------------
-template <bool FROM_RAW>
+// The weighted row goes out as the ramp product's A operand in the form the
+// product reads (AOut): fp32, or split into a high and a low part -- tf32
+// (fp32 storage), bf16, or fp16 of the row scaled by a power of two so its
+// largest value lies in [2^14, 2^15) (row_scale[m] = 1 / that factor).
+
+// Round to the nearest TF32 value (10 explicit mantissa bits, ties to even).
+__device__ __forceinline__ float tf32_rn(float x) {
+    uint32_t b = __float_as_uint(x);
+    if ((b & 0x7f800000u) != 0x7f800000u) b = (b + 0xfffu + ((b >> 13) & 1u)) & 0xffffe000u;
+    return __uint_as_float(b);
+}
+
+template <int OUT>
+__device__ __forceinline__ void store4(void* hi, void* lo, size_t at, const float v[4]) {
+    if constexpr (OUT == AOUT_F32) {
+        *reinterpret_cast<float4*>(static_cast<float*>(hi) + at) = make_float4(v[0], v[1], v[2], v[3]);
+    } else if constexpr (OUT == AOUT_TF32X2) {
+        float h[4], l[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { h[k] = tf32_rn(v[k]); l[k] = tf32_rn(v[k] - h[k]); }
+        *reinterpret_cast<float4*>(static_cast<float*>(hi) + at) = make_float4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<float4*>(static_cast<float*>(lo) + at) = make_float4(l[0], l[1], l[2], l[3]);
+    } else if constexpr (OUT == AOUT_BF16X2) {
+        __nv_bfloat162 h[2], l[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            h[k] = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+            const float2 hf = __bfloat1622float2(h[k]);
+            l[k] = __floats2bfloat162_rn(v[2 * k] - hf.x, v[2 * k + 1] - hf.y);
+        }
+        *reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(hi) + at) = *reinterpret_cast<uint2*>(h);
+        *reinterpret_cast<uint2*>(static_cast<__nv_bfloat16*>(lo) + at) = *reinterpret_cast<uint2*>(l);
+    } else {
+        __half2 h[2], l[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            h[k] = __floats2half2_rn(v[2 * k], v[2 * k + 1]);
+            const float2 hf = __half22float2(h[k]);
+            l[k] = __floats2half2_rn(v[2 * k] - hf.x, v[2 * k + 1] - hf.y);
+        }
+        *reinterpret_cast<uint2*>(static_cast<__half*>(hi) + at) = *reinterpret_cast<uint2*>(h);
+        *reinterpret_cast<uint2*>(static_cast<__half*>(lo) + at) = *reinterpret_cast<uint2*>(l);
+    }
+}
+
+template <int OUT>
+__device__ __forceinline__ void store1(void* hi, void* lo, size_t at, float v) {
+    if constexpr (OUT == AOUT_F32) {
+        static_cast<float*>(hi)[at] = v;
+    } else if constexpr (OUT == AOUT_TF32X2) {
+        const float h = tf32_rn(v);
+        static_cast<float*>(hi)[at] = h;
+        static_cast<float*>(lo)[at] = tf32_rn(v - h);
+    } else if constexpr (OUT == AOUT_BF16X2) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        static_cast<__nv_bfloat16*>(hi)[at] = h;
+        static_cast<__nv_bfloat16*>(lo)[at] = __float2bfloat16_rn(v - __bfloat162float(h));
+    } else {
+        const __half h = __float2half_rn(v);
+        static_cast<__half*>(hi)[at] = h;
+        static_cast<__half*>(lo)[at] = __float2half_rn(v - __half2float(h));
+    }
+}
+
+template <bool FROM_RAW, int OUT>
 __global__ void __launch_bounds__(256) weight_kernel(PrepParams P, const float* __restrict__ in,
                                                      int width, int rows, int v0, WeightParams W,
-                                                     float* __restrict__ A, int a_pitch,
-                                                     float* __restrict__ e) {
+                                                     AOperand A, float* __restrict__ e) {
     const int row = blockIdx.x, vl = blockIdx.y;
     const int view = (v0 + vl) % W.num_views;
     const int g = view / 9;
     __shared__ float T[16];
+    __shared__ float red[8];
     if (threadIdx.x < 16) T[threadIdx.x] = W.tinv[g * 16 + threadIdx.x];
     __syncthreads();
     const float dmin = W.dmin[g];
     const PWRow r = pw_row(T, (float)row);
     const size_t m = (size_t)vl * rows + row;
-    float* a = A + m * a_pitch;
+    const size_t a0 = m * A.pitch;
     const uint16_t* src = FROM_RAW ? P.raw + ((size_t)vl * P.in_h + row + P.crop_y) * P.in_w + P.crop_x
                                    : nullptr;
     const float* fin = FROM_RAW ? nullptr : in + m * width;
     auto pix = [&](int i) -> float { return FROM_RAW ? prep_pixel((float)src[i], P) : fin[i]; };
+    auto value = [&](int i, float p) -> float {
+        return __fmul_rn(p, __fdiv_rn(dmin, pw_dist(r, u_axis(i, width, W.det_right))));
+    };
+    const int elem = OUT == AOUT_F32 || OUT == AOUT_TF32X2 ? 4 : 2;
     const bool vec = FROM_RAW && ((reinterpret_cast<uintptr_t>(P.raw) & 7) == 0) &&
-                     ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && ((P.crop_x & 3) == 0) &&
-                     ((P.in_w & 3) == 0) && ((width & 3) == 0) && ((a_pitch & 3) == 0);
+                     ((reinterpret_cast<uintptr_t>(A.hi) & 15) == 0) &&
+                     (OUT == AOUT_F32 || (reinterpret_cast<uintptr_t>(A.lo) & 15) == 0) &&
+                     ((P.crop_x & 3) == 0) && ((P.in_w & 3) == 0) && ((width & 3) == 0) &&
+                     (((size_t)A.pitch * elem) % 16 == 0);
+    // fp16: the row's largest magnitude sets its power-of-two scale first
+    float scale = 1.0f;
+    if (OUT == AOUT_FP16X2) {
+        float mx = 0.0f;
+        for (int i = threadIdx.x; i < width; i += blockDim.x) mx = fmaxf(mx, fabsf(value(i, pix(i))));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+        __syncthreads();
+        mx = red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mx = fmaxf(mx, red[w]);
+        scale = (mx > 0.0f && mx <= 3.0e38f) ? ldexpf(1.0f, 14 - ilogbf(mx)) : 1.0f;
+        if (threadIdx.x == 0) A.row_scale[m] = __fdiv_rn(1.0f, scale);
+    }
     if (vec) {
         for (int i4 = threadIdx.x * 4; i4 < width; i4 += blockDim.x * 4) {
             const uint2 raw4 = *reinterpret_cast<const uint2*>(src + i4);
-            float p[4] = {(float)(raw4.x & 0xffffu), (float)(raw4.x >> 16), (float)(raw4.y & 0xffffu),
-                          (float)(raw4.y >> 16)};
-            float4 o;
-            float* op = &o.x;
+            const float p[4] = {(float)(raw4.x & 0xffffu), (float)(raw4.x >> 16), (float)(raw4.y & 0xffffu),
+                                (float)(raw4.y >> 16)};
+            float o[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const float pw = __fdiv_rn(dmin, pw_dist(r, u_axis(i4 + k, width, W.det_right)));
-                op[k] = __fmul_rn(prep_pixel(p[k], P), pw);
-            }
-            *reinterpret_cast<float4*>(a + i4) = o;
+            for (int k = 0; k < 4; ++k) o[k] = value(i4 + k, prep_pixel(p[k], P)) * scale;
+            store4<OUT>(A.hi, A.lo, a0 + i4, o);
         }
     } else {
-        for (int i = threadIdx.x; i < width; i += blockDim.x) {
-            const float pw = __fdiv_rn(dmin, pw_dist(r, u_axis(i, width, W.det_right)));
-            a[i] = __fmul_rn(pix(i), pw);
-        }
+        for (int i = threadIdx.x; i < width; i += blockDim.x) store1<OUT>(A.hi, A.lo, a0 + i, value(i, pix(i)) * scale);
     }
-    for (int i = width + threadIdx.x; i < a_pitch; i += blockDim.x) a[i] = 0.0f;
+    for (int i = width + threadIdx.x; i < A.pitch; i += blockDim.x) store1<OUT>(A.hi, A.lo, a0 + i, 0.0f);
     if (threadIdx.x == 0) {
         // FilterCore.cpp:203-214 -- mean of the three outermost unweighted samples
         const float edge = W.mirror ? __fdiv_rn(__fadd_rn(__fadd_rn(pix(width - 1), pix(width - 2)), pix(width - 3)), 3.0f)
                                     : __fdiv_rn(__fadd_rn(__fadd_rn(pix(0), pix(1)), pix(2)), 3.0f);
         e[m] = edge;
     }
+}
+
+template <bool FROM_RAW>
+cudaError_t launch_weight_t(const PrepParams& p, const float* in, int nv, int v0, int width, int rows,
+                            const WeightParams& w, const AOperand& A, float* e, int threads, cudaStream_t s) {
+    const dim3 grid(rows, nv);
+    switch (A.kind) {
+        case AOUT_F32: weight_kernel<FROM_RAW, AOUT_F32><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e); break;
+        case AOUT_TF32X2: weight_kernel<FROM_RAW, AOUT_TF32X2><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e); break;
+        case AOUT_BF16X2: weight_kernel<FROM_RAW, AOUT_BF16X2><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e); break;
+        case AOUT_FP16X2: weight_kernel<FROM_RAW, AOUT_FP16X2><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -181,16 +274,14 @@ cudaError_t launch_preprocess(const PrepParams& p, int nv, float* out, cudaStrea
 }
 
 cudaError_t launch_weight(const float* in, int nv, int v0, int width, int rows, const WeightParams& w,
-                          float* A, int a_pitch, float* e, cudaStream_t s) {
+                          const AOperand& A, float* e, cudaStream_t s) {
     PrepParams p{};
-    weight_kernel<false><<<dim3(rows, nv), 256, 0, s>>>(p, in, width, rows, v0, w, A, a_pitch, e);
-    return cudaGetLastError();
+    return launch_weight_t<false>(p, in, nv, v0, width, rows, w, A, e, 256, s);
 }
 
-cudaError_t launch_prep_weight(const PrepParams& p, int nv, int v0, const WeightParams& w, float* A,
-                               int a_pitch, float* e, cudaStream_t s) {
-    weight_kernel<true><<<dim3(p.rows, nv), 192, 0, s>>>(p, nullptr, p.width, p.rows, v0, w, A, a_pitch, e);
-    return cudaGetLastError();
+cudaError_t launch_prep_weight(const PrepParams& p, int nv, int v0, const WeightParams& w, const AOperand& A,
+                               float* e, cudaStream_t s) {
+    return launch_weight_t<true>(p, nullptr, nv, v0, p.width, p.rows, w, A, e, 192, s);
 }
 
 }  // namespace jfdk

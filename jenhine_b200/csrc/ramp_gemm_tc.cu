@@ -1,23 +1,30 @@
 // ramp_gemm_tc.cu -- the ramp filter product Q = A T^T + e c^T on the 5th
-// generation tensor cores (tcgen05, sm_100a).
+// generation tensor cores (tcgen05, sm_100a), as a split-precision product.
 //
-// Operands (all K-major, K = filter input columns padded to 32):
-//   A  [M][Kp] fp32  weighted detector rows (prep.cu), loaded by TMA;
-//   Bh [N][Kp], Bl [N][Kp]  the Toeplitz operator split on the host into two
-//      TF32-exact parts (Bh = RN_tf32(T), Bl = RN_tf32(T - Bh)).
-// FP32-class accuracy from TF32 tensor cores: each A tile is split in shared
-// memory into Ah = RN_tf32(A) and Al = RN_tf32(A - Ah) and the CTA issues
-// Ah*Bh + Ah*Bl + Al*Bh (the dropped Al*Bl term is ~2^-22 relative), all
-// accumulated in FP32 in tensor memory.
+// Operands (all K-major, K = filter input columns padded to a multiple of 64):
+//   Ah, Al [M][Kp]  the weighted detector rows split into a high and a low
+//                   part by the producing kernel (prep.cu);
+//   Bh, Bl [N][Kp]  the Toeplitz operator split the same way on the host.
+// The CTA accumulates Ah*Bh + Ah*Bl + Al*Bh in FP32 in tensor memory (the
+// dropped Al*Bl term is below the split's precision).  Element kinds:
+//   TF32x3  tf32 parts in fp32 storage, kind::tf32 -- ~2^-22 relative, the
+//           FP32 form's product;
+//   BF16x3  bf16 parts, kind::f16 -- ~2^-17 relative, twice the MMA rate;
+//   FP16x3  fp16 parts of rows scaled by a power of two per row (row_scale)
+//           and of the operator scaled by b_scale, kind::f16 -- ~2^-22
+//           relative at the bf16 rate; the epilogue undoes both scales.
 //
-// Tile 128 x 128 per CTA, K in blocks of 32 (one 128-byte swizzle atom per
-// row), 3-stage TMA / mbarrier pipeline.  Thread 0 issues TMA and MMA; all four
-// warps split A and, after the last MMA, read the accumulator out of tensor
-// memory (warp w owns TMEM lanes 32w..32w+31 = tile rows) and store rows of Q
-// with the rank-1 truncation-ramp term c[n] e[m] added.
-//
-// Every mbarrier wait is bounded: on timeout the CTA records a code in the
-// context's device status word and skips the rest of its work (no trap).
+// Persistent, warp-specialised CTA of 6 warps, one CTA per SM:
+//   warp 0       TMA producer: 4 tiles per K block into a 3-stage ring;
+//   warp 1       owns the tensor memory; one thread issues the MMAs of a tile
+//                into one of two 128-column accumulators;
+//   warps 2..5   epilogue: read their 32 accumulator lanes (tile rows) with
+//                tcgen05.ld, add c[n] e[m], store rows of Q -- overlapping the
+//                next tile's MMAs in the other accumulator.
+// Every mbarrier wait is bounded: on timeout the CTA raises a shared abort
+// flag and records a code in the context's device status word; every role
+// then stops waiting, the MMA thread drains its MMAs, the producer waits
+// (bounded) for its copies in flight, and the tensor memory is freed.
 // TMA loads never use cluster multicast and read only this GPU's memory.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -31,13 +38,12 @@
 namespace jfdk {
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3;
-constexpr int TILE_A = BM * BK * 4;          // 16 KB
-constexpr int TILE_B = BN * BK * 4;          // 16 KB
-constexpr int STAGE_BYTES = 2 * TILE_A + 2 * TILE_B;  // A, Al, Bh, Bl
+constexpr int BM = 128, BN = 128, STAGES = 3;
+constexpr int TILE = 128 * 128;                       // bytes: 128 rows x 128 bytes of K
+constexpr int STAGE_BYTES = 4 * TILE;                 // Ah, Al, Bh, Bl
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr uint32_t TX_BYTES = TILE_A + 2 * TILE_B;   // bytes TMA delivers per stage
-constexpr uint32_t kWaitLimit = 1u << 22;           // polls before a wait gives up
+constexpr uint32_t kWaitLimit = 1u << 22;            // polls before a wait gives up
+constexpr int kThreads = 192;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -51,8 +57,13 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-// Bounded parity wait: true when the phase with parity `parity` completed.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Bounded parity wait: true when the phase with parity `parity` completed;
+// false when it gave up or another role already aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
     for (uint32_t i = 0; i < kWaitLimit; ++i) {
         uint32_t done;
         asm volatile(
@@ -61,7 +72,9 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
             : "r"(bar), "r"(parity)
             : "memory");
         if (done) return true;
+        if ((i & 255u) == 255u && *abort_flag) return false;
     }
+    *abort_flag = 1;
     return false;
 }
 
@@ -72,34 +85,35 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-// K-major operand tile of `rows` x 128 bytes, 128-byte swizzle, 8-row atoms
+// K-major operand tile of 128 rows x 128 bytes, 128-byte swizzle, 8-row atoms
 // 1024 bytes apart (Blackwell shared-memory matrix descriptor, version 1).
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
     return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
            ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
-// Instruction descriptor: kind::tf32, D = F32, A = B = TF32, both K-major,
-// M = 128, N = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                            ((uint32_t)(BM >> 4) << 24);
+// Instruction descriptor: D = F32, A/B type, both K-major, M = 128, N = 128.
+constexpr uint32_t idesc(uint32_t ab_type) {
+    return (1u << 4) | (ab_type << 7) | (ab_type << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-        " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}"
-        ::"r"(tmem_d), "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate));
+template <int KIND>
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    if constexpr (KIND == RAMP_TF32X3) {
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}"
+            ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc(2)), "r"(accumulate));
+    } else {
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}"
+            ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc(KIND == RAMP_BF16X3 ? 1u : 0u)), "r"(accumulate));
+    }
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-// Round to the nearest TF32 value (10 explicit mantissa bits, ties to even).
-__device__ __forceinline__ float tf32_rn(float x) {
-    uint32_t b = __float_as_uint(x);
-    if ((b & 0x7f800000u) != 0x7f800000u) b = (b + 0xfffu + ((b >> 13) & 1u)) & 0xffffe000u;
-    return __uint_as_float(b);
 }
 
 struct TcArgs {
@@ -107,133 +121,164 @@ struct TcArgs {
     int* status;
 };
 
-__global__ void __launch_bounds__(128, 1) ramp_gemm_tc_kernel(const __grid_constant__ CUtensorMap mapA,
-                                                             const __grid_constant__ CUtensorMap mapBh,
-                                                             const __grid_constant__ CUtensorMap mapBl,
-                                                             TcArgs args) {
+template <int KIND>
+__global__ void __launch_bounds__(kThreads, 1) ramp_tc_kernel(const __grid_constant__ CUtensorMap mapAh,
+                                                              const __grid_constant__ CUtensorMap mapAl,
+                                                              const __grid_constant__ CUtensorMap mapBh,
+                                                              const __grid_constant__ CUtensorMap mapBl,
+                                                              TcArgs args) {
+    constexpr int ELEM = KIND == RAMP_TF32X3 ? 4 : 2;
+    constexpr int BK = 128 / ELEM;          // K elements per 128-byte row
+    constexpr int KSTEPS = 128 / 32;        // MMAs per K block: 32 bytes of K each
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const RampParams& p = args.p;
     const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;     // 1024-aligned for SW128
     uint8_t* gbase = smem_raw + (base - smem_u32(smem_raw));
-    // barrier block after the stages
     const uint32_t bars = base + STAGES * STAGE_BYTES;
     auto full = [&](int s) { return bars + 8u * s; };
     auto empty = [&](int s) { return bars + 8u * (STAGES + s); };
-    const uint32_t done_bar = bars + 8u * (2 * STAGES);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + STAGES * STAGE_BYTES + 8 * (2 * STAGES + 1));
+    auto tfull = [&](int b) { return bars + 8u * (2 * STAGES + b); };
+    auto tempty = [&](int b) { return bars + 8u * (2 * STAGES + 2 + b); };
+    const uint32_t drain_bar = bars + 8u * (2 * STAGES + 4);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gbase + STAGES * STAGE_BYTES + 8 * (2 * STAGES + 5));
     __shared__ int abort_flag;
+    volatile int* abort_v = &abort_flag;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
     const int nk = p.a_pitch / BK;
+    const int tiles_n = (p.N + BN - 1) / BN, tiles = ((p.M + BM - 1) / BM) * tiles_n;
 
     if (tid == 0) {
         abort_flag = 0;
         for (int s = 0; s < STAGES; ++s) { mbar_init(full(s), 1); mbar_init(empty(s), 1); }
-        mbar_init(done_bar, 1);
+        for (int b = 0; b < 2; ++b) { mbar_init(tfull(b), 1); mbar_init(tempty(b), 4); }
+        mbar_init(drain_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&mapA)) : "memory");
     }
-    if (warp == 0) {  // 128 TMEM columns hold the 128 x 128 FP32 accumulator
+    if (warp == 1) {  // two 128-column FP32 accumulators
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     ::"r"(smem_u32(tmem_slot)), "r"(128));
+                     ::"r"(smem_u32(tmem_slot)), "r"(2 * BN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
+    auto stage = [&](int s, int t) { return base + (uint32_t)(s * STAGE_BYTES + t * TILE); };
 
-    auto stageA = [&](int s) { return base + (uint32_t)(s * STAGE_BYTES); };
-    auto stageAl = [&](int s) { return stageA(s) + TILE_A; };
-    auto stageBh = [&](int s) { return stageA(s) + 2 * TILE_A; };
-    auto stageBl = [&](int s) { return stageA(s) + 2 * TILE_A + TILE_B; };
-    auto load_stage = [&](int kb, int s) {
-        mbar_expect_tx(full(s), TX_BYTES);
-        tma_load_2d(stageA(s), &mapA, kb * BK, m0, full(s));
-        tma_load_2d(stageBh(s), &mapBh, kb * BK, n0, full(s));
-        tma_load_2d(stageBl(s), &mapBl, kb * BK, n0, full(s));
-    };
-
-    if (tid == 0)
-        for (int kb = 0; kb < nk && kb < STAGES; ++kb) load_stage(kb, kb);
-
-    for (int kb = 0; kb < nk; ++kb) {
-        const int s = kb % STAGES;
-        const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
-        if (!abort_flag && !mbar_wait(full(s), ph)) abort_flag = 1;
-        // Split A into RN_tf32(A) (in place) and RN_tf32(A - that).  The
-        // swizzle permutes 16-byte chunks within the tile, so an elementwise
-        // pass keeps both tiles in the layout the descriptors describe.
-        if (!abort_flag) {
-            float4* a = reinterpret_cast<float4*>(gbase + s * STAGE_BYTES);
-            float4* al = reinterpret_cast<float4*>(gbase + s * STAGE_BYTES + TILE_A);
-#pragma unroll 4
-            for (int i = tid; i < TILE_A / 16; i += 128) {
-                float4 v = a[i], h, l;
-                h.x = tf32_rn(v.x); h.y = tf32_rn(v.y); h.z = tf32_rn(v.z); h.w = tf32_rn(v.w);
-                l.x = tf32_rn(v.x - h.x); l.y = tf32_rn(v.y - h.y); l.z = tf32_rn(v.z - h.z); l.w = tf32_rn(v.w - h.w);
-                a[i] = h;
-                al[i] = l;
+    if (warp == 0) {
+        // ---- TMA producer ----
+        if (lane == 0) {
+            uint32_t it = 0;
+            for (int t = blockIdx.x; t < tiles && !*abort_v; t += gridDim.x) {
+                const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+                for (int kb = 0; kb < nk; ++kb, ++it) {
+                    const int s = (int)(it % STAGES);
+                    if (it >= STAGES && !mbar_wait(empty(s), ((it / STAGES) - 1) & 1u, abort_v)) break;
+                    mbar_expect_tx(full(s), STAGE_BYTES);
+                    tma_load_2d(stage(s, 0), &mapAh, kb * BK, m0, full(s));
+                    tma_load_2d(stage(s, 1), &mapAl, kb * BK, m0, full(s));
+                    tma_load_2d(stage(s, 2), &mapBh, kb * BK, n0, full(s));
+                    tma_load_2d(stage(s, 3), &mapBl, kb * BK, n0, full(s));
+                }
+            }
+            // copies still in flight land before the CTA exits (bounded)
+            if (*abort_v) {
+                const uint32_t first = it > STAGES ? it - STAGES : 0;
+                for (uint32_t j = first; j < it; ++j) {
+                    int dummy = 0;
+                    mbar_wait(full((int)(j % STAGES)), (j / STAGES) & 1u, &dummy);
+                }
             }
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0 && !abort_flag) {
+    } else if (warp == 1) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            uint32_t it = 0, i = 0;
+            for (int t = blockIdx.x; t < tiles && !*abort_v; t += gridDim.x, ++i) {
+                const int b = (int)(i & 1u);
+                if (i >= 2 && !mbar_wait(tempty(b), ((i >> 1) - 1) & 1u, abort_v)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)(b * BN);
+                bool ok = true;
+                for (int kb = 0; kb < nk; ++kb, ++it) {
+                    const int s = (int)(it % STAGES);
+                    if (!mbar_wait(full(s), (it / STAGES) & 1u, abort_v)) { ok = false; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+                    for (int k = 0; k < KSTEPS; ++k) {
+                        const uint32_t off = (uint32_t)k * 32u;
+                        const uint64_t dah = smem_desc(stage(s, 0) + off), dal = smem_desc(stage(s, 1) + off);
+                        const uint64_t dbh = smem_desc(stage(s, 2) + off), dbl = smem_desc(stage(s, 3) + off);
+                        mma<KIND>(acc, dah, dbh, (kb > 0 || k > 0) ? 1u : 0u);
+                        mma<KIND>(acc, dah, dbl, 1u);
+                        mma<KIND>(acc, dal, dbh, 1u);
+                    }
+                    mma_commit(empty(s));
+                }
+                if (!ok) break;
+                mma_commit(tfull(b));
+            }
+            // all issued MMAs complete before the tensor memory is freed
+            mma_commit(drain_bar);
+            int dummy = 0;
+            mbar_wait(drain_bar, 0, &dummy);
+        }
+    } else {
+        // ---- epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 ----
+        const int quarter = warp & 3;
+        uint32_t i = 0;
+        for (int t = blockIdx.x; t < tiles && !*abort_v; t += gridDim.x, ++i) {
+            const int b = (int)(i & 1u);
+            if (!mbar_wait(tfull(b), (i >> 1) & 1u, abort_v)) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-            for (int k = 0; k < BK / 8; ++k) {  // kind::tf32: K = 8 per MMA (32 bytes)
-                const uint32_t off = (uint32_t)k * 32u;
-                const uint64_t da = smem_desc(stageA(s) + off), dal = smem_desc(stageAl(s) + off);
-                const uint64_t dbh = smem_desc(stageBh(s) + off), dbl = smem_desc(stageBl(s) + off);
-                mma_tf32(tmem, da, dbh, (kb > 0 || k > 0) ? 1u : 0u);
-                mma_tf32(tmem, da, dbl, 1u);
-                mma_tf32(tmem, dal, dbh, 1u);
+            const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
+            const int m = m0 + quarter * 32 + lane;
+            const bool row_ok = m < p.M;
+            float em = 0.0f, rs = 1.0f;
+            float* qrow = nullptr;
+            if (row_ok) {
+                em = p.e[m];
+                if (p.row_scale) rs = p.row_scale[m] * p.b_scale;
+                const int vl = m / p.rows, row = m - vl * p.rows;
+                qrow = p.q + (size_t)vl * p.q_frame_stride + (size_t)row * p.q_pitch;
             }
-            mma_commit(empty(s));
-            // refill the stage used one iteration ago (its MMAs overlap ours)
-            if (kb >= 1 && kb - 1 + STAGES < nk) {
-                const int sp = (kb - 1) % STAGES;
-                if (!mbar_wait(empty(sp), (uint32_t)((kb - 1) / STAGES) & 1u)) abort_flag = 1;
-                else load_stage(kb - 1 + STAGES, sp);
-            }
-        }
-    }
-    if (tid == 0) mma_commit(done_bar);
-    __syncthreads();
-    if (!abort_flag && !mbar_wait(done_bar, 0)) abort_flag = 1;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-
-    // Epilogue: warp w holds tile rows 32w + lane.
-    const int m = m0 + warp * 32 + lane;
-    const bool row_ok = m < p.M && !abort_flag;
-    const float em = row_ok ? p.e[m] : 0.0f;
-    float* qrow = nullptr;
-    if (row_ok) {
-        const int vl = m / p.rows, row = m - vl * p.rows;
-        qrow = p.q + (size_t)vl * p.q_frame_stride + (size_t)row * p.q_pitch;
-    }
 #pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 16) {
-        uint32_t r[16];
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (row_ok) {
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                uint32_t r[16];
+                const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * BN + c0);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                      "=r"(r[15])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                const int n = n0 + c0;
+                if (row_ok && n < p.N) {
+                    float o[16];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int n = n0 + c0 + j;
-                if (n < p.N) qrow[n] = fmaf(__ldg(p.c + n), em, __uint_as_float(r[j]));
+                    for (int j = 0; j < 16; ++j)
+                        o[j] = fmaf(__ldg(p.c + (n + j < p.N ? n + j : p.N - 1)), em, __uint_as_float(r[j]) * rs);
+                    if (p.vec_store && n + 16 <= p.N) {
+                        float4* d = reinterpret_cast<float4*>(qrow + n);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) d[j] = make_float4(o[4 * j], o[4 * j + 1], o[4 * j + 2], o[4 * j + 3]);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                            if (n + j < p.N) qrow[n + j] = o[j];
+                    }
+                }
             }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty(b));
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+    if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN));
     if (tid == 0 && abort_flag) atomicOr(args.status, 1);
 }
 
@@ -256,16 +301,52 @@ EncodeFn encoder() {
     return fn;
 }
 
-bool make_map(CUtensorMap* map, const float* ptr, int rows, int cols_padded, int box_rows) {
+// rows x cols (elements) K-major matrix; box = 128 bytes of K x 128 rows.
+bool make_map(CUtensorMap* map, const void* ptr, int kind, int rows, int cols) {
     EncodeFn enc = encoder();
     if (!enc) return false;
-    const cuuint64_t dims[2] = {(cuuint64_t)cols_padded, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)cols_padded * 4};
-    const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    const int elem = kind == RAMP_TF32X3 ? 4 : 2;
+    const CUtensorMapDataType dt = kind == RAMP_TF32X3   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : kind == RAMP_BF16X3 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)cols * elem};
+    const cuuint32_t box[2] = {(cuuint32_t)(128 / elem), 128u};
     const cuuint32_t estr[2] = {1, 1};
-    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(ptr), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+    return enc(map, dt, 2, const_cast<void*>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int sm_count() {
+    static int n = 0;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+    });
+    return n;
+}
+
+template <int KIND>
+cudaError_t launch_kind(const RampParams& p, const void* Ah, const void* Al, const void* Bh, const void* Bl,
+                        int* status, cudaStream_t s) {
+    CUtensorMap mah, mal, mbh, mbl;
+    if (!make_map(&mah, Ah, KIND, p.M, p.a_pitch) || !make_map(&mal, Al, KIND, p.M, p.a_pitch) ||
+        !make_map(&mbh, Bh, KIND, p.N, p.a_pitch) || !make_map(&mbl, Bl, KIND, p.N, p.a_pitch))
+        return cudaErrorInvalidValue;
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(ramp_tc_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    });
+    if (attr != cudaSuccess) return attr;
+    const int tiles = ((p.M + BM - 1) / BM) * ((p.N + BN - 1) / BN);
+    const int grid = tiles < sm_count() ? tiles : sm_count();
+    TcArgs a{p, status};
+    ramp_tc_kernel<KIND><<<grid, kThreads, SMEM_BYTES, s>>>(mah, mal, mbh, mbl, a);
+    return cudaGetLastError();
 }
 
 }  // namespace
@@ -279,24 +360,16 @@ float tf32_round_host(float x) {
     return r;
 }
 
-cudaError_t launch_ramp_gemm_tc(const RampParams& p, const float* Bh, const float* Bl, int* status,
-                                cudaStream_t s) {
-    if (p.a_pitch % BK != 0) return cudaErrorInvalidValue;
-    CUtensorMap ma, mbh, mbl;
-    if (!make_map(&ma, p.A, p.M, p.a_pitch, BM) || !make_map(&mbh, Bh, p.N, p.a_pitch, BN) ||
-        !make_map(&mbl, Bl, p.N, p.a_pitch, BN))
-        return cudaErrorInvalidValue;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(ramp_gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             SMEM_BYTES);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
+cudaError_t launch_ramp_gemm_tc(const RampParams& p, int kind, const void* Ah, const void* Al, const void* Bh,
+                                const void* Bl, int* status, cudaStream_t s) {
+    const int bk = kind == RAMP_TF32X3 ? 32 : 64;
+    if (p.a_pitch % bk != 0 || p.M < 1 || p.N < 1) return cudaErrorInvalidValue;
+    switch (kind) {
+        case RAMP_TF32X3: return launch_kind<RAMP_TF32X3>(p, Ah, Al, Bh, Bl, status, s);
+        case RAMP_BF16X3: return launch_kind<RAMP_BF16X3>(p, Ah, Al, Bh, Bl, status, s);
+        case RAMP_FP16X3: return launch_kind<RAMP_FP16X3>(p, Ah, Al, Bh, Bl, status, s);
+        default: return cudaErrorInvalidValue;
     }
-    dim3 grid((p.N + BN - 1) / BN, (p.M + BM - 1) / BM);
-    TcArgs a{p, status};
-    ramp_gemm_tc_kernel<<<grid, 128, SMEM_BYTES, s>>>(ma, mbh, mbl, a);
-    return cudaGetLastError();
 }
 
 }  // namespace jfdk

@@ -72,6 +72,22 @@ def test_filter_matches_ramp_operator_and_oracle(torch_cuda, case, oracle):
     assert rel_l2(out, ref) <= 1e-5
 
 
+@pytest.mark.parametrize("kind,bar", [(1, 1e-5), (2, 5e-5), (3, 1e-5), (4, 1e-5)],
+                         ids=["tf32x3", "bf16x3", "fp16x3", "fp32-simt"])
+def test_filter_ramp_products(torch_cuda, case, oracle, kind, bar):
+    """Every ramp product against the oracle's FFT filter, in both forms."""
+    from jenhine_b200 import _lib
+    W = case["prep"].shape[2]
+    H = oracle.filter_spectrum(oracle.fft_length(W), float(case["hsr"]), *case["cut"], case["adj_pts"],
+                               case["adj_db"])
+    ref = oracle.filter_projections(case["prep"], case["ptms"], H, float(case["dso"]))
+    for form in ("fp32", "mixed"):
+        e = engine_for(case, precision=form)
+        e.set_option(_lib.OPT_RAMP_PRODUCT, kind)
+        out = e.filter(to_dev(torch_cuda, case["prep"]), v0=0).cpu().numpy()
+        assert rel_l2(out, ref) <= bar, (form, rel_l2(out, ref))
+
+
 @pytest.mark.parametrize("exact", [True, False])
 def test_backprojection_matches_bpcore(torch_cuda, case, exact):
     e = engine_for(case, bp_exact=exact)
