@@ -150,6 +150,7 @@ WeightParams weight_params(const jfdk_ctx* c) {
     w.L = c->L;
     w.det_right = c->mirror;
     w.mirror = c->mirror;
+    w.pw = c->d_pw;
     return w;
 }
 
@@ -193,11 +194,13 @@ int bp_zpt(const jfdk_ctx* c) { return c->opt_bp_zpt ? c->opt_bp_zpt : 8; }
 // Filtered frames [nv][rows][out_w] of rotation views view0.. -> the BP store,
 // slots slot0..: tapered FP32 quads, or in the mixed form FP16 records with
 // the views' scales.
-jfdk_status pack_frames(jfdk_ctx* c, const float* plain, int nv, int view0, int slot0) {
+// have_absmax: the ramp product already left the frames' maxima in d_absmax.
+jfdk_status pack_frames(jfdk_ctx* c, const float* plain, int nv, int view0, int slot0, bool have_absmax = false) {
     if (mixed(c)) {
         jfdk_status st = ensure_absmax(c, nv);
         if (st) return st;
-        JFDK_LAUNCH(c, launch_frame_absmax(plain, frame_px(c), nv, c->d_absmax, c->stream), "per-view maxima");
+        if (!have_absmax)
+            JFDK_LAUNCH(c, launch_frame_absmax(plain, frame_px(c), nv, c->d_absmax, c->stream), "per-view maxima");
         JFDK_LAUNCH(c, launch_pack_mixed(plain, frame_px(c), nv, c->rows, c->out_w, c->d_tw, view0, c->nviews,
                                          c->d_absmax, c->d_qscale, reinterpret_cast<uint4*>(c->d_q4), frame_px(c),
                                          slot0, c->stream),
@@ -250,6 +253,7 @@ RampParams ramp_params(const jfdk_ctx* c, int nv, float* out) {
     r.row_scale = nullptr;
     r.b_scale = 1.0f;
     r.vec_store = (reinterpret_cast<uintptr_t>(out) % 16 == 0) && (c->out_w % 4 == 0);
+    r.absmax = nullptr;
     return r;
 }
 
@@ -287,7 +291,7 @@ long long jfdk_kernel_launches(const jfdk_ctx* c) { return c ? c->launches : 0; 
 void jfdk_destroy(jfdk_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    dev_free(c->d_ptm); dev_free(c->d_tw); dev_free(c->d_tinv); dev_free(c->d_dmin);
+    dev_free(c->d_ptm); dev_free(c->d_tw); dev_free(c->d_tinv); dev_free(c->d_dmin); dev_free(c->d_pw);
     dev_free(c->d_T); dev_free(c->d_Th); dev_free(c->d_Tl); dev_free(c->d_Tb); dev_free(c->d_Tf);
     dev_free(c->d_status); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_arow);
     dev_free(c->d_plain);
@@ -425,6 +429,10 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_c, c->ops.c.data(), sizeof(float) * c->out_w, cudaMemcpyHostToDevice, c->stream), "upload");
     JFDK_LAUNCH(c, launch_preweight_dmin(c->d_tinv, c->groups, c->rows, c->L, c->in_w, c->mirror, c->d_dmin, c->stream),
                 "pre-weight minimum");
+    if ((st = dev_alloc(c, &c->d_pw, (size_t)c->groups * c->rows * c->in_w, "the pre-weight table"))) return bail(st);
+    JFDK_LAUNCH(c, launch_preweight_table(c->d_tinv, c->d_dmin, c->groups, c->rows, c->in_w, c->mirror, c->d_pw,
+                                          c->stream),
+                "pre-weight table");
     JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "context setup");
     *out = c;
     return JFDK_OK;
@@ -589,11 +597,20 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, in
         JFDK_LAUNCH(c, launch_prep_weight(prep_params(c, d_raw + (size_t)v0 * frame), nv, v0, weight_params(c),
                                           a_operand(c), c->d_e, c->stream),
                     "preprocess + pre-weight");
-        JFDK_LAUNCH(c, launch_ramp(c, ramp_params(c, nv, c->d_plain)), "ramp filter");
+        // mixed form with a tensor-core product: the product's epilogue
+        // leaves each frame's max |q| for the packer (no z-filter between)
+        RampParams rp = ramp_params(c, nv, c->d_plain);
+        const bool fused_max = mixed(c) && ramp_kind(c) != JFDK_RAMP_FP32_SIMT && !c->recon.z_filter;
+        if (fused_max) {
+            if ((st = ensure_absmax(c, nv))) return st;
+            JFDK_CUDA(c, cudaMemsetAsync(c->d_absmax, 0, sizeof(unsigned) * nv, c->stream), "clearing the maxima");
+            rp.absmax = c->d_absmax;
+        }
+        JFDK_LAUNCH(c, launch_ramp(c, rp), "ramp filter");
         if (c->recon.z_filter)
             JFDK_LAUNCH(c, launch_zfilter(c->d_plain, nv, c->rows, c->out_w, frame_px(c), c->out_w, c->stream),
                         "z-filter");
-        if ((st = pack_frames(c, c->d_plain, nv, v0, v0))) return st;
+        if ((st = pack_frames(c, c->d_plain, nv, v0, v0, fused_max))) return st;
     }
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[1], c->stream), "event");
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[2], c->stream), "event");

@@ -91,6 +91,7 @@ struct WeightParams {
     int L;                   // FFT length (pre-weight row length)
     int det_right;
     int mirror;
+    const float* pw;         // [groups][rows][width] weights, or null: computed per row
 };
 cudaError_t launch_preprocess(const PrepParams& p, int nv, float* out, cudaStream_t s);
 
@@ -109,6 +110,9 @@ cudaError_t launch_weight(const float* in, int nv, int v0, int width, int rows, 
 // Raw -> weighted A operand + edge means in one pass (whole-volume path).
 cudaError_t launch_prep_weight(const PrepParams& p, int nv, int v0, const WeightParams& w, const AOperand& A,
                                float* e, cudaStream_t s);
+// The table of pre-weights (needs dmin).
+cudaError_t launch_preweight_table(const float* tinv, const float* dmin, int groups, int rows, int in_w,
+                                   int det_right, float* pw, cudaStream_t s);
 // Frame minimum of the pre-weight distance per group.
 cudaError_t launch_preweight_dmin(const float* tinv, int groups, int rows, int L,
                                   int in_w, int det_right, float* dmin, cudaStream_t s);
@@ -126,6 +130,7 @@ struct RampParams {
     const float* row_scale;  // tensor-core FP16X3: [M] row factors, else null
     float b_scale;           // tensor-core FP16X3: 1 / the operator's scale, else 1
     int vec_store;           // q rows 16-byte aligned: store float4s
+    unsigned* absmax;        // tensor-core kinds: [views] max |q| as float bits (atomicMax; zeroed by the caller), or null
 };
 cudaError_t launch_ramp_gemm(const RampParams& p, cudaStream_t s);
 // Tensor-core split products (ramp_gemm_tc.cu).
@@ -171,6 +176,7 @@ struct jfdk_ctx {
     float2* d_tw = nullptr;      // [views][out_w] taper pairs
     float* d_tinv = nullptr;
     float* d_dmin = nullptr;
+    float* d_pw = nullptr;       // [groups][rows][in_w] pre-weights
     float* d_T = nullptr;
     float* d_Th = nullptr;       // TF32-exact split of the ramp operator
     float* d_Tl = nullptr;

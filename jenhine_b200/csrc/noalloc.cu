@@ -94,6 +94,7 @@ extern "C" jfdk_status jfdk_filter_frames_noalloc(jfdk_ctx* c, const float* d_in
     w.L = c->L;
     w.det_right = c->mirror;
     w.mirror = c->mirror;
+    w.pw = c->d_pw;
     jfdk::AOperand a{};
     a.kind = jfdk::AOUT_F32;
     a.hi = A;

@@ -107,6 +107,24 @@ __global__ void __launch_bounds__(256) preweight_dmin_kernel(const float* __rest
     }
 }
 
+// ---- the pre-weight of every group, row and column --------------------------
+// weight = frame minimum / distance, the same expression the row kernels
+// would evaluate, computed once per context (per 9-view group the reference
+// regenerates it, FilterAgent.cpp:161-192).
+__global__ void __launch_bounds__(256) preweight_table_kernel(const float* __restrict__ tinv,
+                                                              const float* __restrict__ dmin, int rows,
+                                                              int in_w, int det_right, float* __restrict__ pw) {
+    const int g = blockIdx.y, row = blockIdx.x;
+    __shared__ float T[16];
+    if (threadIdx.x < 16) T[threadIdx.x] = tinv[g * 16 + threadIdx.x];
+    __syncthreads();
+    const PWRow r = pw_row(T, (float)row);
+    const float dm = dmin[g];
+    float* out = pw + ((size_t)g * rows + row) * in_w;
+    for (int i = threadIdx.x; i < in_w; i += blockDim.x)
+        out[i] = __fdiv_rn(dm, pw_dist(r, u_axis(i, in_w, det_right)));
+}
+
 // ---- raw -> preprocessed frame (agent path) ---------------------------------
 __global__ void __launch_bounds__(256) preprocess_kernel(PrepParams P, float* __restrict__ out) {
     const int row = blockIdx.x, v = blockIdx.y;
@@ -199,8 +217,9 @@ __global__ void __launch_bounds__(256) weight_kernel(PrepParams P, const float* 
                                    : nullptr;
     const float* fin = FROM_RAW ? nullptr : in + m * width;
     auto pix = [&](int i) -> float { return FROM_RAW ? prep_pixel((float)src[i], P) : fin[i]; };
+    const float* pwrow = W.pw ? W.pw + ((size_t)g * rows + row) * width : nullptr;
     auto value = [&](int i, float p) -> float {
-        return __fmul_rn(p, __fdiv_rn(dmin, pw_dist(r, u_axis(i, width, W.det_right))));
+        return __fmul_rn(p, pwrow ? __ldg(pwrow + i) : __fdiv_rn(dmin, pw_dist(r, u_axis(i, width, W.det_right))));
     };
     const int elem = OUT == AOUT_F32 || OUT == AOUT_TF32X2 ? 4 : 2;
     const bool vec = FROM_RAW && ((reinterpret_cast<uintptr_t>(P.raw) & 7) == 0) &&
@@ -265,6 +284,12 @@ cudaError_t launch_preweight_dmin(const float* tinv, int groups, int rows, int L
     cudaError_t err = cudaMemsetAsync(dmin, 0x7f, sizeof(float) * groups, s);
     if (err != cudaSuccess) return err;
     preweight_dmin_kernel<<<dim3(rows, groups), 256, 0, s>>>(tinv, rows, L, in_w, det_right, dmin);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_preweight_table(const float* tinv, const float* dmin, int groups, int rows, int in_w,
+                                   int det_right, float* pw, cudaStream_t s) {
+    preweight_table_kernel<<<dim3(rows, groups), 256, 0, s>>>(tinv, dmin, rows, in_w, det_right, pw);
     return cudaGetLastError();
 }
 

@@ -235,12 +235,14 @@ __global__ void __launch_bounds__(kThreads, 1) ramp_tc_kernel(const __grid_const
             const int m0 = (t / tiles_n) * BM, n0 = (t % tiles_n) * BN;
             const int m = m0 + quarter * 32 + lane;
             const bool row_ok = m < p.M;
-            float em = 0.0f, rs = 1.0f;
+            float em = 0.0f, rs = 1.0f, amax = 0.0f;
             float* qrow = nullptr;
+            int vl = -1;
             if (row_ok) {
                 em = p.e[m];
                 if (p.row_scale) rs = p.row_scale[m] * p.b_scale;
-                const int vl = m / p.rows, row = m - vl * p.rows;
+                vl = m / p.rows;
+                const int row = m - vl * p.rows;
                 qrow = p.q + (size_t)vl * p.q_frame_stride + (size_t)row * p.q_pitch;
             }
 #pragma unroll 1
@@ -258,8 +260,10 @@ __global__ void __launch_bounds__(kThreads, 1) ramp_tc_kernel(const __grid_const
                 if (row_ok && n < p.N) {
                     float o[16];
 #pragma unroll
-                    for (int j = 0; j < 16; ++j)
+                    for (int j = 0; j < 16; ++j) {
                         o[j] = fmaf(__ldg(p.c + (n + j < p.N ? n + j : p.N - 1)), em, __uint_as_float(r[j]) * rs);
+                        if (n + j < p.N) amax = fmaxf(amax, fabsf(o[j]));
+                    }
                     if (p.vec_store && n + 16 <= p.N) {
                         float4* d = reinterpret_cast<float4*>(qrow + n);
 #pragma unroll
@@ -274,6 +278,16 @@ __global__ void __launch_bounds__(kThreads, 1) ramp_tc_kernel(const __grid_const
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(tempty(b));
+            if (p.absmax) {  // per-view max |q|; non-negative floats order like their bits
+                unsigned bits = __float_as_uint(amax);
+                const int v_first = __shfl_sync(0xffffffffu, vl, 0);
+                if (__all_sync(0xffffffffu, vl == v_first)) {
+                    bits = __reduce_max_sync(0xffffffffu, bits);
+                    if (lane == 0 && v_first >= 0) atomicMax(p.absmax + v_first, bits);
+                } else if (vl >= 0) {
+                    atomicMax(p.absmax + vl, bits);
+                }
+            }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
