@@ -208,6 +208,35 @@ jfdk_status jfdk_set_option(jfdk_ctx* ctx, int key, long long value);
  * CT numbers.  Synchronises the stream. */
 jfdk_status jfdk_stage_times(jfdk_ctx* ctx, float* ms3);
 
+/* ---- derivatives of the FP32 form ------------------------------------------
+ * vol = S q / C is the backprojection of filtered projections q with the
+ * weights C (the backprojected u-taper) fixed; the filter is
+ * y = T (w o x) + c e(x), e(x) the edge mean of x.  Both are linear; these
+ * entry points are their adjoints and the gradient with respect to the
+ * backprojection's projection matrices.  FP32 contexts only
+ * (JFDK_ERR_UNSUPPORTED in the mixed form).  No counterpart in the
+ * reference, which has no derivatives. */
+
+/* Replace the projection matrices the backprojector uses (num_views x 12,
+ * host); the filter's pre-weight and the u-taper keep the matrices given to
+ * jfdk_create.  Used to backproject under per-view motion. */
+jfdk_status jfdk_set_bp_geometry(jfdk_ctx* ctx, const float* h_ptms);
+/* q_bar = S^T (vol_bar / C) for views [v0, v0 + nv): d_vol_bar is
+ * num_pixels_z x y x x, d_q_bar nv x rows x filter_out_w.  C is the weight
+ * volume of the last jfdk_bp_accumulate sequence (JFDK_ERR_STATE without). */
+jfdk_status jfdk_bp_adjoint(jfdk_ctx* ctx, const float* d_vol_bar, int v0, int nv, float* d_q_bar);
+/* x_bar = w o (T^T y_bar) + (c . y_bar) / 3 on the three edge samples:
+ * d_q_bar nv x rows x filter_out_w in, d_p_bar nv x rows x filter_in_w out. */
+jfdk_status jfdk_filter_adjoint(jfdk_ctx* ctx, const float* d_q_bar, int v0, int nv, float* d_p_bar);
+/* Gradient of a loss L(vol) with respect to parameters theta_j of the
+ * projection matrices of views [v0, v0 + nv): d_q the filtered projections
+ * (nv x rows x filter_out_w) the volume d_vol was backprojected from,
+ * d_vol_bar = dL/dvol, d_dptm = dP/dtheta_j (nv x 6 x 12, device),
+ * d_grad (nv x 6 doubles, device) receives dL/dtheta.  Per-CTA partial sums
+ * in FP32, the reduction over the volume in FP64. */
+jfdk_status jfdk_geometry_gradient(jfdk_ctx* ctx, const float* d_q, int v0, int nv, const float* d_vol,
+                                   const float* d_vol_bar, const float* d_dptm, double* d_grad);
+
 /* ---- introspection (tests, autotuner) ------------------------------------ */
 
 /* The per-view BP u-taper (num_views x filter_out_w floats, host), computed as

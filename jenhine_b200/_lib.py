@@ -87,6 +87,10 @@ _SIGS = {
     "jfdk_get_ramp_operator": ([_P, _P, _P], C.c_int),
     "jfdk_kernel_launches": ([_P], C.c_longlong),
     "jfdk_device_check": ([C.c_char_p, C.c_int], C.c_int),
+    "jfdk_set_bp_geometry": ([_P, _P], C.c_int),
+    "jfdk_bp_adjoint": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
+    "jfdk_filter_adjoint": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
+    "jfdk_geometry_gradient": ([_P, _P, C.c_int, C.c_int, _P, _P, _P, _P], C.c_int),
 }
 
 

@@ -39,76 +39,11 @@
 #include <algorithm>
 #include <cstdint>
 
+#include "bp_common.cuh"
 #include "jfdk_internal.h"
 
 namespace jfdk {
 namespace {
-
-__device__ __forceinline__ float ct_number(float mu, float s, float n1) {
-    // CTNumCore::Process: h = mu * s - 1000; above 300 HU the slope is norm1,
-    // capped at 8191.  Separately rounded, no contraction.
-    float h = __fsub_rn(__fmul_rn(mu, s), 1000.f);
-    if (h > 300.0f) {
-        const float t = __fadd_rn(__fmul_rn(__fsub_rn(h, 300.0f), n1), 300.0f);
-        h = (t < 8191.f) ? t : 8191.f;
-    }
-    return h;
-}
-
-__device__ __forceinline__ int16_t to_i16(float f) {
-    if (f != f) return 0;
-    const float t = truncf(f);
-    return t >= 32767.0f ? (int16_t)32767 : (t <= -32768.0f ? (int16_t)-32768 : (int16_t)t);
-}
-
-__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
-
-// Packed f32x2 arithmetic.  Each lane of a single mul / add / fma rounds like
-// the scalar operation, but a packed multiply whose result feeds a packed add
-// can be fused into one fma by the compiler (measured on sm_100a with this
-// toolchain, for both the intrinsics and inline PTX with .rn), so every
-// product that BPCore rounds before adding is computed with scalar
-// __fmul_rn / __fadd_rn, which are never contracted.
-#define JFDK_PACKED_OP(name, op)                                                              \
-    __device__ __forceinline__ float2 name(float2 a, float2 b) {                              \
-        float2 d;                                                                             \
-        asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n " op \
-            " rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"                                          \
-            : "=f"(d.x), "=f"(d.y)                                                            \
-            : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));                                        \
-        return d;                                                                             \
-    }
-JFDK_PACKED_OP(pmul, "mul.rn.f32x2")
-JFDK_PACKED_OP(padd, "add.rn.f32x2")
-JFDK_PACKED_OP(psub, "sub.rn.f32x2")
-#undef JFDK_PACKED_OP
-
-// a * b + c per lane, one rounding (fma.rn.f32x2).
-__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) {
-    float2 d;
-    asm("{\n .reg .b64 ra, rb, rc, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
-        " mov.b64 rc, {%6, %7};\n fma.rn.f32x2 rd, ra, rb, rc;\n mov.b64 {%0, %1}, rd;\n}"
-        : "=f"(d.x), "=f"(d.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-    return d;
-}
-
-// add.rm.f32x2: the lanewise sum rounded toward -infinity.
-__device__ __forceinline__ float2 padd_rm(float2 a, float2 b) {
-    float2 d;
-    asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
-        " add.rm.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
-        : "=f"(d.x), "=f"(d.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return d;
-}
-
-// Floor without the conversion unit: for 0 <= x < 2^23 the sum 2^23 + x has
-// a unit in the last place of 1, so rounding it toward -infinity gives
-// 2^23 + floor(x) exactly; its bit pattern minus that of 2^23 is floor(x) as
-// an integer, and subtracting 2^23 back gives floor(x) as a float.
-constexpr float kMagic = 8388608.0f;   // 2^23
-constexpr int kMagicBits = 0x4B000000;  // bit pattern of 2^23
 
 // Resident CTAs per SM the compiler must allow for: 8 slices per thread fit
 // in 64 registers at 4 CTAs (32 warps) per SM, which measured faster than the
@@ -122,17 +57,14 @@ __global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_kernel(BPParams p)
     const int zb = p.z_begin + blockIdx.z * ZPT;
     if (x >= p.X || y >= p.Y) return;
 
-    // Axes as BPCore builds them (BPCore.cpp:47-66): (i - (n-1)/2) * pitch.
-    const float ax = __fmul_rn(__fadd_rn(-((float)p.X - 1.0f) / 2.0f, (float)x), p.pxy);
-    const float ay = __fmul_rn(__fadd_rn(-((float)p.Y - 1.0f) / 2.0f, (float)y), p.pxy);
+    const float ax = bp_axis(x, p.X, p.pxy), ay = bp_axis(y, p.Y, p.pxy);
     float az[ZPT];
     float2 acc[ZPT];  // (sum, weight)
     const size_t plane = (size_t)p.X * p.Y;
     const size_t base = (size_t)y * p.X + x;
 #pragma unroll
     for (int k = 0; k < ZPT; ++k) {
-        const float a = __fmul_rn(__fadd_rn(-((float)p.Z - 1.0f) / 2.0f, (float)(zb + k)), p.pz);
-        az[k] = a;
+        az[k] = bp_axis(zb + k, p.Z, p.pz);
         const bool in = zb + k < p.z_end;
         acc[k] = (!FINALIZE && p.load_acc && in)
                      ? f2(p.sum[(size_t)(zb + k) * plane + base], p.cnt[(size_t)(zb + k) * plane + base])
@@ -149,23 +81,11 @@ __global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_kernel(BPParams p)
 #pragma unroll 1
     for (int n = 0; n < p.nv; ++n, P4 += 3, q += p.q4_frame, tw += p.U) {
         const float4 r0 = __ldg(P4), r1 = __ldg(P4 + 1), r2 = __ldg(P4 + 2);
-        // (XxPM0 + (YxPM1 + PM3), XxPM4 + (YxPM5 + PM7)) and W (BPCore.cpp:120-145)
-        const float Uxy = __fadd_rn(__fmul_rn(ax, r0.x), __fadd_rn(__fmul_rn(ay, r0.y), r0.w));
-        const float Vxy = __fadd_rn(__fmul_rn(ax, r1.x), __fadd_rn(__fmul_rn(ay, r1.y), r1.w));
-        const float Wxy = __fadd_rn(__fmul_rn(ax, r2.x), __fadd_rn(__fmul_rn(ay, r2.y), r2.w));
-        const float rxy = WZ ? 0.0f : __frcp_rn(Wxy);
+        const XYTerms xy = bp_xy_terms(ax, ay, r0, r1, r2);
+        const float rxy = WZ ? 0.0f : __frcp_rn(xy.W);
 #pragma unroll
         for (int k = 0; k < ZPT; ++k) {
-            const float2 UV = f2(__fadd_rn(Uxy, __fmul_rn(az[k], r0.z)), __fadd_rn(Vxy, __fmul_rn(az[k], r1.z)));
-            float W = Wxy, r = rxy;
-            if (WZ) {
-                W = __fadd_rn(Wxy, __fmul_rn(az[k], r2.z));
-                r = __frcp_rn(W);
-            }
-            const float2 rr = f2(r, r);
-            const float2 q0 = pmul(UV, rr);
-            const float2 rem = pfma(f2(-W, -W), q0, UV);           // exact remainder
-            float2 uv = padd(pfma(rem, rr, q0), f2(0.5f, 0.5f));
+            float2 uv = bp_uv(xy, bp_w_r<WZ>(xy, rxy, az[k], r2.z), az[k], r0.z, r1.z);
             // Branch-free so the loads of all ZPT slices can be in flight at
             // once: a point off the detector reads quad (0, 0) and adds nothing.
             const bool in = (uv.x >= 0.0f) & (uv.x <= umax) & (uv.y >= 0.0f) & (uv.y <= vmax);

@@ -106,7 +106,8 @@ AOperand a_operand(const jfdk_ctx* c) {
 
 jfdk_status ensure_plain(jfdk_ctx* c, int views) {
     if (c->plain_views >= views) return JFDK_OK;
-    dev_free(c->d_plain);
+    dev_free(c->d_plain); dev_free(c->d_Tt); dev_free(c->d_rt); dev_free(c->d_qadj); dev_free(c->d_partial);
+    dev_free(c->d_dptm);
     c->plain_views = 0;
     jfdk_status st = dev_alloc(c, &c->d_plain, (size_t)views * frame_px(c), "the filtered frames");
     if (st) return st;
@@ -378,6 +379,8 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     if ((st = dev_alloc(c, &c->d_Tl, (size_t)c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_Tb, (size_t)2 * c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_Tf, (size_t)2 * c->out_w * a_pitch(c), "the ramp operator"))) return bail(st);
+    const int tt_pitch = (int)round_up(c->out_w, 64);
+    if ((st = dev_alloc(c, &c->d_Tt, (size_t)c->in_w * tt_pitch, "the transposed ramp operator"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_c, (size_t)c->out_w, "the edge response"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_status, 1, "the status word"))) return bail(st);
     if ((st = dev_alloc(c, &c->d_qscale, (size_t)c->nviews, "the view scales"))) return bail(st);
@@ -427,6 +430,14 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
         JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "upload");
     }
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_c, c->ops.c.data(), sizeof(float) * c->out_w, cudaMemcpyHostToDevice, c->stream), "upload");
+    {   // T^T [in_w][round64(out_w)] for the filter adjoint
+        std::vector<float> tt((size_t)c->in_w * tt_pitch, 0.0f);
+        for (int j = 0; j < c->out_w; ++j)
+            for (int i = 0; i < c->in_w; ++i) tt[(size_t)i * tt_pitch + j] = c->ops.T[(size_t)j * c->in_w + i];
+        JFDK_CUDA(c, cudaMemcpyAsync(c->d_Tt, tt.data(), sizeof(float) * tt.size(), cudaMemcpyHostToDevice, c->stream),
+                  "upload");
+        JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "upload");
+    }
     JFDK_LAUNCH(c, launch_preweight_dmin(c->d_tinv, c->groups, c->rows, c->L, c->in_w, c->mirror, c->d_dmin, c->stream),
                 "pre-weight minimum");
     if ((st = dev_alloc(c, &c->d_pw, (size_t)c->groups * c->rows * c->in_w, "the pre-weight table"))) return bail(st);
@@ -643,6 +654,130 @@ jfdk_status jfdk_reconstruct_host(jfdk_ctx* c, const uint16_t* h_raw, float* h_h
     if ((st = jfdk_reconstruct(c, c->d_raw_stage, c->d_hu_stage, nullptr))) return st;
     JFDK_CUDA(c, cudaMemcpyAsync(h_hu, c->d_hu_stage, hu_bytes, cudaMemcpyDeviceToHost, c->stream), "volume download");
     JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "reconstruct_host");
+    return JFDK_OK;
+}
+
+}  // extern "C"
+
+// ---- derivatives ---------------------------------------------------------
+
+namespace {
+
+jfdk_status deriv_check(jfdk_ctx* c, const char* what) {
+    if (mixed(c)) return fail(c, JFDK_ERR_UNSUPPORTED, std::string(what) + ": derivatives are of the FP32 form");
+    if (!c->d_cnt || !c->bp_has_views)
+        return fail(c, JFDK_ERR_STATE, std::string(what) + ": needs the weights of a backprojection (bp_accumulate)");
+    return JFDK_OK;
+}
+
+jfdk_status ensure_rt(jfdk_ctx* c, const float* d_vol_bar) {
+    const size_t n = (size_t)c->X * c->Y * c->Z;
+    if (!c->d_rt) {
+        jfdk_status st = dev_alloc(c, &c->d_rt, n, "the adjoint residual");
+        if (st) return st;
+    }
+    JFDK_LAUNCH(c, launch_residual_over_weight(d_vol_bar, c->d_cnt, n, c->d_rt, c->stream), "residual / weight");
+    return JFDK_OK;
+}
+
+AdjParams adj_params(const jfdk_ctx* c, int v0, int nv) {
+    AdjParams a{};
+    a.ptm = c->d_ptm;
+    a.v0 = v0; a.nv = nv; a.num_views = c->nviews;
+    a.U = c->out_w; a.V = c->rows; a.X = c->X; a.Y = c->Y; a.Z = c->Z;
+    a.pxy = c->pxy; a.pz = c->pz;
+    a.rt = c->d_rt;
+    a.q_frame = frame_px(c);
+    a.tw = c->d_tw;
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+jfdk_status jfdk_set_bp_geometry(jfdk_ctx* c, const float* h_ptms) {
+    if (!c || !h_ptms) return fail(c, JFDK_ERR_INVALID, "set_bp_geometry: bad argument");
+    c->ptms.assign(h_ptms, h_ptms + (size_t)c->nviews * 12);
+    c->w_depends_on_z = false;
+    for (int v = 0; v < c->nviews; ++v)
+        if (c->ptms[(size_t)v * 12 + 10] != 0.0f) c->w_depends_on_z = true;
+    JFDK_CUDA(c, cudaMemcpyAsync(c->d_ptm, c->ptms.data(), sizeof(float) * c->ptms.size(), cudaMemcpyHostToDevice,
+                                 c->stream),
+              "projection matrices upload");
+    JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "projection matrices upload");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_bp_adjoint(jfdk_ctx* c, const float* d_vol_bar, int v0, int nv, float* d_q_bar) {
+    if (!c || !d_vol_bar || !d_q_bar || nv < 0 || v0 < 0 || v0 + nv > c->nviews)
+        return fail(c, JFDK_ERR_INVALID, "bp_adjoint: bad argument");
+    jfdk_status st = deriv_check(c, "bp_adjoint");
+    if (st || nv == 0) return st;
+    if (c->qadj_views < nv) {
+        dev_free(c->d_qadj);
+        c->qadj_views = 0;
+        if ((st = dev_alloc(c, &c->d_qadj, (size_t)nv * frame_px(c), "the quad-space adjoint"))) return st;
+        c->qadj_views = nv;
+    }
+    if ((st = ensure_rt(c, d_vol_bar))) return st;
+    AdjParams a = adj_params(c, v0, nv);
+    a.qbar = c->d_qadj;
+    JFDK_LAUNCH(c, launch_bp_adjoint(a, c->w_depends_on_z, c->stream), "backprojection adjoint");
+    JFDK_LAUNCH(c, launch_unpack_adjoint(c->d_qadj, frame_px(c), nv, c->rows, c->out_w, c->d_tw, v0, c->nviews,
+                                         d_q_bar, c->stream),
+                "backprojection adjoint (unpack)");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_filter_adjoint(jfdk_ctx* c, const float* d_q_bar, int v0, int nv, float* d_p_bar) {
+    if (!c || !d_q_bar || !d_p_bar || nv < 0 || v0 < 0) return fail(c, JFDK_ERR_INVALID, "filter_adjoint: bad argument");
+    if (nv == 0) return JFDK_OK;
+    const int kp = (int)round_up(c->out_w, 64);
+    const size_t m = (size_t)nv * c->rows;
+    // the padded rows of q_bar go where the forward keeps its A operand
+    jfdk_status st = ensure_A(c, (m * kp + 2 * a_pitch(c) - 1) / (2 * a_pitch(c)));
+    if (st) return st;
+    float* ypad = static_cast<float*>(c->d_A);
+    JFDK_LAUNCH(c, launch_pad_rows(d_q_bar, m, c->out_w, ypad, kp, c->stream), "filter adjoint (pad)");
+    RampParams r{};
+    r.A = ypad; r.e = nullptr; r.B = c->d_Tt; r.c = nullptr;
+    r.M = (int)m; r.N = c->in_w; r.K = c->out_w; r.a_pitch = kp;
+    r.rows = c->rows;
+    r.q = d_p_bar; r.q_frame_stride = (long long)c->rows * c->in_w; r.q_pitch = c->in_w;
+    r.b_scale = 1.0f;
+    JFDK_LAUNCH(c, launch_ramp_gemm(r, c->stream), "filter adjoint (transposed product)");
+    JFDK_LAUNCH(c, launch_filter_adjoint_finish(d_q_bar, c->out_w, d_p_bar, c->in_w, c->rows, nv, v0, c->nviews, c->d_pw,
+                                                c->d_c, c->mirror, c->stream),
+                "filter adjoint (weights)");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_geometry_gradient(jfdk_ctx* c, const float* d_q, int v0, int nv, const float* d_vol,
+                                   const float* d_vol_bar, const float* d_dptm, double* d_grad) {
+    if (!c || !d_q || !d_vol || !d_vol_bar || !d_dptm || !d_grad || nv < 0 || v0 < 0 || v0 + nv > c->nviews)
+        return fail(c, JFDK_ERR_INVALID, "geometry_gradient: bad argument");
+    jfdk_status st = deriv_check(c, "geometry_gradient");
+    if (st || nv == 0) return st;
+    if ((st = ensure_Q4(c, nv))) return st;
+    JFDK_LAUNCH(c, launch_pack_quads(d_q, frame_px(c), nv, c->rows, c->out_w, c->d_tw, v0, c->nviews, 1, c->d_q4,
+                                     frame_px(c), 0, c->stream),
+                "packing projections");
+    if ((st = ensure_rt(c, d_vol_bar))) return st;
+    AdjParams a = adj_params(c, v0, nv);
+    a.q4 = c->d_q4;
+    a.vol = d_vol;
+    a.dptm = d_dptm;
+    const size_t need = geometry_gradient_ctas(a) * 6 * (size_t)nv;
+    if (c->partial_n < need) {
+        dev_free(c->d_partial);
+        c->partial_n = 0;
+        if ((st = dev_alloc(c, &c->d_partial, need, "the gradient partial sums"))) return st;
+        c->partial_n = need;
+    }
+    a.partial = c->d_partial;
+    JFDK_LAUNCH(c, launch_geometry_gradient(a, c->w_depends_on_z, d_grad, c->stream), "geometry gradient");
+    ++c->launches;  // the FP64 reduction
     return JFDK_OK;
 }
 

@@ -142,6 +142,31 @@ cudaError_t launch_ramp_gemm_tc(const RampParams& p, int kind, const void* Ah, c
                                 const void* Bl, int* status, cudaStream_t s);
 float tf32_round_host(float x);
 
+// Derivatives (adjoint.cu).
+struct AdjParams {
+    const float* ptm;        // [views][12] backprojection geometry
+    int v0, nv, num_views;   // views [v0, v0 + nv) of the rotation
+    int U, V, X, Y, Z;
+    float pxy, pz;
+    const float* rt;         // [Z][Y][X] vol_bar / weight
+    float4* qbar;            // adjoint out: quad space [nv][V][U]
+    long long q_frame;       // V * U
+    const float4* q4;        // gradient: the forward's tapered quads [nv][V][U]
+    const float2* tw;        // [views][U] taper pairs
+    const float* vol;        // gradient: the forward volume
+    const float* dptm;       // gradient: [nv][6][12] dP / dtheta_j
+    float* partial;          // gradient: [nv][ctas][6] scratch
+};
+cudaError_t launch_residual_over_weight(const float* vol_bar, const float* cnt, size_t n, float* rt, cudaStream_t s);
+cudaError_t launch_bp_adjoint(const AdjParams& p, bool w_depends_on_z, cudaStream_t s);
+cudaError_t launch_unpack_adjoint(const float4* qbar, long long q_frame, int nv, int rows, int U, const float2* tw,
+                                  int view0, int num_views, float* out, cudaStream_t s);
+size_t geometry_gradient_ctas(const AdjParams& p);
+cudaError_t launch_geometry_gradient(const AdjParams& p, bool w_depends_on_z, double* grad, cudaStream_t s);
+cudaError_t launch_pad_rows(const float* src, size_t rows, int w, float* dst, int pitch, cudaStream_t s);
+cudaError_t launch_filter_adjoint_finish(const float* ybar, int out_w, float* xbar, int in_w, int rows, int nv, int v0,
+                                         int num_views, const float* pw, const float* c, int mirror, cudaStream_t s);
+
 cudaError_t launch_zfilter(float* frames, int nv, int rows, int width, long long frame_stride,
                            int pitch, cudaStream_t s);
 
@@ -183,6 +208,8 @@ struct jfdk_ctx {
     uint16_t* d_Tb = nullptr;    // BF16 split: [2][out_w][a_pitch] (high, low)
     uint16_t* d_Tf = nullptr;    // FP16 split of the scaled operator (high, low)
     float tf_inv_scale = 1.0f;   // 1 / the FP16 operator's scale
+    float* d_Tt = nullptr;       // transposed operator [in_w][round64(out_w)] (filter adjoint)
+    float* d_czero = nullptr;    // [in_w] zeros
     float* d_c = nullptr;
     int* d_status = nullptr;     // nonzero: a kernel's bounded wait gave up
 
@@ -199,6 +226,11 @@ struct jfdk_ctx {
     uint16_t* d_raw_stage = nullptr; size_t raw_stage_bytes = 0;
     float* d_hu_stage = nullptr; size_t hu_stage_bytes = 0;
     bool bp_has_views = false;
+    // derivatives (allocated on demand)
+    float* d_rt = nullptr;                           // vol_bar / weight
+    float4* d_qadj = nullptr; int qadj_views = 0;    // quad-space adjoint
+    float* d_partial = nullptr; size_t partial_n = 0;
+    float* d_dptm = nullptr; int dptm_views = 0;
 
     // JFDK_OPT_* settings
     int opt_bp_exact = 0;

@@ -75,13 +75,13 @@ __global__ void __launch_bounds__(256) ramp_gemm_simt_kernel(RampParams p) {
         const int m = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
         if (m >= p.M) continue;
         const int vl = m / p.rows, row = m - vl * p.rows;
-        const float em = p.e[m];
+        const float em = p.c ? p.e[m] : 0.0f;   // no c: the plain product (filter adjoint)
         float* q = p.q + (size_t)vl * p.q_frame_stride + (size_t)row * p.q_pitch;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const int n = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4);
             if (n >= p.N) continue;
-            q[n] = fmaf(p.c[n], em, acc[i][j]);
+            q[n] = p.c ? fmaf(p.c[n], em, acc[i][j]) : acc[i][j];
         }
     }
 }

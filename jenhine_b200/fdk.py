@@ -244,3 +244,38 @@ class FDKEngine:
         self._check(self.lib.jfdk_reconstruct_host(self.ctx, raw.ctypes.data_as(C.c_void_p),
                                                    out.ctypes.data_as(C.c_void_p)))
         return out
+
+    # -- derivatives of the FP32 form (torch CUDA tensors) ------------------------
+    def set_bp_geometry(self, ptms):
+        """Projection matrices the backprojector uses from now on (the filter's
+        pre-weight and the u-taper keep the creation geometry)."""
+        p = np.ascontiguousarray(np.asarray(ptms, np.float32).reshape(self.scan.num_views, 12))
+        self._check(self.lib.jfdk_set_bp_geometry(self.ctx, p.ctypes.data_as(C.c_void_p)))
+
+    def bp_adjoint(self, vol_bar, v0: int = 0, nv: Optional[int] = None, out=None):
+        """S^T (vol_bar / C) for views [v0, v0 + nv), C from the last
+        bp_accumulate sequence."""
+        import torch
+        nv = self.scan.num_views - v0 if nv is None else nv
+        out = out if out is not None else torch.empty((nv, self.rows, self.filter_out_w), dtype=torch.float32,
+                                                      device=vol_bar.device)
+        self._check(self.lib.jfdk_bp_adjoint(self.ctx, _ptr(vol_bar), v0, nv, _ptr(out)))
+        return out
+
+    def filter_adjoint(self, q_bar, v0: int = 0, out=None):
+        import torch
+        nv = q_bar.shape[0]
+        out = out if out is not None else torch.empty((nv, self.rows, self.filter_in_w), dtype=torch.float32,
+                                                      device=q_bar.device)
+        self._check(self.lib.jfdk_filter_adjoint(self.ctx, _ptr(q_bar), v0, nv, _ptr(out)))
+        return out
+
+    def geometry_gradient(self, q, v0: int, vol, vol_bar, dptm, out=None):
+        """dL/dtheta (nv x 6, float64) for views [v0, v0 + q.shape[0]) given
+        dP/dtheta (nv x 6 x 12, float32 CUDA)."""
+        import torch
+        nv = q.shape[0]
+        out = out if out is not None else torch.empty((nv, 6), dtype=torch.float64, device=q.device)
+        self._check(self.lib.jfdk_geometry_gradient(self.ctx, _ptr(q), v0, nv, _ptr(vol), _ptr(vol_bar),
+                                                    _ptr(dptm), _ptr(out)))
+        return out

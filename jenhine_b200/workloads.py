@@ -9,6 +9,8 @@ c2  dental-CBCT size, plain FP32: 600 views over 360 deg, 768 x 768 detector
     (+/- 0.5 px detector shift, +/- 0.2 deg tilt), 20 ellipsoids plus 3
     metal inserts (mu 0.5 /mm), I0 = 5e4.  The orbit is not given for this
     case; it uses c1's SID 500 mm / SDD 800 mm.
+c3  differentiation: 360 views of 512 x 512 at 0.5 mm -> 256^3 at 0.4 mm
+    (the detector pitch is not given for this case; 0.5 mm covers the volume).
 mini_*  reduced versions of c1 / c2 for parity tests.
 
 The reference corrects gain with one scalar bright field
@@ -77,6 +79,14 @@ def c2() -> Workload:
                     ReconConfig(640, 640, 480, 0.125, 0.125, ct_norm0=1.0, ct_norm1=1.0), 20, 3, 5e4)
 
 
+def c3() -> Workload:
+    """Differentiation: 360 views of 512 x 512 (0.5 mm) -> 256^3 at 0.4 mm,
+    10-ellipsoid phantom; per-view rigid motion (jenhine_b200.motion) of
+    +/- 0.5 mm / +/- 0.3 deg is the geometry the gradient is taken at."""
+    return Workload("c3", ScanGeometry(360, 500.0, 800.0, 512, 512, 0.5, 0.5, seed=303),
+                    ReconConfig(256, 256, 256, 0.4, 0.4, ct_norm0=1.0, ct_norm1=1.0), 10, 0, 1e5)
+
+
 def c2_slab() -> Workload:
     """c2's scan backprojected into a 16-slice central slab (profiling case:
     same projections and kernels, 1/30 of the volume)."""
@@ -98,4 +108,4 @@ def mini_c2() -> Workload:
                     beam_hardening=(1.0, 0.05, 0.01))
 
 
-WORKLOADS = {"c1": c1, "c2": c2, "c2_slab": c2_slab, "mini_c1": mini_c1, "mini_c2": mini_c2}
+WORKLOADS = {"c1": c1, "c2": c2, "c2_slab": c2_slab, "c3": c3, "mini_c1": mini_c1, "mini_c2": mini_c2}

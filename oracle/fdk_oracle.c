@@ -666,7 +666,7 @@ void jo_bp_accumulate_f64(double* sum, double* cnt, const float* proj, const flo
  * 0 <= u <= U-1 and 0 <= v <= V-1, bilinear lerps, sum and weight) with the
  * axes, coordinates, projections and arithmetic in double. */
 typedef struct {
-    double* sum; double* cnt; const double* proj; const float* ptms; const float* uw;
+    double* sum; double* cnt; const double* proj; const double* ptms; const float* uw;
     int v0, nv, U, V, X, Y, Z; double pitchXY, pitchZ; const int* pts; int p0, p1;
 } bpp_job;
 
@@ -680,7 +680,7 @@ static void* bpp_worker(void* arg) {
         double s = 0.0, c = 0.0;
         for (int iv = 0; iv < j->nv; ++iv) {
             const int view = j->v0 + iv;
-            const float* P = j->ptms + (size_t)view * 12;
+            const double* P = j->ptms + (size_t)view * 12;
             const double Uc = x * P[0] + y * P[1] + z * P[2] + P[3];
             const double Vc = x * P[4] + y * P[5] + z * P[6] + P[7];
             const double Wc = x * P[8] + y * P[9] + z * P[10] + P[11];
@@ -704,9 +704,9 @@ static void* bpp_worker(void* arg) {
     return NULL;
 }
 
-void jo_bp_points_f64(double* sum, double* cnt, const double* proj, const float* ptms,
-                      const float* uw, int v0, int nv, int U, int V, const int* pts, int npts,
-                      int X, int Y, int Z, float pitchXY, float pitchZ, int nthreads) {
+void jo_bp_points_f64d(double* sum, double* cnt, const double* proj, const double* ptms,
+                       const float* uw, int v0, int nv, int U, int V, const int* pts, int npts,
+                       int X, int Y, int Z, float pitchXY, float pitchZ, int nthreads) {
     if (nthreads < 1) nthreads = 1;
     if (nthreads > npts) nthreads = npts > 0 ? npts : 1;
     pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * nthreads);
@@ -719,6 +719,16 @@ void jo_bp_points_f64(double* sum, double* cnt, const double* proj, const float*
     }
     for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
     free(th); free(jobs);
+}
+
+void jo_bp_points_f64(double* sum, double* cnt, const double* proj, const float* ptms,
+                      const float* uw, int v0, int nv, int U, int V, const int* pts, int npts,
+                      int X, int Y, int Z, float pitchXY, float pitchZ, int nthreads) {
+    const int nviews = v0 + nv;
+    double* pd = (double*)malloc(sizeof(double) * 12 * (size_t)nviews);
+    for (size_t i = 0; i < 12 * (size_t)nviews; ++i) pd[i] = ptms[i];
+    jo_bp_points_f64d(sum, cnt, proj, pd, uw, v0, nv, U, V, pts, npts, X, Y, Z, pitchXY, pitchZ, nthreads);
+    free(pd);
 }
 
 /* BPCore::DoneSlice (BPCore.cpp:198-205): out = sum / cnt. */

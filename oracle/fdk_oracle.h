@@ -101,6 +101,11 @@ void jo_bp_accumulate_f64(double* sum, double* cnt, const float* proj,
 void jo_bp_points_f64(double* sum, double* cnt, const double* proj, const float* ptms,
                       const float* uw, int v0, int nv, int U, int V, const int* pts, int npts,
                       int X, int Y, int Z, float pitchXY, float pitchZ, int nthreads);
+/* The same with FP64 projection matrices (finite-difference checks of the
+ * geometry gradient); the u-taper uw stays as given. */
+void jo_bp_points_f64d(double* sum, double* cnt, const double* proj, const double* ptms,
+                       const float* uw, int v0, int nv, int U, int V, const int* pts, int npts,
+                       int X, int Y, int Z, float pitchXY, float pitchZ, int nthreads);
 /* out = sum / cnt (BPCore::DoneSlice). */
 void jo_bp_finalize(float* out, const float* sum, const float* cnt, size_t n);
 

@@ -52,6 +52,7 @@ class Oracle:
             "jo_filter_rows": [_P, _P, _P, I, I, I, I, _P, I],
             "jo_filter_rows_f64": [_P, _P, _P, I, I, I, I, _P, I],
             "jo_bp_points_f64": [_P, _P, _P, _P, _P, I, I, I, I, _P, I, I, I, I, F, F, I],
+            "jo_bp_points_f64d": [_P, _P, _P, _P, _P, I, I, I, I, _P, I, I, I, I, F, F, I],
             "jo_filter_kernel_f64": [_P, _P, I], "jo_bp_uweights": [_P, _P, I, I],
             "jo_bp_accumulate": [_P, _P, _P, _P, _P, I, I, I, I, I, I, I, F, F, I, I, I],
             "jo_bp_accumulate_f64": [_P, _P, _P, _P, _P, I, I, I, I, I, I, I, F, F, I, I, I],
@@ -252,6 +253,19 @@ class Oracle:
         self.lib.jo_bp_points_f64(_ptr(s), _ptr(c), _ptr(proj), _ptr(ptms), _ptr(uw), 0, nv, U,
                                   det_rows, _ptr(pts), len(pts), X, Y, Z, pitch_xy, pitch_z,
                                   nthreads or os.cpu_count() or 1)
+        return s, c
+
+    def bp_points_f64d(self, proj, ptms64, uw, pts, X, Y, Z, pitch_xy, pitch_z, nthreads=None):
+        """FP64 backprojection of voxels pts with FP64 projection matrices
+        ptms64 (n x 12) and a given u-taper uw (n x U, float32)."""
+        proj = _c(proj, np.float64)
+        nv, V, U = proj.shape
+        pts = _c(pts, np.int32).reshape(-1, 3)
+        s = np.zeros(len(pts), np.float64)
+        c = np.zeros(len(pts), np.float64)
+        self.lib.jo_bp_points_f64d(_ptr(s), _ptr(c), _ptr(proj), _ptr(_c(ptms64, np.float64)), _ptr(_c(uw, _f32)),
+                                   0, nv, U, V, _ptr(pts), len(pts), X, Y, Z, pitch_xy, pitch_z,
+                                   nthreads or os.cpu_count() or 1)
         return s, c
 
     @staticmethod
