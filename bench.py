@@ -2,14 +2,16 @@
 """FDK reconstruction throughput on B200: GUPS (voxel-view updates / s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
-                    [--workload c2] [--precision fp32] [--no-cpu-baseline]
+                    [--workload c2] [--precision both|fp32|mixed] [--no-cpu-baseline]
 
 A step is one full reconstruction of the workload (raw uint16 frames ->
 preprocess -> cosine pre-weight -> ramp filter -> backprojection -> CT
 numbers) with the raw frames already resident in HBM.  Under torchrun each
 rank reconstructs its own seeded scan (independent objects, no data-path
 collective): weak scaling.  value = updates of all ranks / max over ranks of
-the device-timed K steps.
+the device-timed K steps.  By default both forms run back to back: the line's
+value, e2e and roofline are the plain FP32 form's, forms.mixed holds the
+mixed-precision form's numbers and its speed-up over the plain form.
 
 e2e: the same metric through the C ABI's host-buffer call
 (jfdk_reconstruct_host): every step copies the raw frames in from pinned
@@ -46,7 +48,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--workload", default="c2")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp32", "mixed"],
+                    help="both: the plain FP32 form is the line's value, the mixed form under forms.mixed")
     ap.add_argument("--exact", action="store_true", help="BPCore-exact backprojection rounding")
     ap.add_argument("--zpt", type=int, default=0, help="slices per backprojection thread (0: form default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -227,34 +230,13 @@ def run_reference(a, w, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def main():
-    a = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    from jenhine_b200.workloads import WORKLOADS
-    w = WORKLOADS[a.workload]()
-    if a.impl == "reference":
-        run_reference(a, w, rank, world)
-        return
-
-    import numpy as np
+def time_form(a, w, raw, ptms, precision, dist, world, local):
+    """Device-timed steps of one form (raw frames resident in HBM), then the
+    same through the host-buffer call.  Returns a dict of the form's numbers."""
     import torch
-    import datetime
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
     from jenhine_b200 import _lib
     from jenhine_b200.fdk import FDKEngine
-
-    # each rank reconstructs its own scan
-    w.geom.seed += 1000 * rank
-    raw = w.raw_torch()
-    ptms = w.geom.ptms()
-    eng = FDKEngine(w.scan, w.recon, ptms, precision=a.precision, bp_exact=a.exact)
+    eng = FDKEngine(w.scan, w.recon, ptms, precision=precision, bp_exact=a.exact)
     eng.set_option(_lib.OPT_STAGE_TIMING, 1)
     if a.zpt:
         eng.set_option(_lib.OPT_BP_ZPT, a.zpt)
@@ -283,15 +265,16 @@ def main():
         dist.barrier()
     launches = eng.kernel_launches - launches0
     clk = clocks.stop()
-    ms = start.elapsed_time(end) / a.steps
-    ms_t = torch.tensor([ms], device="cuda")
+    ms_t = torch.tensor([start.elapsed_time(end) / a.steps], device="cuda")
     if dist:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = ms_t.item()
-    value = w.updates * world / (ms_max / 1000.0) / 1e9
+    ms = ms_t.item()
+    out = {"value": w.updates * world / (ms / 1000.0) / 1e9, "ms_per_step": ms, "s_per_volume": ms / 1000.0,
+           "stages_ms": {"preprocess_weight_filter": statistics.mean(s[0] for s in stage_ms),
+                         "backprojection_hu": statistics.mean(s[2] for s in stage_ms)},
+           "gpu_launches": launches, "clocks": clk}
 
     # end to end through the host-buffer call, pinned memory
-    e2e = None
     if not a.no_e2e:
         raw_h = torch.empty(raw.shape, dtype=torch.uint16, pin_memory=True)
         raw_h.copy_(raw.cpu())
@@ -302,56 +285,104 @@ def main():
         if dist:
             dist.barrier()
         s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = eng.kernel_launches
         s2.record()
         for _ in range(a.steps):
             eng.reconstruct_host(raw_np, out_np)
         e2.record()
         torch.cuda.synchronize()
+        out["gpu_launches"] += eng.kernel_launches - l0
         ems = torch.tensor([s2.elapsed_time(e2) / a.steps], device="cuda")
         if dist:
             dist.all_reduce(ems, op=dist.ReduceOp.MAX)
-        e2e = {"value": w.updates * world / (ems.item() / 1000.0) / 1e9, "unit": "GUPS",
-               "h2d_bytes_per_step": int(raw.numel() * 2), "d2h_bytes_per_step": int(vol.numel() * 4),
-               "ms_per_step": ems.item()}
+        out["e2e"] = {"value": w.updates * world / (ems.item() / 1000.0) / 1e9, "unit": "GUPS",
+                      "h2d_bytes_per_step": int(raw.numel() * 2), "d2h_bytes_per_step": int(vol.numel() * 4),
+                      "ms_per_step": ems.item()}
+    eng.close()
+    return out
+
+
+def roofline(w, bp_ms, kernel, prof):
+    """HBM roofline of the backprojection kernel: algorithmic bytes (the
+    filtered projections read once, the volume written once) over its
+    CUDA-event time."""
+    peak, peak_kind = measured_peaks()
+    r, g = w.recon, w.geom
+    alg = g.n_views * g.det_v * g.det_u * 4 + r.num_pixels_x * r.num_pixels_y * r.num_pixels_z * 4
+    achieved = alg / (bp_ms / 1000.0) / 1e9
+    return {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs ({'of measured' if peak_kind == 'measured' else 'of fallback'})",
+            "algorithmic_bytes_per_launch": alg, "traffic": profile_traffic(prof),
+            "note": "the backprojector is bound by instruction issue and L1 traffic (its footprint reads "
+                    "hit L1/L2), not by HBM: frac shows the distance to the memory floor"}
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from jenhine_b200.workloads import WORKLOADS
+    w = WORKLOADS[a.workload]()
+    if a.impl == "reference":
+        run_reference(a, w, rank, world)
+        return
+
+    import torch
+    import datetime
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    # each rank reconstructs its own scan
+    w.geom.seed += 1000 * rank
+    raw = w.raw_torch()
+    ptms = w.geom.ptms()
+    forms = ["fp32", "mixed"] if a.precision == "both" else [a.precision]
+    res = {f: time_form(a, w, raw, ptms, f, dist, world, local) for f in forms}
 
     if rank == 0:
-        bp_ms = statistics.mean(s[2] for s in stage_ms)
-        pf_ms = statistics.mean(s[0] for s in stage_ms)
-        peak, peak_kind = measured_peaks()
-        g = w.geom
-        proj_bytes = g.n_views * g.det_v * g.det_u * 4
-        vol_bytes = r.num_pixels_x * r.num_pixels_y * r.num_pixels_z * 4
-        alg = proj_bytes + vol_bytes
-        achieved = alg / (bp_ms / 1000.0) / 1e9
+        head = res[forms[0]]
         line = {
-            "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": world, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": ms_max, "s_per_volume": ms_max / 1000.0,
+            "metric": METRIC, "value": head["value"], "unit": "GUPS", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": head["ms_per_step"], "s_per_volume": head["s_per_volume"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": DATA, "config": dict(workload_config(w), precision=a.precision,
-                                         bp_rounding="bpcore-exact" if a.exact else "fast",
-                                         parallelism=f"{world} independent scans, one per GPU"),
-            "stages_ms": {"preprocess_weight_filter": pf_ms, "backprojection_hu": bp_ms},
-            "roofline": {"kernel": "bp_kernel (backprojection + normalisation + CT numbers)",
-                         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                         "algorithmic_bytes_per_launch": alg,
-                         "traffic": profile_traffic(f"bp_kernel_{w.name}"),
-                         "note": "BP is issue/L1-bound, not HBM-bound: the HBM fraction shows how far the "
-                                 "kernel is from the memory floor"},
-            "gpu_launches": launches,
-            "clocks": clk,
+            "data": DATA,
+            "config": dict(workload_config(w), precision=forms[0],
+                           forms="value/e2e: the plain FP32 form; forms.mixed: the mixed-precision form"
+                           if len(forms) == 2 else forms[0],
+                           bp_rounding="bpcore-exact" if a.exact else "fast",
+                           parallelism=f"{world} independent scans, one per GPU"),
+            "stages_ms": head["stages_ms"],
+            "roofline": roofline(w, head["stages_ms"]["backprojection_hu"],
+                                 "bp_kernel (backprojection + normalisation + CT numbers)",
+                                 f"bp_kernel_{w.name}" if forms[0] == "fp32" else f"bp_mixed_kernel_{w.name}"),
+            "gpu_launches": sum(r["gpu_launches"] for r in res.values()),
+            "clocks": head["clocks"],
         }
-        if e2e:
-            line["e2e"] = e2e
+        if "e2e" in head:
+            line["e2e"] = head["e2e"]
+        if len(forms) == 2:
+            m = dict(res["mixed"])
+            m["roofline"] = roofline(w, m["stages_ms"]["backprojection_hu"],
+                                     "bp_mixed_kernel (FP16 records, FP32 accumulation)", f"bp_mixed_kernel_{w.name}")
+            m["speedup_vs_fp32"] = head["ms_per_step"] / m["ms_per_step"]
+            line["forms"] = {"fp32": {k: v for k, v in head.items()}, "mixed": m}
         if not a.no_cpu_baseline and world == 1:
+            from jenhine_b200.fdk import FDKEngine
+            g = w.geom
             nvb = min(60, g.n_views)
+            eng = FDKEngine(w.scan, w.recon, ptms)
             raw_np = raw[:12].cpu().numpy()
             filt = eng.filter(eng.preprocess(raw[:nvb]), 0).cpu().numpy()
+            eng.close()
             gups, cores, kind, sample, spent, _ = cpu_sample(w, raw_np, filt, ptms)
             line["cpu_baseline"] = {"value": gups, "unit": "GUPS", "cores": cores, "kind": kind,
                                     "sample": sample, "seconds": spent}
         print(json.dumps(line), flush=True)
-    eng.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
