@@ -317,12 +317,97 @@ def roofline(w, bp_ms, kernel, prof):
                     "hit L1/L2), not by HBM: frac shows the distance to the memory floor"}
 
 
+def run_batch(a, rank, world, local):
+    """--workload batch: 16 seeded scans of uneven size (workloads.batch()),
+    reconstructed (a) one jfdk_reconstruct launch sequence per scan and (b) as
+    one batch -- every scan's filter stage and one persistent backprojection,
+    replayed as a CUDA graph.  value = aggregate GUPS of (b)."""
+    import torch
+    from jenhine_b200.fdk import FDKBatch, FDKEngine
+    from jenhine_b200.workloads import batch
+    if a.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the batch workload is timed on the GPU engine only; "
+                                                                  "the reference arm runs the c2 workload"}), flush=True)
+        return
+    torch.cuda.set_device(local)
+    scans = batch()
+    for w in scans:
+        w.geom.seed += 1000 * rank
+    updates = sum(w.updates for w in scans)
+    raws = [w.raw_torch() for w in scans]
+    forms = ["fp32", "mixed"] if a.precision == "both" else [a.precision]
+    res = {}
+    for form in forms:
+        engines = [FDKEngine(w.scan, w.recon, w.geom.ptms(), precision=form) for w in scans]
+        b = FDKBatch(engines, autotune=True, graph=True)
+        outs = [torch.empty((w.recon.num_pixels_z, w.recon.num_pixels_y, w.recon.num_pixels_x), device="cuda")
+                for w in scans]
+        ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+        # one launch sequence per scan
+        for _ in range(a.warmup):
+            for e, r, o in zip(engines, raws, outs):
+                e.reconstruct(r, o)
+        torch.cuda.synchronize()
+        s0, e0 = ev(), ev()
+        s0.record()
+        for _ in range(a.steps):
+            for e, r, o in zip(engines, raws, outs):
+                e.reconstruct(r, o)
+        e0.record()
+        torch.cuda.synchronize()
+        single_ms = s0.elapsed_time(e0) / a.steps
+        # one batch: direct run + graph recording, then replays
+        for _ in range(a.warmup):
+            b.run(raws, outs)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        time.sleep(0.5)
+        l0 = b.launches
+        s1, e1 = ev(), ev()
+        s1.record()
+        for _ in range(a.steps):
+            b.run(raws, outs)
+        e1.record()
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        batch_ms = s1.elapsed_time(e1) / a.steps
+        res[form] = {"value": updates / (batch_ms / 1000.0) / 1e9, "ms_per_step": batch_ms,
+                     "one_launch_each": {"value": updates / (single_ms / 1000.0) / 1e9, "ms_per_step": single_ms},
+                     "speedup_vs_one_launch_each": single_ms / batch_ms,
+                     "gpu_launches": (b.launches - l0), "clocks": clk}
+        b.close()
+        for e in engines:
+            e.close()
+    if rank == 0:
+        head = res[forms[0]]
+        line = {"metric": "aggregate GUPS, 16 seeded scans of uneven size: one graph-replayed batch "
+                          "(persistent backprojection) vs one launch sequence per scan",
+                "value": head["value"], "unit": "GUPS", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+                "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": DATA,
+                "config": {"workload": "batch: " + ", ".join(
+                    f"{w.recon.num_pixels_x}x{w.recon.num_pixels_y}x{w.recon.num_pixels_z}/{w.geom.n_views}v/"
+                    f"{w.geom.det_u}" for w in scans), "updates_per_step": updates, "precision": forms[0],
+                    "l2": "inputs larger than L2"},
+                "one_launch_each": head["one_launch_each"],
+                "speedup_vs_one_launch_each": head["speedup_vs_one_launch_each"],
+                "gpu_launches": head["gpu_launches"], "clocks": head["clocks"]}
+        if len(forms) == 2:
+            line["forms"] = res
+        print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     from jenhine_b200.workloads import WORKLOADS
+    if a.workload == "batch":
+        run_batch(a, rank, world, local)
+        return
     w = WORKLOADS[a.workload]()
     if a.impl == "reference":
         run_reference(a, w, rank, world)

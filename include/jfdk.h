@@ -237,6 +237,40 @@ jfdk_status jfdk_filter_adjoint(jfdk_ctx* ctx, const float* d_q_bar, int v0, int
 jfdk_status jfdk_geometry_gradient(jfdk_ctx* ctx, const float* d_q, int v0, int nv, const float* d_vol,
                                    const float* d_vol_bar, const float* d_dptm, double* d_grad);
 
+/* ---- autotuner and batches (no counterpart in the reference) -------------- */
+
+/* Pick the backprojection's voxel tile depth (JFDK_OPT_BP_ZPT: 4 or 8 slices
+ * per thread, a 32 x 8 x ZPT tile per CTA) and the filter stage's views per
+ * chunk (JFDK_OPT_VIEW_CHUNK: 16, 32 or 64) for this context's shape by
+ * timing the candidates on the device (a 32-slice slab, the first 128 views
+ * of zero frames).  Results are cached per shape in the process and, when
+ * $JFDK_AUTOTUNE_CACHE names a file, appended to it and read back by later
+ * processes.  Synchronises the context's stream. */
+enum { JFDK_AUTOTUNE_FORCE = 1 };  /* re-time even when the shape is cached */
+jfdk_status jfdk_autotune(jfdk_ctx* ctx, int flags);
+
+/* A batch of scans (one context each, all of the same form) reconstructed
+ * together: every scan's filter stage, then ONE persistent backprojection
+ * launch over the tiles of all scans (scans in order; a CTA takes the next
+ * tile when it finishes one, so scans of uneven size leave no tail).  With
+ * JFDK_BATCH_GRAPH the first jfdk_batch_run with a set of buffers runs the
+ * pipeline directly and records it as a CUDA graph; later runs with the same
+ * buffers replay the graph (one launch from the host).  The batch runs on
+ * `cuda_stream` (NULL: a stream of its own, ordered after the legacy default
+ * stream); the contexts' own streams are restored after each run.  Each
+ * volume equals the scan's own jfdk_reconstruct bit for bit. */
+typedef struct jfdk_batch jfdk_batch;
+enum { JFDK_BATCH_AUTOTUNE = 1, JFDK_BATCH_GRAPH = 2 };
+jfdk_status jfdk_batch_create(jfdk_batch** out, jfdk_ctx* const* ctxs, int n, int flags, void* cuda_stream);
+void jfdk_batch_destroy(jfdk_batch* batch);
+const char* jfdk_batch_last_error(const jfdk_batch* batch);
+/* d_raw[i]: scan i's raw frames (device), d_hu[i]: its HU volume (device). */
+jfdk_status jfdk_batch_run(jfdk_batch* batch, const uint16_t* const* d_raw, float* const* d_hu);
+/* Kernels the batch has run: its persistent launches, plus every kernel of
+ * each graph replay (a direct run's filter-stage kernels are counted by the
+ * contexts, jfdk_kernel_launches). */
+long long jfdk_batch_launches(const jfdk_batch* batch);
+
 /* ---- introspection (tests, autotuner) ------------------------------------ */
 
 /* The per-view BP u-taper (num_views x filter_out_w floats, host), computed as

@@ -28,6 +28,8 @@ OPT_STAGE_TIMING = 3
 OPT_BP_ZPT = 4
 OPT_FILTER_SIMT = 5
 OPT_RAMP_PRODUCT = 6
+AUTOTUNE_FORCE = 1
+BATCH_AUTOTUNE, BATCH_GRAPH = 1, 2
 RAMP_DEFAULT, RAMP_TF32X3, RAMP_BF16X3, RAMP_FP16X3, RAMP_FP32_SIMT = 0, 1, 2, 3, 4
 
 
@@ -91,6 +93,12 @@ _SIGS = {
     "jfdk_bp_adjoint": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
     "jfdk_filter_adjoint": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
     "jfdk_geometry_gradient": ([_P, _P, C.c_int, C.c_int, _P, _P, _P, _P], C.c_int),
+    "jfdk_autotune": ([_P, C.c_int], C.c_int),
+    "jfdk_batch_create": ([C.POINTER(_P), _P, C.c_int, C.c_int, _P], C.c_int),
+    "jfdk_batch_destroy": ([_P], None),
+    "jfdk_batch_last_error": ([_P], C.c_char_p),
+    "jfdk_batch_run": ([_P, _P, _P], C.c_int),
+    "jfdk_batch_launches": ([_P], C.c_longlong),
 }
 
 

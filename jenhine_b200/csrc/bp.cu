@@ -51,10 +51,10 @@ namespace {
 constexpr int bp_min_blocks(int zpt) { return zpt == 8 ? 4 : 1; }
 
 template <int ZPT, bool FINALIZE, bool EXACT, bool WZ>
-__global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_kernel(BPParams p) {
-    const int x = blockIdx.x * 32 + threadIdx.x;
-    const int y = blockIdx.y * 8 + threadIdx.y;
-    const int zb = p.z_begin + blockIdx.z * ZPT;
+__device__ __forceinline__ void bp_block(const BPParams& p, int bx, int by, int bz) {
+    const int x = bx * 32 + threadIdx.x;
+    const int y = by * 8 + threadIdx.y;
+    const int zb = p.z_begin + bz * ZPT;
     if (x >= p.X || y >= p.Y) return;
 
     const float ax = bp_axis(x, p.X, p.pxy), ay = bp_axis(y, p.Y, p.pxy);
@@ -150,10 +150,10 @@ __device__ __forceinline__ float rcp_approx(float x) {
 }
 
 template <int ZPT, bool FINALIZE, bool WZ>
-__global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_mixed_kernel(BPParams p) {
-    const int x = blockIdx.x * 32 + threadIdx.x;
-    const int y = blockIdx.y * 8 + threadIdx.y;
-    const int zb = p.z_begin + blockIdx.z * ZPT;
+__device__ __forceinline__ void bp_mixed_block(const BPParams& p, int bx, int by, int bz) {
+    const int x = bx * 32 + threadIdx.x;
+    const int y = by * 8 + threadIdx.y;
+    const int zb = p.z_begin + bz * ZPT;
     if (x >= p.X || y >= p.Y) return;
     const float ax = (x - 0.5f * (p.X - 1)) * p.pxy;
     const float ay = (y - 0.5f * (p.Y - 1)) * p.pxy;
@@ -229,6 +229,62 @@ __global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_mixed_kernel(BPPar
             p.sum[idx] = acc[k].x;
             p.cnt[idx] = acc[k].y;
         }
+    }
+}
+
+// One CTA = one 32 x 8 x ZPT voxel tile of one launch's grid.
+template <int ZPT, bool FINALIZE, bool EXACT, bool WZ>
+__global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_kernel(BPParams p) {
+    bp_block<ZPT, FINALIZE, EXACT, WZ>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <int ZPT, bool FINALIZE, bool WZ>
+__global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_mixed_kernel(BPParams p) {
+    bp_mixed_block<ZPT, FINALIZE, WZ>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Persistent backprojection over the tiles of several scans: each CTA takes
+// the next tile of the batch's work list (scans in order, tiles of a scan in
+// the grid order x, y, z) until the list is exhausted, so the tail of one
+// scan runs beside the start of the next.  The scan's parameters are copied
+// to shared memory per tile.
+template <bool MIXED>
+__global__ void __launch_bounds__(256, 4) bp_batch_kernel(const BatchScan* __restrict__ scans, int nscans,
+                                                          unsigned* __restrict__ counter, unsigned total) {
+    __shared__ BPParams sp;
+    __shared__ unsigned s_item;
+    __shared__ int s_scan;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (;;) {
+        if (tid == 0) {
+            const unsigned it = atomicAdd(counter, 1u);
+            int s = 0;
+            while (s + 1 < nscans && it >= scans[s + 1].first_tile) ++s;
+            s_item = it;
+            s_scan = s;
+        }
+        __syncthreads();
+        const unsigned it = s_item;
+        if (it >= total) break;
+        const BatchScan& b = scans[s_scan];
+        if (tid < (int)(sizeof(BPParams) / 4)) reinterpret_cast<int*>(&sp)[tid] = reinterpret_cast<const int*>(&b.p)[tid];
+        __syncthreads();
+        const unsigned local = it - b.first_tile;
+        const int bx = (int)(local % b.gx), by = (int)((local / b.gx) % b.gy), bz = (int)(local / (b.gx * b.gy));
+        if (MIXED) {
+            if (b.zpt == 4) {
+                if (b.wz) bp_mixed_block<4, true, true>(sp, bx, by, bz); else bp_mixed_block<4, true, false>(sp, bx, by, bz);
+            } else {
+                if (b.wz) bp_mixed_block<8, true, true>(sp, bx, by, bz); else bp_mixed_block<8, true, false>(sp, bx, by, bz);
+            }
+        } else {
+            if (b.zpt == 4) {
+                if (b.wz) bp_block<4, true, false, true>(sp, bx, by, bz); else bp_block<4, true, false, false>(sp, bx, by, bz);
+            } else {
+                if (b.wz) bp_block<8, true, false, true>(sp, bx, by, bz); else bp_block<8, true, false, false>(sp, bx, by, bz);
+            }
+        }
+        __syncthreads();   // sp and s_item are rewritten for the next tile
     }
 }
 
@@ -392,6 +448,28 @@ cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depen
 cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, cudaStream_t s) {
     if (finalize) return w_depends_on_z ? go_mixed2<true, true>(p, zpt, s) : go_mixed2<true, false>(p, zpt, s);
     return w_depends_on_z ? go_mixed2<false, true>(p, zpt, s) : go_mixed2<false, false>(p, zpt, s);
+}
+
+cudaError_t launch_bp_batch(const BatchScan* d_scans, int nscans, unsigned total_tiles, bool mixed_form,
+                            unsigned* counter, int ctas, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    if (mixed_form)
+        bp_batch_kernel<true><<<ctas, dim3(32, 8), 0, s>>>(d_scans, nscans, counter, total_tiles);
+    else
+        bp_batch_kernel<false><<<ctas, dim3(32, 8), 0, s>>>(d_scans, nscans, counter, total_tiles);
+    return cudaGetLastError();
+}
+
+cudaError_t bp_batch_ctas(bool mixed_form, int* ctas) {
+    int dev = 0, sms = 0, per = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = mixed_form ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bp_batch_kernel<true>, 256, 0)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bp_batch_kernel<false>, 256, 0);
+    *ctas = sms * (per > 0 ? per : 1);
+    return e;
 }
 
 cudaError_t launch_frame_absmax(const float* plain, long long frame, int nv, unsigned* absmax, cudaStream_t s) {

@@ -2,6 +2,9 @@
 // and the stage / whole-volume entry points.  No exception leaves this file.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <map>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -258,6 +261,65 @@ RampParams ramp_params(const jfdk_ctx* c, int nv, float* out) {
     return r;
 }
 
+}  // namespace
+
+namespace jfdk {
+
+// Everything jfdk_reconstruct does before the backprojection, for the first
+// nviews views: per chunk of views raw -> weighted rows -> filtered frames
+// (L2-sized buffers) -> [z-filter] -> the BP store of the rotation.
+jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nviews) {
+    if (nviews < 0 || nviews > c->nviews) nviews = c->nviews;
+    if (c->in_w != c->used_u)
+        return fail(c, JFDK_ERR_UNSUPPORTED, "reconstruct: conjugate-view compositing (filter width != frame width)");
+    jfdk_status st = ensure_Q4(c, c->nviews);
+    if (st) return st;
+    const int chunk = std::min(c->opt_view_chunk, c->nviews);
+    if ((st = ensure_A(c, (size_t)chunk * c->rows))) return st;
+    if ((st = ensure_plain(c, chunk))) return st;
+    const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;
+    for (int v0 = 0; v0 < nviews; v0 += chunk) {
+        const int nv = std::min(chunk, nviews - v0);
+        JFDK_LAUNCH(c, launch_prep_weight(prep_params(c, d_raw + (size_t)v0 * frame), nv, v0, weight_params(c),
+                                          a_operand(c), c->d_e, c->stream),
+                    "preprocess + pre-weight");
+        // mixed form with a tensor-core product: the product's epilogue
+        // leaves each frame's max |q| for the packer (no z-filter between)
+        RampParams rp = ramp_params(c, nv, c->d_plain);
+        const bool fused_max = mixed(c) && ramp_kind(c) != JFDK_RAMP_FP32_SIMT && !c->recon.z_filter;
+        if (fused_max) {
+            if ((st = ensure_absmax(c, nv))) return st;
+            JFDK_CUDA(c, cudaMemsetAsync(c->d_absmax, 0, sizeof(unsigned) * nv, c->stream), "clearing the maxima");
+            rp.absmax = c->d_absmax;
+        }
+        JFDK_LAUNCH(c, launch_ramp(c, rp), "ramp filter");
+        if (c->recon.z_filter)
+            JFDK_LAUNCH(c, launch_zfilter(c->d_plain, nv, c->rows, c->out_w, frame_px(c), c->out_w, c->stream),
+                        "z-filter");
+        if ((st = pack_frames(c, c->d_plain, nv, v0, v0, fused_max))) return st;
+    }
+    return JFDK_OK;
+}
+
+// The finalizing backprojection of every view into d_hu / d_hu16 with CT
+// numbers (the store filled by reconstruct_filter_stage).
+BPParams reconstruct_bp_params(const jfdk_ctx* c, float* d_hu, int16_t* d_hu16) {
+    BPParams b = bp_params(c);
+    b.view_base = 0; b.v0 = 0; b.nv = c->nviews;
+    b.out = d_hu; b.out16 = d_hu16; b.apply_ct = 1;
+    if (mixed(c)) {
+        b.qh = reinterpret_cast<const uint4*>(c->d_q4);
+        b.qscale = c->d_qscale;
+    }
+    return b;
+}
+
+int bp_slices_per_thread(const jfdk_ctx* c) { return bp_zpt(c); }
+bool mixed_form(const jfdk_ctx* c) { return mixed(c); }
+
+}  // namespace jfdk
+
+namespace {
 }  // namespace
 
 extern "C" {
@@ -591,44 +653,13 @@ jfdk_status jfdk_ctnum(jfdk_ctx* c, float* d, size_t n) {
 
 jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, int16_t* d_hu16) {
     if (!c || !d_raw || (!d_hu && !d_hu16)) return fail(c, JFDK_ERR_INVALID, "reconstruct: bad argument");
-    if (c->in_w != c->used_u)
-        return fail(c, JFDK_ERR_UNSUPPORTED, "reconstruct: conjugate-view compositing (filter width != frame width)");
-    jfdk_status st = ensure_Q4(c, c->nviews);
-    if (st) return st;
-    const int chunk = std::min(c->opt_view_chunk, c->nviews);
-    if ((st = ensure_A(c, (size_t)chunk * c->rows))) return st;
-    if ((st = ensure_plain(c, chunk))) return st;
-    const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;
     const bool timing = c->opt_stage_timing != 0;
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[0], c->stream), "event");
-    // per chunk of views: raw -> weighted rows -> filtered frames (L2-sized
-    // buffers) -> [z-filter] -> tapered quads of the whole rotation
-    for (int v0 = 0; v0 < c->nviews; v0 += chunk) {
-        const int nv = std::min(chunk, c->nviews - v0);
-        JFDK_LAUNCH(c, launch_prep_weight(prep_params(c, d_raw + (size_t)v0 * frame), nv, v0, weight_params(c),
-                                          a_operand(c), c->d_e, c->stream),
-                    "preprocess + pre-weight");
-        // mixed form with a tensor-core product: the product's epilogue
-        // leaves each frame's max |q| for the packer (no z-filter between)
-        RampParams rp = ramp_params(c, nv, c->d_plain);
-        const bool fused_max = mixed(c) && ramp_kind(c) != JFDK_RAMP_FP32_SIMT && !c->recon.z_filter;
-        if (fused_max) {
-            if ((st = ensure_absmax(c, nv))) return st;
-            JFDK_CUDA(c, cudaMemsetAsync(c->d_absmax, 0, sizeof(unsigned) * nv, c->stream), "clearing the maxima");
-            rp.absmax = c->d_absmax;
-        }
-        JFDK_LAUNCH(c, launch_ramp(c, rp), "ramp filter");
-        if (c->recon.z_filter)
-            JFDK_LAUNCH(c, launch_zfilter(c->d_plain, nv, c->rows, c->out_w, frame_px(c), c->out_w, c->stream),
-                        "z-filter");
-        if ((st = pack_frames(c, c->d_plain, nv, v0, v0, fused_max))) return st;
-    }
+    jfdk_status st = jfdk::reconstruct_filter_stage(c, d_raw, c->nviews);
+    if (st) return st;
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[1], c->stream), "event");
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[2], c->stream), "event");
-    BPParams b = bp_params(c);
-    b.view_base = 0; b.v0 = 0; b.nv = c->nviews;
-    b.out = d_hu; b.out16 = d_hu16; b.apply_ct = 1;
-    if ((st = run_bp(c, b, true))) return st;
+    if ((st = run_bp(c, jfdk::reconstruct_bp_params(c, d_hu, d_hu16), true))) return st;
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[3], c->stream), "event");
     return JFDK_OK;
 }
@@ -782,3 +813,133 @@ jfdk_status jfdk_geometry_gradient(jfdk_ctx* c, const float* d_q, int v0, int nv
 }
 
 }  // extern "C"
+
+// ---- autotuner -------------------------------------------------------------
+
+namespace {
+
+std::mutex g_tune_mutex;
+std::map<std::string, std::pair<int, int>> g_tune_cache;   // shape -> (slices per thread, views per chunk)
+bool g_tune_file_read = false;
+
+std::string tune_key(const jfdk_ctx* c) {
+    char k[256];
+    std::snprintf(k, sizeof k, "p%d_r%d_v%d_u%d_h%d_w%d_x%d_y%d_z%d_wz%d", c->precision, ramp_kind(c), c->nviews,
+                  c->used_u, c->used_v, c->in_w, c->X, c->Y, c->Z, c->w_depends_on_z ? 1 : 0);
+    return k;
+}
+
+// Optional persistent cache: $JFDK_AUTOTUNE_CACHE, lines "key zpt chunk".
+void tune_file_load() {
+    if (g_tune_file_read) return;
+    g_tune_file_read = true;
+    const char* path = std::getenv("JFDK_AUTOTUNE_CACHE");
+    if (!path) return;
+    std::FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    char key[256];
+    int z, ch;
+    while (std::fscanf(f, "%255s %d %d", key, &z, &ch) == 3)
+        if ((z == 4 || z == 8) && (ch == 16 || ch == 32 || ch == 64)) g_tune_cache[key] = {z, ch};
+    std::fclose(f);
+}
+
+void tune_file_append(const std::string& key, int z, int ch) {
+    const char* path = std::getenv("JFDK_AUTOTUNE_CACHE");
+    if (!path) return;
+    std::FILE* f = std::fopen(path, "a");
+    if (!f) return;
+    std::fprintf(f, "%s %d %d\n", key.c_str(), z, ch);
+    std::fclose(f);
+}
+
+// The smaller of two timed runs after one warm-up run.
+template <class F>
+jfdk_status time_ms(jfdk_ctx* c, F&& run, float* ms) {
+    cudaEvent_t a, b;
+    JFDK_CUDA(c, cudaEventCreate(&a), "event");
+    JFDK_CUDA(c, cudaEventCreate(&b), "event");
+    jfdk_status st = run();
+    float best = 1e30f;
+    for (int i = 0; i < 2 && !st; ++i) {
+        cudaEventRecord(a, c->stream);
+        st = run();
+        cudaEventRecord(b, c->stream);
+        cudaEventSynchronize(b);
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, a, b);
+        best = std::min(best, t);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms = best;
+    return st;
+}
+
+}  // namespace
+
+extern "C" jfdk_status jfdk_autotune(jfdk_ctx* c, int flags) {
+    if (!c) return JFDK_ERR_INVALID;
+    const std::string key = tune_key(c);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        tune_file_load();
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end() && !(flags & JFDK_AUTOTUNE_FORCE)) {
+            c->opt_bp_zpt = it->second.first;
+            c->opt_view_chunk = it->second.second;
+            return JFDK_OK;
+        }
+    }
+    jfdk_status st = ensure_Q4(c, c->nviews);
+    if (st) return st;
+    // voxel tile depth: a finalizing backprojection of a central slab into a
+    // slab-sized buffer (the kernel indexes the output by absolute slice, so
+    // it is given the buffer's address minus the slab's offset)
+    const int nz = std::min(c->Z, 32);
+    const int z0 = (c->Z - nz) / 2;
+    const size_t plane = (size_t)c->X * c->Y;
+    float* slab = nullptr;
+    if ((st = dev_alloc(c, &slab, plane * nz, "the autotuner's slab"))) return st;
+    int best_z = 8;
+    float best_t = 1e30f;
+    for (int zpt : {4, 8}) {
+        c->opt_bp_zpt = zpt;
+        BPParams b = jfdk::reconstruct_bp_params(c, slab - (ptrdiff_t)(z0 * plane), nullptr);
+        b.z_begin = z0;
+        b.z_end = z0 + nz;
+        b.apply_ct = 0;
+        float t = 0.0f;
+        st = time_ms(c, [&] { return run_bp(c, b, true); }, &t);
+        if (st) break;
+        if (t < best_t) { best_t = t; best_z = zpt; }
+    }
+    dev_free(slab);
+    if (st) return st;
+    c->opt_bp_zpt = best_z;
+    // views per chunk: the filter stage over the first views of zero frames
+    int best_c = c->opt_view_chunk;
+    if (c->in_w == c->used_u) {
+        const int nsub = std::min(c->nviews, 128);
+        uint16_t* raw = nullptr;
+        const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;
+        if ((st = dev_alloc(c, &raw, frame * nsub, "the autotuner's frames"))) return st;
+        JFDK_CUDA(c, cudaMemsetAsync(raw, 0, frame * nsub * sizeof(uint16_t), c->stream), "autotune");
+        best_t = 1e30f;
+        for (int ch : {16, 32, 64}) {
+            c->opt_view_chunk = ch;
+            float t = 0.0f;
+            st = time_ms(c, [&] { return jfdk::reconstruct_filter_stage(c, raw, nsub); }, &t);
+            if (st) break;
+            if (t < best_t) { best_t = t; best_c = ch; }
+        }
+        cudaStreamSynchronize(c->stream);
+        dev_free(raw);
+        if (st) return st;
+    }
+    c->opt_view_chunk = best_c;
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    g_tune_cache[key] = {best_z, best_c};
+    tune_file_append(key, best_z, best_c);
+    return JFDK_OK;
+}

@@ -54,9 +54,27 @@ struct BPParams {
     float ct_scale, ct_norm1;
 };
 
+// One scan of a batched backprojection (bp_batch_kernel): its parameters
+// (finalizing launch over all its views), its grid and its first tile in the
+// batch's work list.
+struct BatchScan {
+    BPParams p;
+    unsigned first_tile;
+    int gx, gy, gz;
+    int zpt;                 // 4 or 8
+    int wz;                  // W depends on z
+    int pad[2];
+};
+
 // Launchers (return cudaError_t of the launch).
 // zpt: slices per thread (4, 8 or 16).
 cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, cudaStream_t s);
+// All tiles of nscans scans in one persistent launch of `ctas` CTAs (the
+// SMs' resident CTAs); *counter is the work-list cursor (cleared here).
+cudaError_t launch_bp_batch(const BatchScan* d_scans, int nscans, unsigned total_tiles, bool mixed_form,
+                            unsigned* counter, int ctas, cudaStream_t s);
+// CTAs of a full persistent wave: SMs x resident CTAs per SM.
+cudaError_t bp_batch_ctas(bool mixed_form, int* ctas);
 // Mixed-precision form: FP16 footprints with a per-view scale (qh, qscale).
 cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, cudaStream_t s);
 // absmax[f] = bit pattern of max |plain[f][...]| over each of nv frames.
@@ -243,3 +261,12 @@ struct jfdk_ctx {
     long long launches = 0;
     std::string err;
 };
+
+namespace jfdk {
+// Stages of jfdk_reconstruct, shared with the batch (batch.cpp).
+// nviews: the first views only (the autotuner), or all when out of range.
+jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nviews);
+BPParams reconstruct_bp_params(const jfdk_ctx* c, float* d_hu, int16_t* d_hu16);
+int bp_slices_per_thread(const jfdk_ctx* c);
+bool mixed_form(const jfdk_ctx* c);
+}  // namespace jfdk

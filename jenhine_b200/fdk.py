@@ -154,6 +154,11 @@ class FDKEngine:
     def kernel_launches(self) -> int:
         return self.lib.jfdk_kernel_launches(self.ctx)
 
+    def autotune(self, force: bool = False):
+        """Pick slices per thread and views per chunk for this shape (timed on
+        the device; cached per shape)."""
+        self._check(self.lib.jfdk_autotune(self.ctx, _lib.AUTOTUNE_FORCE if force else 0))
+
     def set_option(self, key: int, value: int):
         self._check(self.lib.jfdk_set_option(self.ctx, key, int(value)))
 
@@ -279,3 +284,59 @@ class FDKEngine:
         self._check(self.lib.jfdk_geometry_gradient(self.ctx, _ptr(q), v0, nv, _ptr(vol), _ptr(vol_bar),
                                                     _ptr(dptm), _ptr(out)))
         return out
+
+
+class FDKBatch:
+    """Scans of uneven size reconstructed together: each scan's filter stage,
+    then one persistent backprojection launch over all scans' tiles, recorded
+    as a CUDA graph on the first run with a set of buffers and replayed after.
+
+        batch = FDKBatch([engine_0, ..., engine_n], autotune=True)
+        batch.run([raw_0, ...], [vol_0, ...])   # torch CUDA tensors
+    """
+
+    def __init__(self, engines, autotune: bool = True, graph: bool = True, stream=None):
+        import torch
+        self.lib = _lib.load()
+        self.h = None
+        self.engines = list(engines)
+        self.stream = stream if stream is not None else torch.cuda.Stream()
+        arr = (C.c_void_p * len(self.engines))(*[e.ctx for e in self.engines])
+        h = C.c_void_p()
+        flags = (_lib.BATCH_AUTOTUNE if autotune else 0) | (_lib.BATCH_GRAPH if graph else 0)
+        st = self.lib.jfdk_batch_create(C.byref(h), arr, len(self.engines), flags,
+                                        C.c_void_p(self.stream.cuda_stream))
+        self.h = h.value
+        if st != _lib.JFDK_OK:
+            msg = self.lib.jfdk_batch_last_error(self.h).decode() if self.h else ""
+            self.close()
+            raise _lib.JfdkError(st, msg)
+
+    def run(self, raws, outs):
+        """Reconstruct every scan (HU volumes into outs), ordered after the
+        caller's current stream, and the caller's stream after it."""
+        import torch
+        cur = torch.cuda.current_stream()
+        self.stream.wait_stream(cur)
+        r = (C.c_void_p * len(raws))(*[x.data_ptr() for x in raws])
+        o = (C.c_void_p * len(outs))(*[x.data_ptr() for x in outs])
+        st = self.lib.jfdk_batch_run(self.h, r, o)
+        if st != _lib.JFDK_OK:
+            raise _lib.JfdkError(st, self.lib.jfdk_batch_last_error(self.h).decode())
+        cur.wait_stream(self.stream)
+        return outs
+
+    @property
+    def launches(self) -> int:
+        return self.lib.jfdk_batch_launches(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.jfdk_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

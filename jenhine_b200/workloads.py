@@ -11,6 +11,7 @@ c2  dental-CBCT size, plain FP32: 600 views over 360 deg, 768 x 768 detector
     case; it uses c1's SID 500 mm / SDD 800 mm.
 c3  differentiation: 360 views of 512 x 512 at 0.5 mm -> 256^3 at 0.4 mm
     (the detector pitch is not given for this case; 0.5 mm covers the volume).
+batch  16 seeded scans of uneven size for the batched launch (batch()).
 mini_*  reduced versions of c1 / c2 for parity tests.
 
 The reference corrects gain with one scalar bright field
@@ -20,6 +21,8 @@ properties of the synthetic detector, left in the raw frames.
 from __future__ import annotations
 
 import dataclasses
+
+import numpy as np
 
 from .fdk import ReconConfig, ScanConfig
 from .phantom import ScanGeometry, random_phantom
@@ -85,6 +88,32 @@ def c3() -> Workload:
     +/- 0.5 mm / +/- 0.3 deg is the geometry the gradient is taken at."""
     return Workload("c3", ScanGeometry(360, 500.0, 800.0, 512, 512, 0.5, 0.5, seed=303),
                     ReconConfig(256, 256, 256, 0.4, 0.4, ct_norm0=1.0, ct_norm1=1.0), 10, 0, 1e5)
+
+
+BATCH_VOLUMES = ((128, 128, 128), (256, 256, 256), (384, 384, 256), (512, 512, 400))
+BATCH_VIEWS = (180, 360, 600, 720)
+BATCH_DETECTORS = (256, 512, 768, 1024)
+
+
+def batch(n: int = 16, seed: int = 404) -> list:
+    """Batching: n scans of uneven size, each drawn by seed -- volume from
+    BATCH_VOLUMES, views from BATCH_VIEWS, square detector from
+    BATCH_DETECTORS, SID 450-600 mm, SDD 700-900 mm.  The detector is 200 mm
+    wide (pixel = 200 / width mm) and the volume 100 mm across in x and y
+    (cubic voxels); neither is given for this case.  10-ellipsoid phantoms."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        X, Y, Z = BATCH_VOLUMES[rng.integers(len(BATCH_VOLUMES))]
+        views = int(BATCH_VIEWS[rng.integers(len(BATCH_VIEWS))])
+        det = int(BATCH_DETECTORS[rng.integers(len(BATCH_DETECTORS))])
+        sid = float(rng.uniform(450.0, 600.0))
+        sdd = float(rng.uniform(700.0, 900.0))
+        pix = 200.0 / det
+        vox = 100.0 / X
+        out.append(Workload(f"batch{i}", ScanGeometry(views, sid, sdd, det, det, pix, pix, seed=seed * 100 + i),
+                            ReconConfig(X, Y, Z, vox, vox, ct_norm0=1.0, ct_norm1=1.0), 10, 0, 1e5))
+    return out
 
 
 def c2_slab() -> Workload:

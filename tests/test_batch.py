@@ -1,0 +1,79 @@
+"""Batches of scans of uneven size (jfdk_batch_*, jfdk_autotune): one persistent
+backprojection launch over all scans' tiles, recorded as a CUDA graph and
+replayed.  Each scan's volume must equal its own jfdk_reconstruct bit for
+bit with the same options: the batch runs the same per-voxel arithmetic.  In
+the FP32 form the options the autotuner picks (tile depth, views per chunk)
+do not change the arithmetic either; in the mixed form the coordinates step
+from each thread's first slice, so the tile depth moves u, v by rounding and
+the single reconstructions are taken with the batch's tuned options."""
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# (views, detector, volume) of four small scans of uneven size
+SHAPES = [(36, 48, (24, 24, 24)), (60, 64, (32, 32, 20)), (24, 40, (16, 16, 16)), (48, 56, (40, 24, 12))]
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    return torch
+
+
+def make_scans(precision, shapes=SHAPES):
+    from jenhine_b200.fdk import FDKEngine, ReconConfig
+    from jenhine_b200.phantom import ScanGeometry
+    from jenhine_b200.workloads import Workload
+    out = []
+    for i, (views, det, (X, Y, Z)) in enumerate(shapes):
+        pix = 60.0 / det
+        vox = 30.0 / X
+        w = Workload(f"s{i}", ScanGeometry(views, 480.0 + 20 * i, 760.0 + 30 * i, det, det, pix, pix, seed=900 + i),
+                     ReconConfig(X, Y, Z, vox, vox, ct_norm0=1.0, ct_norm1=1.0), 6, 0, 1e5)
+        e = FDKEngine(w.scan, w.recon, w.geom.ptms(), precision=precision)
+        out.append((w, e, w.raw_torch()))
+    return out
+
+
+def same(torch, a, b):
+    return torch.equal(torch.nan_to_num(a, 1e30), torch.nan_to_num(b, 1e30))
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_batch_equals_single_reconstructions(torch_cuda, precision):
+    torch = torch_cuda
+    from jenhine_b200.fdk import FDKBatch
+    scans = make_scans(precision)
+    untuned = [e.reconstruct(raw).clone() for _, e, raw in scans]
+    batch = FDKBatch([e for _, e, _ in scans], autotune=True, graph=True)
+    refs = [e.reconstruct(raw).clone() for _, e, raw in scans]   # with the tuned options
+    if precision == "fp32":
+        assert all(same(torch, u, r) for u, r in zip(untuned, refs))
+    raws = [raw for _, _, raw in scans]
+    outs = [torch.full_like(r, -7.0) for r in refs]
+    batch.run(raws, outs)            # direct run, recorded as a graph
+    torch.cuda.synchronize()
+    assert all(same(torch, o, r) for o, r in zip(outs, refs))
+    for o in outs:
+        o.fill_(-7.0)
+    n0 = batch.launches
+    batch.run(raws, outs)            # graph replay
+    torch.cuda.synchronize()
+    assert batch.launches > n0
+    assert all(same(torch, o, r) for o, r in zip(outs, refs))
+    outs2 = [torch.empty_like(r) for r in refs]
+    batch.run(raws, outs2)           # new buffers: recorded again
+    torch.cuda.synchronize()
+    assert all(same(torch, o, r) for o, r in zip(outs2, refs))
+    batch.close()
+
+
+def test_batch_rejects_mixed_forms(torch_cuda):
+    from jenhine_b200 import _lib
+    from jenhine_b200.fdk import FDKBatch
+    a = make_scans("fp32", SHAPES[:1])
+    b = make_scans("mixed", SHAPES[:1])
+    with pytest.raises(_lib.JfdkError):
+        FDKBatch([a[0][1], b[0][1]], autotune=False)
