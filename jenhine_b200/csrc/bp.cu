@@ -130,12 +130,17 @@ __device__ __forceinline__ void bp_block(const BPParams& p, int bx, int by, int 
 }
 
 // ---- mixed precision ---------------------------------------------------------
-// Record per (slot, row r, column c), 16 bytes:
-//   .x  half2 (p[r][c], p[r+1][c]) / s       the tapered footprint, divided by
-//   .y  half2 (p[r][c+1], p[r+1][c+1]) / s   the view's power-of-two scale s
-//   .z  float w[c]                           the taper at c
-//   .w  float w[c+1] - w[c]                  and its step to c+1
-// so one 16-byte load per sample fetches everything the sample needs.
+// Record per (slot, row r, column c), 16 bytes: the tapered footprint
+// p00 = p[r][c], p01 = p[r][c+1], p10 = p[r+1][c], p11 = p[r+1][c+1],
+// divided by the view's power-of-two scale s, as the coefficients of the
+// bilinear form  val = p00 + fx dx + fy (dy + fx dxy):
+//   .x  half2 (p00, dx = p01 - p00) / s
+//   .y  half2 (dy = p10 - p00, dxy = p11 - p10 - p01 + p00) / s
+//   .z  float w[c]                 the taper at c
+//   .w  float w[c+1] - w[c]        and its step to c+1
+// so one 16-byte load per sample fetches everything the sample needs, and
+// the interpolation is two FP16 x FP16 + FP32 fused multiply-adds
+// (fma.rn.f32.f16, products exact in FP32) and one FP32 one.
 // The coordinates use an approximate reciprocal of W and fused
 // multiply-adds; when W does not depend on z the slices of a thread are
 // equally spaced on the detector and u, v advance by a constant per slice.
@@ -169,7 +174,7 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, int bx, int by
                      : f2(0.0f, 0.0f);
     }
     const unsigned um1 = (unsigned)(p.U - 1), vm1 = (unsigned)(p.V - 1), uu = (unsigned)p.U;
-    const float2 neg1 = f2(-1.0f, -1.0f), magic = f2(kMagic, kMagic);
+    const float2 magic = f2(kMagic, kMagic);
 
     const float4* P4 = reinterpret_cast<const float4*>(p.ptm + (size_t)p.v0 * 12);
     const float* sc = p.qscale + p.v0;
@@ -208,10 +213,14 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, int bx, int by
             const bool in = (iu < um1) & (iv < vm1);                  // negative / NaN wrap to large
             const unsigned idx = in ? iv * uu + iu : 0u;
             const uint4 rec = __ldg(q + idx);
-            const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&rec.x));  // column c, rows r, r+1
-            const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&rec.y));  // column c+1
-            const float2 tb = pfma(f2(f.x, f.x), pfma(lo, neg1, hi), lo);
-            const float val = fmaf(f.y, tb.y - tb.x, tb.x);
+            float v1, inner;   // p00 + fx dx, dy + fx dxy (fx rounded to FP16)
+            asm("{\n .reg .f16 a, dx, dy, dxy, fh;\n .reg .f32 af, dyf;\n"
+                " mov.b32 {a, dx}, %2;\n mov.b32 {dy, dxy}, %3;\n"
+                " cvt.rn.f16.f32 fh, %4;\n cvt.f32.f16 af, a;\n cvt.f32.f16 dyf, dy;\n"
+                " fma.rn.f32.f16 %0, fh, dx, af;\n fma.rn.f32.f16 %1, fh, dxy, dyf;\n}"
+                : "=f"(v1), "=f"(inner)
+                : "r"(rec.x), "r"(rec.y), "f"(f.x));
+            const float val = fmaf(f.y, inner, v1);
             const float c = fmaf(f.x, __uint_as_float(rec.w), __uint_as_float(rec.z));
             if (in) acc[k] = pfma(f2(s, 1.0f), f2(val, c), acc[k]);
         }
@@ -302,13 +311,14 @@ __global__ void __launch_bounds__(256) frame_absmax_kernel(const float* __restri
     if ((threadIdx.x & 31) == 0) atomicMax(out + blockIdx.y, __float_as_uint(m));
 }
 
-// Power-of-two scale of a view: max |q| / s lies in [2^13, 2^14), so a
-// stored value and the difference of two (below 2^15) stay inside the FP16
-// range, and dividing by s is exact.  An all-zero (or non-finite) view gets 1.
+// Power-of-two scale of a view: max |q| / s lies in [2^12, 2^13), so every
+// coefficient of the bilinear form (|dxy| < 4 max) stays inside the FP16
+// range (65504), and dividing by s is exact.  An all-zero (or non-finite)
+// view gets 1.
 __device__ __forceinline__ float view_scale(unsigned maxbits) {
     const float m = __uint_as_float(maxbits);
     if (!(m > 0.0f) || !(m <= 3.0e38f)) return 1.0f;
-    return ldexpf(1.0f, ilogbf(m) - 13);
+    return ldexpf(1.0f, ilogbf(m) - 12);
 }
 
 // Filtered frames -> mixed-precision records in slots [slot0, slot0 + nv),
@@ -331,8 +341,17 @@ __global__ void __launch_bounds__(256) pack_mixed_kernel(const float* __restrict
     const float2 w = tw[(size_t)view * U + c];
     const float p00 = src[0] * w.x, p10 = down ? src[U] * w.x : 0.0f;
     const float p01 = right ? src[1] * w.y : 0.0f, p11 = (right && down) ? src[U + 1] * w.y : 0.0f;
-    const __half2 lo = __floats2half2_rn(p00 * inv, p10 * inv);
-    const __half2 hi = __floats2half2_rn(p01 * inv, p11 * inv);
+    // Each coefficient is rounded against the already rounded ones, so every
+    // corner the form reproduces carries the rounding of one coefficient
+    // only: p00 that of a, p01 that of dx (a difference, usually far smaller
+    // than the values), p10 that of dy, p11 that of dxy.
+    const float a = p00 * inv, b = p01 * inv, cc = p10 * inv, d = p11 * inv;   // exact: inv a power of two
+    const __half ha = __float2half_rn(a);
+    const float ra = __half2float(ha);
+    const __half hdx = __float2half_rn(b - ra), hdy = __float2half_rn(cc - ra);
+    const __half hdxy = __float2half_rn(d - (ra + __half2float(hdx) + __half2float(hdy)));
+    const __half2 lo = __halves2half2(ha, hdx);
+    const __half2 hi = __halves2half2(hdy, hdxy);
     uint4 rec;
     rec.x = *reinterpret_cast<const unsigned*>(&lo);
     rec.y = *reinterpret_cast<const unsigned*>(&hi);
