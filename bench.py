@@ -302,13 +302,13 @@ def time_form(a, w, raw, ptms, precision, dist, world, local):
     return out
 
 
-def roofline(w, bp_ms, kernel, prof):
+def roofline(w, bp_ms, kernel, prof, proj_bytes=4):
     """HBM roofline of the backprojection kernel: algorithmic bytes (the
-    filtered projections read once, the volume written once) over its
-    CUDA-event time."""
+    filtered projections read once at proj_bytes per sample, the volume
+    written once) over its CUDA-event time."""
     peak, peak_kind = measured_peaks()
     r, g = w.recon, w.geom
-    alg = g.n_views * g.det_v * g.det_u * 4 + r.num_pixels_x * r.num_pixels_y * r.num_pixels_z * 4
+    alg = g.n_views * g.det_v * g.det_u * proj_bytes + r.num_pixels_x * r.num_pixels_y * r.num_pixels_z * 4
     achieved = alg / (bp_ms / 1000.0) / 1e9
     return {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs ({'of measured' if peak_kind == 'measured' else 'of fallback'})",
@@ -444,7 +444,8 @@ def main():
             "stages_ms": head["stages_ms"],
             "roofline": roofline(w, head["stages_ms"]["backprojection_hu"],
                                  "bp_kernel (backprojection + normalisation + CT numbers)",
-                                 f"bp_kernel_{w.name}" if forms[0] == "fp32" else f"bp_mixed_kernel_{w.name}"),
+                                 f"bp_kernel_{w.name}" if forms[0] == "fp32" else f"bp_mixed_kernel_{w.name}",
+                                 proj_bytes=4 if forms[0] == "fp32" else 2),
             "gpu_launches": sum(r["gpu_launches"] for r in res.values()),
             "clocks": head["clocks"],
         }
@@ -453,7 +454,8 @@ def main():
         if len(forms) == 2:
             m = dict(res["mixed"])
             m["roofline"] = roofline(w, m["stages_ms"]["backprojection_hu"],
-                                     "bp_mixed_kernel (FP16 records, FP32 accumulation)", f"bp_mixed_kernel_{w.name}")
+                                     "bp_mixed_kernel (FP16 records, FP32 accumulation)", f"bp_mixed_kernel_{w.name}",
+                                     proj_bytes=2)
             m["speedup_vs_fp32"] = head["ms_per_step"] / m["ms_per_step"]
             line["forms"] = {"fp32": {k: v for k, v in head.items()}, "mixed": m}
         if not a.no_cpu_baseline and world == 1:
