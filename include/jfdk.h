@@ -130,12 +130,24 @@ jfdk_status jfdk_filter_frames(jfdk_ctx* ctx, const float* d_in, int v0, int nv,
  * loads the library until the process exits) instead of memory allocated on
  * first use; nothing is allocated or freed.  Limit: nv * rows * pitch + nv *
  * rows floats must fit in 1,048,576 floats, where pitch is filter_in_w rounded
- * up to a multiple of 16 (for a 768 x 768 frame: one view per call); larger
+ * up to a multiple of 64 (for a 768 x 768 frame: one view per call); larger
  * requests return JFDK_ERR_INVALID.  The first call on each device looks up
  * the array's device address (with that device current) and caches it: make
  * that first call before any stream capture.  All calls share the array:
  * calls whose kernels can overlap on the GPU race and must be serialised. */
 jfdk_status jfdk_filter_frames_noalloc(jfdk_ctx* ctx, const float* d_in, int v0, int nv, float* d_out);
+
+/* CompositeAgent::ProcessTask + CompositeCore::Process
+ * (CompositeAgent/CompositeAgent.cpp:72-83, CompositeCore.cpp:59-149):
+ * nv pairs of preprocessed frames -- d_dirc[f] of view v0 + f and d_conj[f] of
+ * view (v0 + f + N/2) % N, each rows x width -- into d_out, nv x rows x
+ * (2 width): the direct frame in one half (the right half when
+ * detector_on_right), in the other the conjugate frame resampled at the points
+ * the direct view's extended detector sees, blended with the direct edge over
+ * 40 columns.  The context must have filter_input_width = 2 x the frame width
+ * (JFDK_ERR_STATE otherwise); jfdk_reconstruct then composites on the fly. */
+jfdk_status jfdk_composite_frames(jfdk_ctx* ctx, const float* d_dirc, const float* d_conj, int v0, int nv,
+                                  float* d_out);
 
 /* ZFilterAgent::ProcessTask (FilterAgent/ZFilterAgent.cpp:49-71) in place on
  * nv frames of rows x width. */

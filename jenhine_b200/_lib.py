@@ -79,6 +79,7 @@ _SIGS = {
     "jfdk_filter_frames": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
     "jfdk_filter_frames_noalloc": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
     "jfdk_zfilter_frames": ([_P, _P, C.c_int], C.c_int),
+    "jfdk_composite_frames": ([_P, _P, _P, C.c_int, C.c_int, _P], C.c_int),
     "jfdk_bp_reset": ([_P], C.c_int),
     "jfdk_bp_accumulate": ([_P, _P, C.c_int, C.c_int], C.c_int),
     "jfdk_finalize": ([_P, C.c_int, C.c_int, C.c_int, _P, _P], C.c_int),

@@ -226,6 +226,24 @@ std::string build_host_operators(const jfdk_scan_params& scan, const jfdk_recon_
         if (!invert4_f64(md, inv)) return "singular transform matrix for view " + std::to_string(src);
         for (int i = 0; i < 16; ++i) ops.tinv[(size_t)g * 16 + i] = (float)inv[i];
     }
+    // -- inverse transform matrix of every view, solved in float in LAPACK's
+    //    order like CompositeCore::Inverse (CompositeAgent/CompositeCore.cpp:186-191),
+    //    one right-hand side (a column of I) at a time --
+    ops.tinv_view.assign((size_t)N * 16, 0.0f);
+    for (int v = 0; v < N; ++v) {
+        const float* P = ptms + (size_t)v * 12;
+        float tm[16];
+        std::memcpy(tm, P, 8 * sizeof(float));
+        tm[8] = s20 * P[8]; tm[9] = s20 * P[9]; tm[10] = 0.0f; tm[11] = s23 * P[11];
+        std::memcpy(tm + 12, P + 8, 4 * sizeof(float));
+        for (int j = 0; j < 4; ++j) {
+            float A[16], e[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            std::memcpy(A, tm, sizeof A);
+            e[j] = 1.0f;
+            solve4_f32(A, e);
+            for (int i = 0; i < 4; ++i) ops.tinv_view[(size_t)v * 16 + i * 4 + j] = e[i];
+        }
+    }
     // -- filter spectrum and the equivalent dense operator --
     const int L = fft_length(in_w);
     ops.H = filter_spectrum(L, hsr, recon.filter_cutoff_start, recon.filter_cutoff_end, adj_pts, adj_db);

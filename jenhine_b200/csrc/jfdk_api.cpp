@@ -146,6 +146,23 @@ jfdk_status ensure_acc(jfdk_ctx* c) {
     return dev_alloc(c, &c->d_cnt, n, "the backprojection weight volume");
 }
 
+// Conjugate-view compositing is on when the filter reads rows twice the
+// frame width (the reference's CompositeAgent -> FilterAgent(2U) chain).
+bool compositing(const jfdk_ctx* c) { return c->in_w == 2 * c->used_u; }
+
+CompositeParams composite_params(const jfdk_ctx* c) {
+    CompositeParams p{};
+    if (!compositing(c)) return p;
+    p.tinv = c->d_tinv_view;
+    p.ptm = c->d_ptm;
+    p.mask = c->d_cmask;
+    p.num_views = c->nviews;
+    p.W = c->used_u;
+    p.H = c->used_v;
+    p.det_right = c->mirror;
+    return p;
+}
+
 WeightParams weight_params(const jfdk_ctx* c) {
     WeightParams w{};
     w.tinv = c->d_tinv;
@@ -155,6 +172,14 @@ WeightParams weight_params(const jfdk_ctx* c) {
     w.det_right = c->mirror;
     w.mirror = c->mirror;
     w.pw = c->d_pw;
+    return w;
+}
+
+// Weight pass over raw frames: with compositing, rows are composited first
+// (the conjugate frames come from the same rotation).
+WeightParams weight_params_raw(const jfdk_ctx* c) {
+    WeightParams w = weight_params(c);
+    w.comp = composite_params(c);
     return w;
 }
 
@@ -270,8 +295,9 @@ namespace jfdk {
 // (L2-sized buffers) -> [z-filter] -> the BP store of the rotation.
 jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nviews) {
     if (nviews < 0 || nviews > c->nviews) nviews = c->nviews;
-    if (c->in_w != c->used_u)
-        return fail(c, JFDK_ERR_UNSUPPORTED, "reconstruct: conjugate-view compositing (filter width != frame width)");
+    if (c->in_w != c->used_u && !compositing(c))
+        return fail(c, JFDK_ERR_UNSUPPORTED,
+                    "reconstruct: filter input width must be the frame width or twice it (compositing)");
     jfdk_status st = ensure_Q4(c, c->nviews);
     if (st) return st;
     const int chunk = std::min(c->opt_view_chunk, c->nviews);
@@ -280,9 +306,14 @@ jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nvi
     const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;
     for (int v0 = 0; v0 < nviews; v0 += chunk) {
         const int nv = std::min(chunk, nviews - v0);
-        JFDK_LAUNCH(c, launch_prep_weight(prep_params(c, d_raw + (size_t)v0 * frame), nv, v0, weight_params(c),
-                                          a_operand(c), c->d_e, c->stream),
-                    "preprocess + pre-weight");
+        PrepParams pp = prep_params(c, d_raw + (size_t)v0 * frame);
+        if (compositing(c)) {
+            pp.width = c->in_w;
+            pp.raw_rotation = d_raw;
+            pp.raw_frame = (long long)frame;
+        }
+        JFDK_LAUNCH(c, launch_prep_weight(pp, nv, v0, weight_params_raw(c), a_operand(c), c->d_e, c->stream),
+                    compositing(c) ? "preprocess + compositing + pre-weight" : "preprocess + pre-weight");
         // mixed form with a tensor-core product: the product's epilogue
         // leaves each frame's max |q| for the packer (no z-filter between)
         RampParams rp = ramp_params(c, nv, c->d_plain);
@@ -355,6 +386,7 @@ void jfdk_destroy(jfdk_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
     dev_free(c->d_ptm); dev_free(c->d_tw); dev_free(c->d_tinv); dev_free(c->d_dmin); dev_free(c->d_pw);
+    dev_free(c->d_tinv_view); dev_free(c->d_cmask);
     dev_free(c->d_T); dev_free(c->d_Th); dev_free(c->d_Tl); dev_free(c->d_Tb); dev_free(c->d_Tf);
     dev_free(c->d_status); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_arow);
     dev_free(c->d_plain);
@@ -506,6 +538,21 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     JFDK_LAUNCH(c, launch_preweight_table(c->d_tinv, c->d_dmin, c->groups, c->rows, c->in_w, c->mirror, c->d_pw,
                                           c->stream),
                 "pre-weight table");
+    if (compositing(c)) {   // per-view inverse TMs and CompositeCore's 40-column masks
+        if ((st = dev_alloc(c, &c->d_tinv_view, (size_t)c->nviews * 16, "the inverse transforms"))) return bail(st);
+        if ((st = dev_alloc(c, &c->d_cmask, 80, "the compositing masks"))) return bail(st);
+        float mask[80];
+        const float pi = 3.14159265358979323846f;
+        for (int i = 0; i < 40; ++i) {   // CompositeCore.cpp:195-223
+            mask[i] = c->mirror ? std::cos((float)i / 40.0f * pi) * -0.5f + 0.5f
+                                : std::cos((float)i / 40.0f * pi) * 0.5f + 0.5f;
+            mask[40 + i] = 1.0f - mask[i];
+        }
+        JFDK_CUDA(c, cudaMemcpyAsync(c->d_tinv_view, c->ops.tinv_view.data(), sizeof(float) * c->nviews * 16,
+                                     cudaMemcpyHostToDevice, c->stream),
+                  "upload");
+        JFDK_CUDA(c, cudaMemcpyAsync(c->d_cmask, mask, sizeof mask, cudaMemcpyHostToDevice, c->stream), "upload");
+    }
     JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "context setup");
     *out = c;
     return JFDK_OK;
@@ -596,6 +643,18 @@ jfdk_status jfdk_filter_frames(jfdk_ctx* c, const float* d_in, int v0, int nv, f
     JFDK_LAUNCH(c, launch_weight(d_in, nv, v0, c->in_w, c->rows, weight_params(c), a_operand(c), c->d_e, c->stream),
                 "pre-weight");
     JFDK_LAUNCH(c, launch_ramp(c, ramp_params(c, nv, d_out)), "ramp filter");
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_composite_frames(jfdk_ctx* c, const float* d_dirc, const float* d_conj, int v0, int nv,
+                                  float* d_out) {
+    if (!c || !d_dirc || !d_conj || !d_out || nv < 0 || v0 < 0)
+        return fail(c, JFDK_ERR_INVALID, "composite: bad argument");
+    if (!compositing(c))
+        return fail(c, JFDK_ERR_STATE, "composite: the context's filter input width is not twice the frame width");
+    if (nv == 0) return JFDK_OK;
+    JFDK_LAUNCH(c, launch_composite_frames(d_dirc, d_conj, v0, nv, composite_params(c), d_out, c->stream),
+                "compositing");
     return JFDK_OK;
 }
 
@@ -919,7 +978,7 @@ extern "C" jfdk_status jfdk_autotune(jfdk_ctx* c, int flags) {
     c->opt_bp_zpt = best_z;
     // views per chunk: the filter stage over the first views of zero frames
     int best_c = c->opt_view_chunk;
-    if (c->in_w == c->used_u) {
+    if (c->in_w == c->used_u) {   // (compositing reads conjugate frames of the whole rotation)
         const int nsub = std::min(c->nviews, 128);
         uint16_t* raw = nullptr;
         const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;

@@ -18,6 +18,7 @@ namespace jfdk {
 struct HostOperators {
     std::vector<float> uw;      // [views][out_w]   BP u-taper (BPCore.cpp:68-100)
     std::vector<float> tinv;    // [groups][16]     inverse TM per 9-view group
+    std::vector<float> tinv_view;  // [views][16]   inverse TM per view, float solve (compositing)
     std::vector<float> T;       // [out_w][in_w]    ramp operator (Toeplitz)
     std::vector<float> c;       // [out_w]          edge-ramp response
     std::vector<float> H;       // [L/2+1]          filter spectrum
@@ -94,6 +95,18 @@ cudaError_t launch_finalize(const float* sum, const float* cnt, size_t n, int ap
                             cudaStream_t s);
 cudaError_t launch_ctnum(float* d, size_t n, float ct_scale, float norm1, cudaStream_t s);
 
+// Conjugate-view compositing (CompositeCore): the direct frame of view k in
+// one half of a 2W-wide row, the frame of view (k + N/2) % N resampled into the
+// other half, blended over 40 columns with the direct edge.
+struct CompositeParams {
+    const float* tinv;       // [views][16] inverse TM of each view
+    const float* ptm;        // [views][12]
+    const float* mask;       // [80]: the direct frame's transition mask, then the conjugate's
+    int num_views;           // views per rotation
+    int W, H;                // frame (half the composite row)
+    int det_right;           // the detector sits right of the principal point: direct half on the right
+};
+
 struct PrepParams {
     const uint16_t* raw;     // [nv][in_h][in_w]
     int in_w, in_h, crop_x, crop_y;
@@ -101,6 +114,8 @@ struct PrepParams {
     float bright_field;
     float bhc0, bhc1, bhc2;
     int do_bhc;
+    const uint16_t* raw_rotation;   // compositing: frame 0 of the rotation (conjugate frames), else null
+    long long raw_frame;            // compositing: elements per raw frame
 };
 struct WeightParams {
     const float* tinv;       // [groups][16]
@@ -110,6 +125,7 @@ struct WeightParams {
     int det_right;
     int mirror;
     const float* pw;         // [groups][rows][width] weights, or null: computed per row
+    CompositeParams comp;    // comp.W > 0: rows are composited from raw frames first (width = 2 comp.W)
 };
 cudaError_t launch_preprocess(const PrepParams& p, int nv, float* out, cudaStream_t s);
 
@@ -122,6 +138,10 @@ struct AOperand {
     float* row_scale;     // FP16X2: [M] 1 / the row's power-of-two scale
     int pitch;            // elements per row (K padded)
 };
+// Composite nv preprocessed direct / conjugate frame pairs of views
+// v0.. into out [nv][H][2W] (CompositeAgent path).
+cudaError_t launch_composite_frames(const float* dirc, const float* conj, int v0, int nv, const CompositeParams& c,
+                                    float* out, cudaStream_t s);
 // Pre-weight + edge mean of frames already preprocessed (agent path).
 cudaError_t launch_weight(const float* in, int nv, int v0, int width, int rows, const WeightParams& w,
                           const AOperand& A, float* e, cudaStream_t s);
@@ -220,6 +240,8 @@ struct jfdk_ctx {
     float* d_tinv = nullptr;
     float* d_dmin = nullptr;
     float* d_pw = nullptr;       // [groups][rows][in_w] pre-weights
+    float* d_tinv_view = nullptr;  // [views][16] (compositing)
+    float* d_cmask = nullptr;      // [80] compositing transition masks
     float* d_T = nullptr;
     float* d_Th = nullptr;       // TF32-exact split of the ramp operator
     float* d_Tl = nullptr;

@@ -133,6 +133,86 @@ __global__ void __launch_bounds__(256) preprocess_kernel(PrepParams P, float* __
     for (int i = threadIdx.x; i < P.width; i += blockDim.x) dst[i] = prep_pixel((float)src[i], P);
 }
 
+// ---- conjugate-view compositing (CompositeAgent/CompositeCore.cpp:59-149) ----
+// Value of column c in [0, 2W) of row r of view k's composite row, the float
+// operations in CompositeCore's order: the conjugate half resampled at the
+// points the direct view's extended detector would see (MatrixMultiplier
+// products of the view's inverse TM and the conjugate PTM, quotients, v
+// clamped, ippiRemap's inside-only rule and lerps), the 40 columns next to
+// the direct half blended with the direct row's 5-sample edge mean, the
+// direct half copied.  dirc(i) and conj(iy, ix) return preprocessed pixels.
+template <class D, class C>
+__device__ __forceinline__ float composite_value(const CompositeParams& cp, int k, int r, int c, float edge, D dirc,
+                                                 C conj) {
+    const int W = cp.W, tw = 40;
+    const int dircOff = cp.det_right ? W : 0, conjOff = cp.det_right ? 0 : W;
+    if (c >= dircOff && c < dircOff + W) return dirc(c - dircOff);
+    const int cc = c - conjOff;
+    const float* T = cp.tinv + (size_t)k * 16;
+    const float* P = cp.ptm + (size_t)((k + cp.num_views / 2) % cp.num_views) * 12;
+    const float uvw[4] = {cp.det_right ? __fsub_rn((float)cc, (float)W) : (float)(cc + W), (float)r, 0.0f, 1.0f};
+    float xyz[4], q[3];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) a = __fadd_rn(a, __fmul_rn(T[i * 4 + j], uvw[j]));
+        xyz[i] = a;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float a = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) a = __fadd_rn(a, __fmul_rn(P[i * 4 + j], xyz[j]));
+        q[i] = a;
+    }
+    const float u = __fdiv_rn(q[0], q[2]);
+    float v = __fdiv_rn(q[1], q[2]);
+    if (v < 0.0f) v = 0.0f;
+    if (v > (float)cp.H - 1.0f) v = (float)cp.H - 1.0f;
+    float o = 0.0f;
+    if (u >= 0.0f && u <= (float)(W - 1) && v >= 0.0f && v <= (float)(cp.H - 1)) {
+        const int ix = (int)floorf(u), iy = (int)floorf(v);
+        const int ix1 = ix + 1 < W ? ix + 1 : W - 1, iy1 = iy + 1 < cp.H ? iy + 1 : cp.H - 1;
+        const float fx = __fsub_rn(u, (float)ix), fy = __fsub_rn(v, (float)iy);
+        const float p00 = conj(iy, ix), p01 = conj(iy, ix1), p10 = conj(iy1, ix), p11 = conj(iy1, ix1);
+        const float t0 = __fadd_rn(p00, __fmul_rn(fx, __fsub_rn(p01, p00)));
+        const float t1 = __fadd_rn(p10, __fmul_rn(fx, __fsub_rn(p11, p10)));
+        o = __fadd_rn(t0, __fmul_rn(fy, __fsub_rn(t1, t0)));
+    }
+    const int transOff = cp.det_right ? W - tw : W;
+    if (c >= transOff && c < transOff + tw) {
+        const int i = c - transOff;
+        o = __fadd_rn(__fmul_rn(o, cp.mask[tw + i]), __fmul_rn(edge, cp.mask[i]));
+    }
+    return o;
+}
+
+// The direct row's edge mean: its first (detector right) or last 5 samples,
+// summed in double and divided in float (as the library's ippsMean stand-in).
+template <class D>
+__device__ __forceinline__ float composite_edge(const CompositeParams& cp, D dirc) {
+    double sum = 0.0;
+    const int b = cp.det_right ? 0 : cp.W - 5;
+    for (int i = 0; i < 5; ++i) sum += (double)dirc(b + i);
+    return __fdiv_rn((float)sum, 5.0f);
+}
+
+__global__ void __launch_bounds__(256) composite_frames_kernel(const float* __restrict__ dirc,
+                                                               const float* __restrict__ conj, int v0,
+                                                               CompositeParams cp, float* __restrict__ out) {
+    const int r = blockIdx.x, f = blockIdx.y, k = (v0 + f) % cp.num_views;
+    const float* drow = dirc + ((size_t)f * cp.H + r) * cp.W;
+    const float* cfr = conj + (size_t)f * cp.H * cp.W;
+    auto D = [&](int i) { return drow[i]; };
+    auto Cj = [&](int iy, int ix) { return cfr[(size_t)iy * cp.W + ix]; };
+    __shared__ float edge;
+    if (threadIdx.x == 0) edge = composite_edge(cp, D);
+    __syncthreads();
+    float* o = out + ((size_t)f * cp.H + r) * 2 * cp.W;
+    for (int c = threadIdx.x; c < 2 * cp.W; c += blockDim.x) o[c] = composite_value(cp, k, r, c, edge, D, Cj);
+}
+
 // ---- pre-weight + edge mean of a preprocessed row --------------------------
 // The weighted row goes out as the ramp product's A operand in the form the
 // product reads (AOut): fp32, or split into a high and a low part -- tf32
@@ -216,13 +296,31 @@ __global__ void __launch_bounds__(256) weight_kernel(PrepParams P, const float* 
     const uint16_t* src = FROM_RAW ? P.raw + ((size_t)vl * P.in_h + row + P.crop_y) * P.in_w + P.crop_x
                                    : nullptr;
     const float* fin = FROM_RAW ? nullptr : in + m * width;
-    auto pix = [&](int i) -> float { return FROM_RAW ? prep_pixel((float)src[i], P) : fin[i]; };
+    // compositing from raw frames: direct frame = this view's, conjugate =
+    // view (view + N/2) % N of the rotation, both preprocessed on the fly
+    const CompositeParams& cp = W.comp;
+    const bool comp = FROM_RAW && cp.W > 0;
+    const uint16_t* craw = comp ? P.raw_rotation + (size_t)((view + cp.num_views / 2) % cp.num_views) * P.raw_frame +
+                                      (size_t)P.crop_y * P.in_w + P.crop_x
+                                : nullptr;
+    auto dpix = [&](int i) -> float { return prep_pixel((float)src[i], P); };
+    auto cpix = [&](int iy, int ix) -> float { return prep_pixel((float)craw[(size_t)iy * P.in_w + ix], P); };
+    __shared__ float s_edge;
+    if (comp) {
+        if (threadIdx.x == 0) s_edge = composite_edge(cp, dpix);
+        __syncthreads();
+    }
+    auto pix = [&](int i) -> float {
+        if (!FROM_RAW) return fin[i];
+        if (comp) return composite_value(cp, view, row, i, s_edge, dpix, cpix);
+        return prep_pixel((float)src[i], P);
+    };
     const float* pwrow = W.pw ? W.pw + ((size_t)g * rows + row) * width : nullptr;
     auto value = [&](int i, float p) -> float {
         return __fmul_rn(p, pwrow ? __ldg(pwrow + i) : __fdiv_rn(dmin, pw_dist(r, u_axis(i, width, W.det_right))));
     };
     const int elem = OUT == AOUT_F32 || OUT == AOUT_TF32X2 ? 4 : 2;
-    const bool vec = FROM_RAW && ((reinterpret_cast<uintptr_t>(P.raw) & 7) == 0) &&
+    const bool vec = FROM_RAW && !comp && ((reinterpret_cast<uintptr_t>(P.raw) & 7) == 0) &&
                      ((reinterpret_cast<uintptr_t>(A.hi) & 15) == 0) &&
                      (OUT == AOUT_F32 || (reinterpret_cast<uintptr_t>(A.lo) & 15) == 0) &&
                      ((P.crop_x & 3) == 0) && ((P.in_w & 3) == 0) && ((width & 3) == 0) &&
@@ -295,6 +393,12 @@ cudaError_t launch_preweight_table(const float* tinv, const float* dmin, int gro
 
 cudaError_t launch_preprocess(const PrepParams& p, int nv, float* out, cudaStream_t s) {
     preprocess_kernel<<<dim3(p.rows, nv), 256, 0, s>>>(p, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_composite_frames(const float* dirc, const float* conj, int v0, int nv, const CompositeParams& c,
+                                    float* out, cudaStream_t s) {
+    composite_frames_kernel<<<dim3(c.H, nv), 256, 0, s>>>(dirc, conj, v0, c, out);
     return cudaGetLastError();
 }
 

@@ -210,6 +210,15 @@ class FDKEngine:
         self._check(self.lib.jfdk_filter_frames_noalloc(self.ctx, _ptr(frames), v0, nv, _ptr(out)))
         return out
 
+    def composite(self, dirc, conj, v0: int = 0, out=None):
+        """CompositeCore on pairs of preprocessed frames (views v0.. and their
+        conjugates): (nv, rows, 2 width)."""
+        import torch
+        nv, H, W = dirc.shape
+        out = out if out is not None else torch.empty((nv, H, 2 * W), dtype=torch.float32, device=dirc.device)
+        self._check(self.lib.jfdk_composite_frames(self.ctx, _ptr(dirc), _ptr(conj), v0, nv, _ptr(out)))
+        return out
+
     def zfilter(self, frames):
         self._check(self.lib.jfdk_zfilter_frames(self.ctx, _ptr(frames), frames.shape[0]))
         return frames

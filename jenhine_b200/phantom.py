@@ -33,6 +33,7 @@ class ScanGeometry:
     flex_shift_px: float = 0.0   # seeded per-view detector shift, +/- px
     flex_tilt_deg: float = 0.0   # seeded per-view in-plane detector tilt, +/- deg
     seed: int = 0
+    offset_u_px: float = 0.0     # detector offset: the principal point moves by this many columns
 
     @property
     def half_sample_rate(self) -> float:
@@ -56,7 +57,7 @@ class ScanGeometry:
             ct, st = math.cos(tilt[k]), math.sin(tilt[k])
             eu = ct * eu0 + st * ev0
             ev = -st * eu0 + ct * ev0
-            cu = self.det_u / 2.0 - 1.0 + shift[k, 0]
+            cu = self.det_u / 2.0 - 1.0 + shift[k, 0] + self.offset_u_px
             cv = self.det_v / 2.0 - 1.0 + shift[k, 1]
             out.append((src, n_hat, eu, ev, cu, cv))
         return out

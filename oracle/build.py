@@ -43,6 +43,7 @@ REF_SOURCES = [
     "FilterAgent/FilterCore.cpp",
     "FilterAgent/PreFilterWeightGenerator.cpp",
     "BPAgent/BPCore.cpp",
+    "CompositeAgent/CompositeCore.cpp",
     "CTNumAgent/CTNumCore.cpp",
     "TransformMatrix/MatrixConvertor.cpp",
     "TransformMatrix/ProjectionMatrixModifier.cpp",

@@ -523,6 +523,78 @@ void jo_filter_rows_f64(double* out, const float* in, const float* preweight,
 }
 
 /* ======================================================================
+ * Conjugate-view compositing -- CompositeAgent/CompositeCore.cpp
+ * ==================================================================== */
+
+/* CompositeCore::Process (CompositeCore.cpp:59-149) for one view: out is
+ * [H][2W], the direct frame in one half and, in the other, the conjugate
+ * frame resampled at the points the direct view's extended detector would
+ * see, blended with the direct frame's edge over 40 columns. */
+void jo_composite(float* out, const float* dirc, const float* conj, const float ptm_dirc[12],
+                  const float ptm_conj[12], float dso, int W, int H, int detRight) {
+    const int tw = 40, ew = 5;                       /* transWidth, edgeWidth :36-37 */
+    const int W2 = 2 * W;
+    for (size_t i = 0; i < (size_t)W2 * H; ++i) out[i] = 0.0f;
+    /* TM of the direct view and its inverse (LinearEquationSolver, A X = I) */
+    float tm[16], A[16], tinv[16];
+    jo_ptm2tm(tm, ptm_dirc, dso);
+    for (int i = 0; i < 16; ++i) { A[i] = tm[i]; tinv[i] = (i % 5 == 0) ? 1.0f : 0.0f; }
+    jo_solve_f32(4, 4, A, tinv);
+    const int conjOff = detRight ? 0 : W, dircOff = detRight ? W : 0;
+    for (int r = 0; r < H; ++r) {
+        for (int c = 0; c < W; ++c) {
+            /* GenerateUVW1Grid :153-183: (u, v, 0, 1) beyond the direct edge */
+            const float uvw[4] = {detRight ? (float)c - (float)W : (float)(c + W), (float)r, 0.0f, 1.0f};
+            float xyz[4], q[3];
+            for (int i = 0; i < 4; ++i) {               /* MatrixMultiplier 4x4 . 4x1 */
+                float acc = 0.0f;
+                for (int k = 0; k < 4; ++k) acc += tinv[i * 4 + k] * uvw[k];
+                xyz[i] = acc;
+            }
+            for (int i = 0; i < 3; ++i) {               /* 3x4 . 4x1, the conjugate PTM */
+                float acc = 0.0f;
+                for (int k = 0; k < 4; ++k) acc += ptm_conj[i * 4 + k] * xyz[k];
+                q[i] = acc;
+            }
+            const float u = q[0] / q[2];
+            float v = q[1] / q[2];
+            if (v < 0.0f) v = 0.0f;                     /* LowerBound, UpperBound :84-85 */
+            if (v > (float)H - 1.0f) v = (float)H - 1.0f;
+            /* ImgEditor::Remap, restated: written only inside the frame */
+            if (!(u >= 0.0f && u <= (float)(W - 1) && v >= 0.0f && v <= (float)(H - 1))) continue;
+            const int ix = (int)floorf(u), iy = (int)floorf(v);
+            const int ix1 = ix + 1 < W ? ix + 1 : W - 1, iy1 = iy + 1 < H ? iy + 1 : H - 1;
+            const float fx = u - (float)ix, fy = v - (float)iy;
+            const float p00 = conj[(size_t)iy * W + ix], p01 = conj[(size_t)iy * W + ix1];
+            const float p10 = conj[(size_t)iy1 * W + ix], p11 = conj[(size_t)iy1 * W + ix1];
+            const float t0 = p00 + fx * (p01 - p00), t1 = p10 + fx * (p11 - p10);
+            out[(size_t)r * W2 + conjOff + c] = t0 + fy * (t1 - t0);
+        }
+    }
+    /* transition masks :195-223: direct 1 -> 0 (or 0 -> 1), conjugate 1 - that */
+    float md[40], mc[40];
+    for (int i = 0; i < tw; ++i) {
+        md[i] = detRight ? cosf((float)i / (float)tw * JO_PI_F) * -0.5f + 0.5f
+                         : cosf((float)i / (float)tw * JO_PI_F) * 0.5f + 0.5f;
+        mc[i] = 1.0f - md[i];
+    }
+    const int transOff = detRight ? W - tw : W, tempOff = detRight ? W : 0;
+    for (int r = 0; r < H; ++r) {
+        float* o = out + (size_t)r * W2;
+        for (int i = 0; i < tw; ++i) o[transOff + i] = o[transOff + i] * mc[i];
+        /* the direct row's edge mean (ippsMean over 5 samples: summed in
+         * double, divided in float) into the temporary region :103-124 */
+        const float* d = dirc + (size_t)r * W + (detRight ? 0 : W - ew);
+        double sum = 0.0;
+        for (int i = 0; i < ew; ++i) sum += d[i];
+        const float edge = (float)sum / (float)ew;
+        for (int i = 0; i < tw; ++i) o[tempOff + i] = edge * md[i];
+        for (int i = 0; i < tw; ++i) o[transOff + i] = o[transOff + i] + o[tempOff + i];
+        for (int i = 0; i < W; ++i) o[dircOff + i] = dirc[(size_t)r * W + i];
+    }
+}
+
+/* ======================================================================
  * Backprojection -- BPAgent/BPCore.cpp
  * ==================================================================== */
 

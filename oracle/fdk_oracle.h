@@ -80,6 +80,12 @@ void jo_filter_rows_f64(double* out, const float* in, const float* preweight,
 /* Equivalent real, even space kernel h_eff[L] = IDFT_L(H) (double). */
 void jo_filter_kernel_f64(double* h, const float* H, int L);
 
+/* ---- conjugate-view compositing (CompositeAgent/CompositeCore) -------- */
+/* One view: dirc, conj [H][W] preprocessed frames of views k and
+ * (k + N/2) % N, out [H][2W]. */
+void jo_composite(float* out, const float* dirc, const float* conj, const float ptm_dirc[12],
+                  const float ptm_conj[12], float dso, int W, int H, int detRight);
+
 /* ---- backprojection (BPAgent/BPCore) ---------------------------------- */
 /* u-taper per view: w[nViews][U]. */
 void jo_bp_uweights(float* w, const float* ptms, int nViews, int U);

@@ -51,6 +51,7 @@ class Oracle:
             "jo_filter_spectrum": [_P, I, F, F, F, _P, _P, I],
             "jo_filter_rows": [_P, _P, _P, I, I, I, I, _P, I],
             "jo_filter_rows_f64": [_P, _P, _P, I, I, I, I, _P, I],
+            "jo_composite": [_P, _P, _P, _P, _P, F, I, I, I],
             "jo_bp_points_f64": [_P, _P, _P, _P, _P, I, I, I, I, _P, I, I, I, I, F, F, I],
             "jo_bp_points_f64d": [_P, _P, _P, _P, _P, I, I, I, I, _P, I, I, I, I, F, F, I],
             "jo_filter_kernel_f64": [_P, _P, I], "jo_bp_uweights": [_P, _P, I, I],
@@ -157,6 +158,21 @@ class Oracle:
                                 w_out, int(mirror), _ptr(_c(H, _f32)), L)
         return out.reshape(rows.shape[:-1] + (w_out,))
 
+    def composite(self, pre, ptms, dso, det_right, v0=0, nv=None):
+        """The restated CompositeCore over views [v0, v0 + nv) of the
+        rotation pre [N][H][W]: [nv][H][2W]."""
+        pre = _c(pre, _f32)
+        N, H, W = pre.shape
+        ptms = _c(ptms, _f32).reshape(-1, 12)
+        nv = N - v0 if nv is None else nv
+        out = np.empty((nv, H, 2 * W), _f32)
+        for i in range(nv):
+            k = (v0 + i) % N
+            kc = (k + N // 2) % N
+            self.lib.jo_composite(_ptr(out[i]), _ptr(pre[k]), _ptr(pre[kc]), _ptr(ptms[k]), _ptr(ptms[kc]), dso, W,
+                                  H, int(det_right))
+        return out
+
     def filter_rows_f64(self, rows, H, L, w_out=None, mirror=False, preweight=None):
         rows = _c(rows, _f32)
         R, W = rows.reshape(-1, rows.shape[-1]).shape
@@ -185,19 +201,21 @@ class Oracle:
             out[v] = self.filter_rows_f64(proj[v, r0:r1], H, L, W, mirror, cache[s])
         return out
 
-    def filter_projections(self, proj, ptms, H, dso, mirror=False):
-        """FilterAgent over views 0..N-1: the 9-view pre-weight grouping."""
+    def filter_projections(self, proj, ptms, H, dso, mirror=False, w_out=None):
+        """FilterAgent over views 0..N-1: the 9-view pre-weight grouping;
+        rows of width W in, w_out (default W) out."""
         proj = _c(proj, _f32)
         V, Hh, W = proj.shape
+        w_out = W if w_out is None else w_out
         L = self.fft_length(W)
-        out = np.empty_like(proj)
+        out = np.empty((V, Hh, w_out), _f32)
         cache = {}
         for v in range(V):
             s = self.preweight_source_view(v, V)
             if s not in cache:
                 cache.clear()
                 cache[s] = self.preweight_for_view(ptms[s], dso, W, Hh, mirror)
-            out[v] = self.filter_rows(proj[v], H, L, W, mirror, cache[s])
+            out[v] = self.filter_rows(proj[v], H, L, w_out, mirror, cache[s])
         return out
 
     # -- backprojection -----------------------------------------------------
@@ -323,6 +341,7 @@ class RefCores:
             "jref_filter_rows_noweight": [_P, _P, I, I, I, I, F, F, F, _P, _P, I],
             "jref_bp": [_P, _P, _P, I, I, I, I, I, I, F, F, I],
             "jref_ctnum": [_P, I, I, I, F, F, F], "jref_fft_length": [I],
+            "jref_composite": [_P, _P, I, I, _P, I, I, I, I, F, I],
         }
         for name, args in sig.items():
             fn = getattr(self.lib, name)
@@ -371,6 +390,17 @@ class RefCores:
         self.lib.jref_filter(_ptr(out), _ptr(proj), V, W, H, w_out, int(mirror), hsr, cut_start,
                              cut_end, _ptr(ap), _ptr(ad), ap.size, _ptr(ptms), ptms.shape[0], dso,
                              nthreads)
+        return out
+
+    def composite(self, pre, ptms, dso, det_right, v0=0, nv=None, nthreads=1):
+        """CompositeCore over views [v0, v0 + nv) of the rotation pre
+        [N][H][W]: [nv][H][2W]."""
+        pre = _c(pre, _f32)
+        N, H, W = pre.shape
+        nv = N - v0 if nv is None else nv
+        out = np.empty((nv, H, 2 * W), _f32)
+        self.lib.jref_composite(_ptr(out), _ptr(pre), v0, nv, _ptr(_c(ptms, _f32)), N, W, H, int(det_right),
+                                dso, nthreads)
         return out
 
     def filter_rows_noweight(self, rows, hsr, cut_start=0.0, cut_end=0.0, adj_pts=(), adj_db=(),

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "BPAgent/BPCore.h"
+#include "CompositeAgent/CompositeCore.h"
 #include "CTNumAgent/CTNumCore.h"
 #include "FilterAgent/FilterCore.h"
 #include "FilterAgent/PreFilterWeightGenerator.h"
@@ -160,6 +161,26 @@ int jref_bp(float* out, const float* proj, const float* ptms, int nViews,
 int jref_ctnum(float* inout, int width, int height, int nSlices, float norm0, float norm1, float muWater) {
     CTNumCore core(width, height, norm0, norm1, muWater);
     for (int s = 0; s < nSlices; ++s) core.Process(inout + (size_t)s * width * height);
+    return 0;
+}
+
+// CompositeAgent + CompositeCore over views [v0, v0 + nv): pre holds the
+// preprocessed frames of the whole rotation [N][H][W]; out [nv][H][2W].  View
+// k is composited with view (k + N/2) % N, as InputAgent pairs them
+// (JEngine/InputAgent.cpp:45-90, CompositeAgent.cpp:72-83).
+int jref_composite(float* out, const float* pre, int v0, int nv, const float* ptms, int N, int W, int H,
+                   int detRight, float dso, int nthreads) {
+    std::vector<std::unique_ptr<CompositeCore>> cores;
+    nthreads = std::max(1, std::min(nthreads, nv));
+    const std::vector<ProjectionMatrix> pm = to_ptms(ptms, N);   // the cores keep a reference to it
+    for (int t = 0; t < nthreads; ++t) cores.emplace_back(new CompositeCore(W, H, detRight != 0, dso, pm));
+    const size_t px = (size_t)W * H;
+    parallel_for(nv, nthreads, [&](int t, int i) {
+        const int k = (v0 + i) % N, kc = (k + N / 2) % N;
+        FloatVec o(px * 2), d(pre + px * k, pre + px * (k + 1)), c(pre + px * kc, pre + px * (kc + 1));
+        cores[t]->Process(o, d, c, (size_t)k);
+        std::memcpy(out + px * 2 * i, o.data(), sizeof(float) * px * 2);
+    });
     return 0;
 }
 

@@ -35,6 +35,13 @@ CASES = {
                     vol=(32, 32, 24, 2.5, 2.5), phantom=dict(n=20, n_metal=3), i0=5e4,
                     bf=50000.0, bhc=(1.0, 0.05, 0.01), norm=(1.2, 0.9),
                     filt=dict(cut_start=0.0, cut_end=0.0, adj_pts=(0.05, 0.1), adj_db=(1.0, -1.0))),
+    # offset detector (principal point 10 columns from its left edge) read
+    # with conjugate-view compositing, as the reference application does
+    # (CompositeAgent before a 2W-wide, mirrored FilterAgent)
+    "mini_comp": dict(geom=dict(n_views=40, sid=500.0, sdd=800.0, det_u=48, det_v=36, pixel_u=2.6,
+                                pixel_v=2.6, offset_u_px=-13.0, seed=44),
+                      vol=(32, 32, 20, 2.5, 2.5), phantom=dict(n=10), i0=1e5, bf=50000.0,
+                      bhc=(1.0, 0.0, 0.0), norm=(1.0, 1.0), composite=dict(det_right=True)),
 }
 
 
@@ -48,8 +55,17 @@ def make(name: str, c: dict, ref: RefCores) -> str:
     hsr = g.half_sample_rate
     f = c.get("filt", {})
     prep = ref.preprocess(raw, c["bf"], c["bhc"])
-    filt = ref.filter(prep, ptms, hsr, float(dso), f.get("cut_start", 0.0), f.get("cut_end", 0.0),
-                      f.get("adj_pts", ()), f.get("adj_db", ()), nthreads=4)
+    comp = c.get("composite")
+    extra = {}
+    if comp:   # CompositeCore, then the 2W-wide FilterCore (mirrored when the detector is on the right)
+        cmp_ = ref.composite(prep, ptms, float(dso), comp["det_right"], nthreads=4)
+        filt = ref.filter(cmp_, ptms, hsr, float(dso), f.get("cut_start", 0.0), f.get("cut_end", 0.0),
+                          f.get("adj_pts", ()), f.get("adj_db", ()), mirror=comp["det_right"], w_out=g.det_u,
+                          nthreads=4)
+        extra = dict(comp=cmp_, det_right=np.int32(comp["det_right"]))
+    else:
+        filt = ref.filter(prep, ptms, hsr, float(dso), f.get("cut_start", 0.0), f.get("cut_end", 0.0),
+                          f.get("adj_pts", ()), f.get("adj_db", ()), nthreads=4)
     bp = ref.bp(filt, ptms, X, Y, Z, pxy, pz, nthreads=4)
     hu = ref.ctnum(bp, *c["norm"])
     pw0 = ref.preweight(ptms, g.det_u, g.det_v, float(dso), 4)
@@ -61,15 +77,17 @@ def make(name: str, c: dict, ref: RefCores) -> str:
         cut=np.asarray([f.get("cut_start", 0.0), f.get("cut_end", 0.0)], np.float32),
         adj_pts=np.asarray(f.get("adj_pts", ()), np.float32),
         adj_db=np.asarray(f.get("adj_db", ()), np.float32),
-        prep=prep, preweight_v4=pw0, filt=filt, bp=bp, hu=hu)
+        prep=prep, preweight_v4=pw0, filt=filt, bp=bp, hu=hu, **extra)
     return path
 
 
-def main() -> None:
+def main(names=None) -> None:
     ref = RefCores()
     for name, c in CASES.items():
+        if names and name not in names:
+            continue
         print(make(name, c, ref))
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -32,6 +32,9 @@ def engine_for(g, **kw):
                       num_dets_v=raw.shape[1], detector_pixel_size=0.0,
                       bright_field=float(g["bright_field"]), beam_hardening=tuple(g["bhc"]),
                       half_sample_rate=float(g["hsr"]))
+    if "det_right" in g:   # conjugate-view compositing: the filter reads 2W-wide rows
+        scan.filter_input_width = 2 * raw.shape[2]
+        scan.detector_on_right = bool(g["det_right"])
     recon = ReconConfig(X, Y, Z, pxy, pz, ct_norm0=float(g["norm"][0]), ct_norm1=float(g["norm"][1]),
                         filter_cutoff_start=float(g["cut"][0]), filter_cutoff_end=float(g["cut"][1]),
                         adjust_points=tuple(g["adj_pts"]), adjust_level_db=tuple(g["adj_db"]))

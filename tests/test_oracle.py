@@ -222,3 +222,15 @@ def test_fp64_fdk_pinned_to_reference_outputs(oracle, golden):
     inside = interior(g, pts).reshape(Z, Y, X)
     assert inside.any()
     assert np.max(np.abs(hu - ref)[both & inside]) < 0.05
+
+
+def test_composite_restatement_matches_reference_core(oracle):
+    """CompositeCore (compiled reference) output stored in the fixture, and the
+    restatement: bit for bit; the 2W-wide mirrored FilterCore on it."""
+    g = load_golden("mini_comp")
+    comp = oracle.composite(g["prep"], g["ptms"], float(g["dso"]), bool(g["det_right"]))
+    np.testing.assert_array_equal(comp, g["comp"])
+    W = g["prep"].shape[2]
+    H = oracle.filter_spectrum(oracle.fft_length(2 * W), float(g["hsr"]))
+    f = oracle.filter_projections(g["comp"], g["ptms"], H, float(g["dso"]), mirror=True, w_out=W)
+    assert rel_l2(f, g["filt"]) < 1e-6
