@@ -3,6 +3,7 @@
 // Constructor signatures and pipe wiring follow the reference agents so they
 // drop into the same agent list (JEngine/JEngine.cpp:186-314):
 //   PreProcessingAgent  PreProcessingAgent/PreProcessingAgent.h:17-30   "Proj" UINT16Vec -> FloatVec
+//   CompositeAgent      CompositeAgent/CompositeAgent.h:15-55           "Proj" FloatVec pairs -> FloatVec (2W)
 //   FilterAgent         FilterAgent/FilterAgent.h:19-33                 "Proj" FloatVec  -> FloatVec
 //   ZFilterAgent        FilterAgent/ZFilterAgent.h                      "Proj" FloatVec  -> FloatVec
 //   DeviceUploadAgent   (Tex2DUploadAgent, CUDA/Tex2DUploadAgent.h)     "Proj" FloatVec  -> DeviceMemory<float>
@@ -52,6 +53,29 @@ private:
     std::vector<std::unique_ptr<StageContext>> stages;
     std::shared_ptr<Pipe<UINT16Vec>> pipeIn;
     std::shared_ptr<Pipe<FloatVec>> pipeOut;
+};
+
+// Reads (direct, conjugate) frame pairs -- the order InputAgent writes them,
+// JEngine/InputAgent.cpp:45-90 -- and writes one 2W-wide composite frame per
+// pair (jfdk_composite_frames).
+class CompositeAgent : public ConcurrentAgentBase {
+public:
+    CompositeAgent(size_t numThreads, size_t inputWidth, size_t inputHeight, bool detectorAtTheRight,
+                   float sourceOriginDistance, const std::vector<ProjectionMatrix>& projectionMatrices);
+    ~CompositeAgent() override;
+
+private:
+    struct Task : TaskBase {
+        Pipe<FloatVec>::ReadToken ReadToken;
+        Pipe<FloatVec>::WriteToken WriteToken;
+    };
+    void SetPipesImpl() override;
+    void ManagerWorkFlow() override;
+    void ProcessTask(size_t threadIndex, std::unique_ptr<TaskBase> task) override;
+
+    const size_t width, height, numViewsPerRot;
+    std::vector<std::unique_ptr<StageContext>> stages;
+    std::shared_ptr<Pipe<FloatVec>> pipeIn, pipeOut;
 };
 
 class FilterAgent : public ConcurrentAgentBase {

@@ -186,6 +186,61 @@ void PreProcessingAgent::ProcessTask(size_t ti, std::unique_ptr<TaskBase> base) 
     st.Sync();
 }
 
+// ---- CompositeAgent (CompositeAgent/CompositeAgent.cpp:9-83) --------------------
+
+CompositeAgent::CompositeAgent(size_t numThreads, size_t inputWidth, size_t inputHeight, bool detectorAtTheRight,
+                               float sourceOriginDistance, const std::vector<ProjectionMatrix>& projectionMatrices)
+    : ConcurrentAgentBase("CompositeAgent", numThreads), width(inputWidth), height(inputHeight),
+      numViewsPerRot(projectionMatrices.size()) {
+    jfdk_scan_params s = scan_defaults(projectionMatrices.size(), inputWidth, inputHeight);
+    s.dso = sourceOriginDistance;
+    s.detector_on_right = detectorAtTheRight ? 1 : 0;
+    s.filter_input_width = (int)(2 * inputWidth);   // a compositing context
+    const std::vector<float> p = flatten(projectionMatrices);
+    for (size_t t = 0; t < numThreads; ++t) stages.emplace_back(new StageContext(s, recon_defaults(1, 1, 1), p));
+}
+CompositeAgent::~CompositeAgent() = default;
+
+void CompositeAgent::SetPipesImpl() {
+    pipeIn = BranchPipeFromTrunk<FloatVec>("Proj");
+    pipeIn->SetConsumer(GetAgentName(), GetNumThreads(), 2, 0);
+    pipeOut = CreateNewPipe<FloatVec>("Proj");
+    pipeOut->SetProducer(GetAgentName(), GetNumThreads(), 1);
+    pipeOut->SetTemplate(FloatVec(width * height * 2, 0.0f), {width * 2, height});
+    MergePipeToTrunk(pipeOut);
+}
+
+void CompositeAgent::ManagerWorkFlow() {
+    try {
+        while (true) {
+            WaitIdleWorkerIndex();
+            Task task;
+            task.ReadToken = pipeIn->GetReadToken();
+            task.WriteToken = pipeOut->GetWriteToken(1, task.ReadToken.IsShotEnd());
+            SubmitTask(std::make_unique<Task>(task));
+        }
+    } catch (PipeClosedAndEmptySignal&) {
+        pipeOut->Close();
+    }
+}
+
+void CompositeAgent::ProcessTask(size_t ti, std::unique_ptr<TaskBase> base) {
+    Task* task = static_cast<Task*>(base.get());
+    ThreadOccupiedScope occupied(this);
+    StageContext& st = *stages[ti];
+    // token i holds frames 2i (view i) and 2i + 1 (its conjugate)
+    const int view = (int)((task->ReadToken.GetStartIndex() / 2) % numViewsPerRot);
+    const size_t px = width * height;
+    auto* d_in = static_cast<float*>(st.Buffer(0, px * 2 * 4));
+    auto* d_out = static_cast<float*>(st.Buffer(1, px * 2 * 4));
+    st.Upload(d_in, task->ReadToken.GetBuffer(0).data(), px * 4);
+    st.Upload(d_in + px, task->ReadToken.GetBuffer(1).data(), px * 4);
+    st.Check(jfdk_composite_frames(st.ctx, d_in, d_in + px, view, 1, d_out));
+    st.Download(task->WriteToken.GetBuffer(0).data(), d_out, px * 2 * 4);
+    WaitAsyncScope wait(&occupied);
+    st.Sync();
+}
+
 // ---- FilterAgent (FilterAgent/FilterAgent.cpp:10-192) --------------------------
 
 FilterAgent::FilterAgent(size_t nThreads, size_t /*nRowsPerThread*/, size_t nInputWidth, size_t nInputHeight,

@@ -1,10 +1,11 @@
 // test_agents_gpu.cpp -- the reference's GPU agent chain on libjfdk.so:
-// Source -> PreProcessingAgent -> FilterAgent -> DeviceUploadAgent ->
-// BPCUDAAgent -> DeviceMemoryDownloadAgent -> CTNumAgent -> Sink
-// (the order of JEngine/JEngine.cpp:186-314 without compositing).
+// Source -> PreProcessingAgent -> [CompositeAgent] -> FilterAgent ->
+// DeviceUploadAgent -> BPCUDAAgent -> DeviceMemoryDownloadAgent -> CTNumAgent
+// -> Sink (the order of JEngine/JEngine.cpp:186-314).
 //
 // usage: test_agents_gpu <case.bin> <out.bin>
-//   case.bin: int32 header [views, detU, detV, X, Y, Z], float32 [dso, hsr,
+//   case.bin: int32 header [views, detU, detV, X, Y, Z, comp] (comp: -1 no
+//   compositing, else 1 when the detector is on the right), float32 [dso, hsr,
 //   bright, bhc0, bhc1, bhc2, pitchXY, pitchZ, norm0, norm1, cutStart,
 //   cutEnd, nAdj], nAdj adjust points, nAdj levels, views*12 PTM floats,
 //   views*detV*detU uint16 frames.  out.bin: Z*Y*X float32 HU.
@@ -18,8 +19,10 @@ using namespace JEngine;
 
 class FrameSource : public SequentialAgentBase {
 public:
-    FrameSource(const std::vector<UINT16Vec>& frames, size_t w, size_t h, int shots)
-        : SequentialAgentBase("InputAgent", 1), frames(frames), w(w), h(h), shots(shots) {}
+    // pairs: write view k and then view (k + N/2) % N, as InputAgent does for
+    // compositing (JEngine/InputAgent.cpp:45-90)
+    FrameSource(const std::vector<UINT16Vec>& frames, size_t w, size_t h, int shots, bool pairs)
+        : SequentialAgentBase("InputAgent", 1), frames(frames), w(w), h(h), shots(shots), pairs(pairs) {}
 
 private:
     void SetPipesImpl() override {
@@ -29,14 +32,22 @@ private:
         MergePipeToTrunk(out);
     }
     void WorkFlow0() override {
+        const size_t n = frames.size();
         for (int s = 0; s < shots; ++s)
-            for (size_t i = 0; i < frames.size(); ++i)
-                out->GetWriteToken(1, i + 1 == frames.size()).GetBuffer(0) = frames[i];
+            for (size_t i = 0; i < n; ++i) {
+                if (!pairs) {
+                    out->GetWriteToken(1, i + 1 == n).GetBuffer(0) = frames[i];
+                } else {
+                    out->GetWriteToken(1, false).GetBuffer(0) = frames[i];
+                    out->GetWriteToken(1, i + 1 == n).GetBuffer(0) = frames[(i + n / 2) % n];
+                }
+            }
         out->Close();
     }
     const std::vector<UINT16Vec>& frames;
     size_t w, h;
     int shots;
+    bool pairs;
     std::shared_ptr<Pipe<UINT16Vec>> out;
 };
 
@@ -63,11 +74,12 @@ private:
 int main(int argc, char** argv) {
     if (argc < 3) return 2;
     std::ifstream f(argv[1], std::ios::binary);
-    int hdr[6];
+    int hdr[7];
     float prm[13];
     f.read((char*)hdr, sizeof hdr);
     f.read((char*)prm, sizeof prm);
     const size_t V = hdr[0], U = hdr[1], H = hdr[2], X = hdr[3], Y = hdr[4], Z = hdr[5];
+    const bool comp = hdr[6] >= 0, detRight = hdr[6] == 1;
     const int nAdj = (int)prm[12];
     FloatVec adjP(nAdj), adjL(nAdj);
     f.read((char*)adjP.data(), 4 * nAdj);
@@ -80,11 +92,12 @@ int main(int argc, char** argv) {
 
     const int shots = 2;  // two scans back to back: the second must not see the first
     std::vector<std::shared_ptr<AgentBase>> agents;
-    agents.push_back(std::make_shared<FrameSource>(frames, U, H, shots));
+    agents.push_back(std::make_shared<FrameSource>(frames, U, H, shots, comp));
     agents.push_back(std::make_shared<PreProcessingAgent>(2, 1, U, H, 0, 0, 0, 0, U, H, prm[2],
                                                           FloatVec{prm[3], prm[4], prm[5]}));
-    agents.push_back(std::make_shared<FilterAgent>(2, 240, U, H, U, false, prm[1], prm[10], prm[11], adjP, adjL,
-                                                   ptms, prm[0]));
+    if (comp) agents.push_back(std::make_shared<CompositeAgent>(2, U, H, detRight, prm[0], ptms));
+    agents.push_back(std::make_shared<FilterAgent>(2, 240, comp ? 2 * U : U, H, U, detRight, prm[1], prm[10], prm[11],
+                                                   adjP, adjL, ptms, prm[0]));
     agents.push_back(std::make_shared<DeviceUploadAgent>("Proj", U, H));
     agents.push_back(std::make_shared<BPCUDAAgent>(ptms, U, H, X, Y, Z, prm[6], prm[7], Z, 1, "", 7));
     agents.push_back(std::make_shared<DeviceMemoryDownloadAgent>("Slice", X, Y));

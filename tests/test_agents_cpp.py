@@ -35,7 +35,8 @@ def _write_case(path, g):
     raw = g["raw"]
     V, H, U = raw.shape
     X, Y, Z = (int(v) for v in g["vol"])
-    hdr = np.array([V, U, H, X, Y, Z], np.int32)
+    comp = int(g["det_right"]) if "det_right" in g else -1
+    hdr = np.array([V, U, H, X, Y, Z, comp], np.int32)
     adj_p, adj_l = g["adj_pts"].astype(np.float32), g["adj_db"].astype(np.float32)
     prm = np.array([g["dso"], g["hsr"], g["bright_field"], *g["bhc"], *g["pitch"], *g["norm"], *g["cut"],
                     adj_p.size], np.float32)
@@ -45,7 +46,7 @@ def _write_case(path, g):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["mini_c1", "mini_c2"])
+@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_comp"])
 def test_agent_chain_gpu(tmp_path, name):
     import torch
     if not torch.cuda.is_available():
