@@ -32,6 +32,7 @@ struct jfdk_ctx;
 namespace JEngine {
 
 class StageContext;  // a jfdk context + its stream (Agents.cpp)
+class PinnedSlots;   // page-locked slots of a host pipe (Agents.cpp)
 
 class PreProcessingAgent : public ConcurrentAgentBase {
 public:
@@ -119,15 +120,23 @@ private:
     std::shared_ptr<Pipe<FloatVec>> pipeIn, pipeOut;
 };
 
+// Host frames -> device frames.  The slots of the host pipe are page-locked
+// in GetReady, so each frame goes to the device as one asynchronous DMA on the
+// agent's own stream, straight from the pipe slot (no driver staging copy).
 class DeviceUploadAgent : public SequentialAgentBase {
 public:
     DeviceUploadAgent(const std::string& pipeName, size_t width, size_t height);
+    ~DeviceUploadAgent() override;
+    void GetReady() override;
+    size_t NumPinnedSlots() const;
 
 private:
     void SetPipesImpl() override;
     void WorkFlow0() override;
     const std::string pipeName;
     const size_t width, height;
+    std::unique_ptr<PinnedSlots> pinned;
+    void* stream = nullptr;  // cudaStream_t
     std::shared_ptr<Pipe<FloatVec>> pipeIn;
     std::shared_ptr<Pipe<DeviceMemory<float>>> pipeOut;
 };
@@ -154,15 +163,22 @@ private:
     std::shared_ptr<Pipe<DeviceMemory<float>>> pipeIn, pipeOut;
 };
 
+// Device slices -> host slices, into page-locked slots of its output pipe
+// (the mirror of DeviceUploadAgent).
 class DeviceMemoryDownloadAgent : public SequentialAgentBase {
 public:
     DeviceMemoryDownloadAgent(const std::string& pipeName, size_t width, size_t height);
+    ~DeviceMemoryDownloadAgent() override;
+    void GetReady() override;
+    size_t NumPinnedSlots() const;
 
 private:
     void SetPipesImpl() override;
     void WorkFlow0() override;
     const std::string pipeName;
     const size_t width, height;
+    std::unique_ptr<PinnedSlots> pinned;
+    void* stream = nullptr;  // cudaStream_t
     std::shared_ptr<Pipe<DeviceMemory<float>>> pipeIn;
     std::shared_ptr<Pipe<FloatVec>> pipeOut;
 };

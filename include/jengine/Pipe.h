@@ -130,6 +130,8 @@ public:
     ReadToken GetReadToken() { return ReadToken(AcquireRead(), this); }
 
     T& Slot(size_t pos) { return buffers[pos % buffers.size()]; }
+    // Slots allocated so far (0 until the pipe has its template, producer and consumer).
+    size_t NumSlots() const { return buffers.size(); }
 
 private:
     void AllocateSlots(size_t n) override { buffers.resize(n, buffers[0]); }

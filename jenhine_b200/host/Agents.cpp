@@ -350,10 +350,66 @@ void ZFilterAgent::ProcessTask(size_t ti, std::unique_ptr<TaskBase> base) {
     st.Sync();
 }
 
+// ---- page-locked pipe slots ------------------------------------------------------
+
+// Registers every slot of a host pipe with cudaHostRegister, so that copies to
+// and from the slots are DMA from / to them directly.  A slot the driver does
+// not register (e.g. a small one sharing a page with another registration)
+// stays pageable: its copies are still correct, through the driver's staging.
+class PinnedSlots {
+public:
+    template <class T>
+    explicit PinnedSlots(Pipe<std::vector<T>>& p) {
+        for (size_t i = 0; i < p.NumSlots(); ++i) {
+            std::vector<T>& s = p.Slot(i);
+            if (s.empty()) continue;
+            if (cudaHostRegister(s.data(), s.size() * sizeof(T), cudaHostRegisterDefault) == cudaSuccess)
+                ptrs.push_back(s.data());
+            else
+                cudaGetLastError();
+        }
+    }
+    ~PinnedSlots() {
+        for (void* p : ptrs) cudaHostUnregister(p);
+    }
+    size_t Count() const { return ptrs.size(); }
+
+private:
+    std::vector<void*> ptrs;
+};
+
+static cudaStream_t new_stream() {
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        ThrowExceptionAndLog("CUDA failed to create a stream");
+    }
+    return s;
+}
+
+// One frame, asynchronously on `stream`, complete when this returns (the
+// pipe token that owns the memory is released right after).
+static void copy_frame(void* d, const void* s, size_t n, cudaMemcpyKind k, void* stream) {
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(d, s, n, k, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        ThrowExceptionAndLog("CUDA frame copy failed");
+    }
+}
+
 // ---- DeviceUploadAgent (CUDA/Tex2DUploadAgent.cpp:19-67) ------------------------
 
 DeviceUploadAgent::DeviceUploadAgent(const std::string& pipeName, size_t width, size_t height)
     : SequentialAgentBase("DeviceUploadAgent", 1), pipeName(pipeName), width(width), height(height) {}
+DeviceUploadAgent::~DeviceUploadAgent() {
+    pinned.reset();
+    if (stream) cudaStreamDestroy(static_cast<cudaStream_t>(stream));
+}
+void DeviceUploadAgent::GetReady() {
+    pinned.reset(new PinnedSlots(*pipeIn));
+    if (!stream) stream = new_stream();
+}
+size_t DeviceUploadAgent::NumPinnedSlots() const { return pinned ? pinned->Count() : 0; }
 
 void DeviceUploadAgent::SetPipesImpl() {
     pipeIn = BranchPipeFromTrunk<FloatVec>(pipeName);
@@ -370,7 +426,8 @@ void DeviceUploadAgent::WorkFlow0() {
             auto rt = pipeIn->GetReadToken();
             auto wt = pipeOut->GetWriteToken(1, rt.IsShotEnd());
             ThreadOccupiedScope occupied(this);
-            CopyToDevice(wt.GetBuffer(0).Data(), rt.GetBuffer(0).data(), width * height * sizeof(float));
+            copy_frame(wt.GetBuffer(0).Data(), rt.GetBuffer(0).data(), width * height * sizeof(float),
+                       cudaMemcpyHostToDevice, stream);
         }
     } catch (PipeClosedAndEmptySignal&) {
         pipeOut->Close();
@@ -441,6 +498,15 @@ void BPCUDAAgent::WorkFlow0() {
 
 DeviceMemoryDownloadAgent::DeviceMemoryDownloadAgent(const std::string& pipeName, size_t width, size_t height)
     : SequentialAgentBase("DeviceMemoryDownloadAgent", 1), pipeName(pipeName), width(width), height(height) {}
+DeviceMemoryDownloadAgent::~DeviceMemoryDownloadAgent() {
+    pinned.reset();
+    if (stream) cudaStreamDestroy(static_cast<cudaStream_t>(stream));
+}
+void DeviceMemoryDownloadAgent::GetReady() {
+    pinned.reset(new PinnedSlots(*pipeOut));
+    if (!stream) stream = new_stream();
+}
+size_t DeviceMemoryDownloadAgent::NumPinnedSlots() const { return pinned ? pinned->Count() : 0; }
 
 void DeviceMemoryDownloadAgent::SetPipesImpl() {
     pipeIn = BranchPipeFromTrunk<DeviceMemory<float>>(pipeName);
@@ -457,7 +523,8 @@ void DeviceMemoryDownloadAgent::WorkFlow0() {
             auto rt = pipeIn->GetReadToken();
             auto wt = pipeOut->GetWriteToken(1, rt.IsShotEnd());
             ThreadOccupiedScope occupied(this);
-            CopyToHost(wt.GetBuffer(0).data(), rt.GetBuffer(0).CData(), width * height * sizeof(float));
+            copy_frame(wt.GetBuffer(0).data(), rt.GetBuffer(0).CData(), width * height * sizeof(float),
+                       cudaMemcpyDeviceToHost, stream);
         }
     } catch (PipeClosedAndEmptySignal&) {
         pipeOut->Close();

@@ -3,17 +3,22 @@
 // DeviceUploadAgent -> BPCUDAAgent -> DeviceMemoryDownloadAgent -> CTNumAgent
 // -> Sink (the order of JEngine/JEngine.cpp:186-314).
 //
-// usage: test_agents_gpu <case.bin> <out.bin>
+// usage: test_agents_gpu <case.bin> <out.bin> [folder]
+//   With a folder, the frames come from its Proj_%d.prj files and the
+//   orbit from its PTM.dat (InputAgent, ReadPTMFile), and the slices go to
+//   slice_%d.slc files there (OutputAgent) -- the application's file chain.
 //   case.bin: int32 header [views, detU, detV, X, Y, Z, comp] (comp: -1 no
 //   compositing, else 1 when the detector is on the right), float32 [dso, hsr,
 //   bright, bhc0, bhc1, bhc2, pitchXY, pitchZ, norm0, norm1, cutStart,
 //   cutEnd, nAdj], nAdj adjust points, nAdj levels, views*12 PTM floats,
 //   views*detV*detU uint16 frames.  out.bin: Z*Y*X float32 HU.
 #include <cstdio>
+#include <cstring>
 #include <fstream>
 #include <vector>
 
 #include "jengine/Agents.h"
+#include "jengine/IO.h"
 
 using namespace JEngine;
 
@@ -89,31 +94,65 @@ int main(int argc, char** argv) {
     std::vector<UINT16Vec> frames(V, UINT16Vec(U * H));
     for (auto& fr : frames) f.read((char*)fr.data(), 2 * U * H);
     if (!f) return 3;
+    const std::filesystem::path folder = argc > 3 ? argv[3] : "";
+    if (!folder.empty()) {
+        try {
+            auto fromFile = ReadPTMFile(folder / "PTM.dat", V);
+            for (size_t v = 0; v < V; ++v)
+                if (std::memcmp(fromFile[v].Data(), ptms[v].Data(), 48) != 0) {
+                    std::printf("PTM.dat view %zu differs\n", v);
+                    return 7;
+                }
+            ptms = fromFile;
+        } catch (std::exception& e) {
+            std::printf("exception: %s\n", e.what());
+            return 4;
+        }
+    }
 
     const int shots = 2;  // two scans back to back: the second must not see the first
     std::vector<std::shared_ptr<AgentBase>> agents;
-    agents.push_back(std::make_shared<FrameSource>(frames, U, H, shots, comp));
+    if (folder.empty())
+        agents.push_back(std::make_shared<FrameSource>(frames, U, H, shots, comp));
+    else
+        agents.push_back(std::make_shared<InputAgent>(U, H, V, shots, folder, "Proj_%d.prj", comp));
     agents.push_back(std::make_shared<PreProcessingAgent>(2, 1, U, H, 0, 0, 0, 0, U, H, prm[2],
                                                           FloatVec{prm[3], prm[4], prm[5]}));
     if (comp) agents.push_back(std::make_shared<CompositeAgent>(2, U, H, detRight, prm[0], ptms));
     agents.push_back(std::make_shared<FilterAgent>(2, 240, comp ? 2 * U : U, H, U, detRight, prm[1], prm[10], prm[11],
                                                    adjP, adjL, ptms, prm[0]));
-    agents.push_back(std::make_shared<DeviceUploadAgent>("Proj", U, H));
+    auto upload = std::make_shared<DeviceUploadAgent>("Proj", U, H);
+    agents.push_back(upload);
     agents.push_back(std::make_shared<BPCUDAAgent>(ptms, U, H, X, Y, Z, prm[6], prm[7], Z, 1, "", 7));
-    agents.push_back(std::make_shared<DeviceMemoryDownloadAgent>("Slice", X, Y));
+    auto download = std::make_shared<DeviceMemoryDownloadAgent>("Slice", X, Y);
+    agents.push_back(download);
     agents.push_back(std::make_shared<CTNumAgent>(2, X, Y, prm[8], prm[9], 0.02f));
     auto sink = std::make_shared<SliceSink>(Z);
-    agents.push_back(sink);
+    if (folder.empty())
+        agents.push_back(sink);
+    else
+        agents.push_back(std::make_shared<OutputAgent>(X, Y, folder, "slice_%d.slc"));
 
     std::vector<std::shared_ptr<PipeBase>> trunk;
     try {
         for (auto& a : agents) a->SetPipes(trunk);
         for (auto& a : agents) a->GetReady();
+        std::printf("pinned slots: upload %zu, download %zu\n", upload->NumPinnedSlots(), download->NumPinnedSlots());
+        if (upload->NumPinnedSlots() == 0 || download->NumPinnedSlots() == 0) return 8;
         for (auto& a : agents) a->Start();
         for (auto& a : agents) a->Join();
     } catch (std::exception& e) {
         std::printf("exception: %s\n", e.what());
         return 4;
+    }
+    if (!folder.empty()) {  // the slice files, numbered on across both scans
+        for (size_t s = 0; s < shots * Z; ++s) {
+            std::ifstream in(folder / FormatName("slice_%d.slc", s), std::ios::binary);
+            FloatVec x(X * Y);
+            in.read((char*)x.data(), 4 * X * Y);
+            if (!in) break;
+            sink->slices.push_back(x);
+        }
     }
     std::printf("slices received: %zu (expected %zu)\n", sink->slices.size(), shots * Z);
     if (sink->slices.size() != shots * Z) return 5;

@@ -31,6 +31,18 @@ def test_pipeline_runtime_cpu(tmp_path):
     assert "OK (0 failures)" in r.stdout
 
 
+def test_file_format_agents_cpu(tmp_path):
+    """InputAgent / OutputAgent / ReadPTMFile (include/jengine/IO.h) on files
+    the test program writes and reads back."""
+    exe = str(tmp_path / "test_io")
+    host = os.path.join(ROOT, "jenhine_b200", "host")
+    _build(exe, [os.path.join(CPP, "test_io.cpp"), os.path.join(host, "Pipe.cpp"), os.path.join(host, "Agent.cpp"),
+                 os.path.join(host, "IO.cpp")])
+    r = subprocess.run([exe, str(tmp_path / "files")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "OK (0 failures)" in r.stdout
+
+
 def _write_case(path, g):
     raw = g["raw"]
     V, H, U = raw.shape
@@ -45,9 +57,22 @@ def _write_case(path, g):
             f.write(np.ascontiguousarray(a).tobytes())
 
 
+def _write_files(folder, g):
+    """The application's input files: Proj_%d.prj (uint16 frame, no header)
+    per view and PTM.dat (12 numbers per view, written with enough digits to
+    read back the same float32)."""
+    os.makedirs(folder, exist_ok=True)
+    for v, frame in enumerate(g["raw"].astype(np.uint16)):
+        frame.tofile(os.path.join(folder, f"Proj_{v}.prj"))
+    with open(os.path.join(folder, "PTM.dat"), "w") as f:
+        for p in g["ptms"].astype(np.float32).reshape(-1, 12):
+            f.write(" ".join("%.9g" % x for x in p) + "\n")
+
+
 @pytest.mark.gpu
+@pytest.mark.parametrize("files", [False, True], ids=["pipes", "files"])
 @pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_comp"])
-def test_agent_chain_gpu(tmp_path, name):
+def test_agent_chain_gpu(tmp_path, name, files):
     import torch
     if not torch.cuda.is_available():
         pytest.skip("no GPU")
@@ -59,7 +84,12 @@ def test_agent_chain_gpu(tmp_path, name):
     g = load_golden(name)
     case, out = str(tmp_path / "case.bin"), str(tmp_path / "out.bin")
     _write_case(case, g)
-    r = subprocess.run([exe, case, out], capture_output=True, text=True, timeout=300)
+    args = [exe, case, out]
+    if files:
+        folder = str(tmp_path / "scan")
+        _write_files(folder, g)
+        args.append(folder)
+    r = subprocess.run(args, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     X, Y, Z = (int(v) for v in g["vol"])
     hu = np.fromfile(out, np.float32).reshape(Z, Y, X)
