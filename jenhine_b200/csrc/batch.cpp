@@ -66,7 +66,7 @@ jfdk_status upload_scans(jfdk_batch* b, float* const* d_hu, unsigned* total) {
         s.zpt = bp_slices_per_thread(c) == 4 ? 4 : 8;
         s.wz = c->w_depends_on_z ? 1 : 0;
         s.gx = (c->X + 31) / 32;
-        s.gy = (c->Y + 7) / 8;
+        s.gy = (c->Y + kBPTileY - 1) / kBPTileY;
         s.gz = (c->Z + s.zpt - 1) / s.zpt;
         s.first_tile = first;
         first += (unsigned)s.gx * s.gy * s.gz;

@@ -22,7 +22,7 @@
 // writes it).  The taper is stored as pairs (w[c], w[c+1]).  The volume is
 // [z][y][x], x fastest.
 //
-// Work split.  A CTA is 32 x 8 threads over (x, y); each thread owns ZPT
+// Work split.  A CTA is 32 x kBPTileY threads over (x, y); each thread owns ZPT
 // consecutive slices of its (x, y) column and keeps (sum, weight) pairs in
 // registers across all views of the launch, so a launch covering every view
 // stores the volume once and never reads it.
@@ -45,30 +45,33 @@
 namespace jfdk {
 namespace {
 
+constexpr int kBPThreads = 32 * kBPTileY;
+
 // Resident CTAs per SM the compiler must allow for: 8 slices per thread fit
-// in 64 registers at 4 CTAs (32 warps) per SM, which measured faster than the
-// 80-register, 3-CTA allocation the compiler picks unconstrained.
-constexpr int bp_min_blocks(int zpt) { return zpt == 8 ? 4 : 1; }
+// in 64 registers at 32 warps per SM, which measured faster than the
+// 80-register allocation the compiler picks unconstrained.  Small CTAs
+// (4 warps, 8 per SM) measured 4 % faster than 8-warp ones: a finishing CTA
+// leaves fewer warps idle while the SM waits for the next.
+constexpr int bp_min_blocks(int zpt) { return zpt == 8 ? 1024 / kBPThreads : 1; }
 
 template <int ZPT, bool FINALIZE, bool EXACT, bool WZ>
 __device__ __forceinline__ void bp_block(const BPParams& p, int bx, int by, int bz) {
     const int x = bx * 32 + threadIdx.x;
-    const int y = by * 8 + threadIdx.y;
+    const int y = by * kBPTileY + threadIdx.y;
     const int zb = p.z_begin + bz * ZPT;
     if (x >= p.X || y >= p.Y) return;
 
     const float ax = bp_axis(x, p.X, p.pxy), ay = bp_axis(y, p.Y, p.pxy);
     float az[ZPT];
     float2 acc[ZPT];  // (sum, weight)
-    const size_t plane = (size_t)p.X * p.Y;
-    const size_t base = (size_t)y * p.X + x;
 #pragma unroll
     for (int k = 0; k < ZPT; ++k) {
         az[k] = bp_axis(zb + k, p.Z, p.pz);
-        const bool in = zb + k < p.z_end;
-        acc[k] = (!FINALIZE && p.load_acc && in)
-                     ? f2(p.sum[(size_t)(zb + k) * plane + base], p.cnt[(size_t)(zb + k) * plane + base])
-                     : f2(0.0f, 0.0f);
+        acc[k] = f2(0.0f, 0.0f);
+        if (!FINALIZE && p.load_acc && zb + k < p.z_end) {
+            const size_t i = ((size_t)(zb + k) * p.Y + y) * p.X + x;
+            acc[k] = f2(p.sum[i], p.cnt[i]);
+        }
     }
     const float umax = (float)(p.U - 1), vmax = (float)(p.V - 1);
     const float2 neg1 = f2(-1.0f, -1.0f);
@@ -113,10 +116,12 @@ __device__ __forceinline__ void bp_block(const BPParams& p, int bx, int by, int 
         }
     }
 
+    // The output index is formed here, not before the view loop, so that it
+    // holds no registers across the loop.
 #pragma unroll
     for (int k = 0; k < ZPT; ++k) {
         if (zb + k >= p.z_end) break;
-        const size_t idx = (size_t)(zb + k) * plane + base;
+        const size_t idx = ((size_t)(zb + k) * p.Y + y) * p.X + x;
         if (FINALIZE) {
             float o = __fdiv_rn(acc[k].x, acc[k].y);   // BPCore::DoneSlice
             if (p.apply_ct) o = ct_number(o, p.ct_scale, p.ct_norm1);
@@ -157,21 +162,20 @@ __device__ __forceinline__ float rcp_approx(float x) {
 template <int ZPT, bool FINALIZE, bool WZ>
 __device__ __forceinline__ void bp_mixed_block(const BPParams& p, int bx, int by, int bz) {
     const int x = bx * 32 + threadIdx.x;
-    const int y = by * 8 + threadIdx.y;
+    const int y = by * kBPTileY + threadIdx.y;
     const int zb = p.z_begin + bz * ZPT;
     if (x >= p.X || y >= p.Y) return;
     const float ax = (x - 0.5f * (p.X - 1)) * p.pxy;
     const float ay = (y - 0.5f * (p.Y - 1)) * p.pxy;
     const float az0 = (zb - 0.5f * (p.Z - 1)) * p.pz;
     float2 acc[ZPT];  // (sum, weight)
-    const size_t plane = (size_t)p.X * p.Y;
-    const size_t base = (size_t)y * p.X + x;
 #pragma unroll
     for (int k = 0; k < ZPT; ++k) {
-        const bool in = zb + k < p.z_end;
-        acc[k] = (!FINALIZE && p.load_acc && in)
-                     ? f2(p.sum[(size_t)(zb + k) * plane + base], p.cnt[(size_t)(zb + k) * plane + base])
-                     : f2(0.0f, 0.0f);
+        acc[k] = f2(0.0f, 0.0f);
+        if (!FINALIZE && p.load_acc && zb + k < p.z_end) {
+            const size_t i = ((size_t)(zb + k) * p.Y + y) * p.X + x;
+            acc[k] = f2(p.sum[i], p.cnt[i]);
+        }
     }
     const unsigned um1 = (unsigned)(p.U - 1), vm1 = (unsigned)(p.V - 1), uu = (unsigned)p.U;
     const float2 magic = f2(kMagic, kMagic);
@@ -228,7 +232,7 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, int bx, int by
 #pragma unroll
     for (int k = 0; k < ZPT; ++k) {
         if (zb + k >= p.z_end) break;
-        const size_t idx = (size_t)(zb + k) * plane + base;
+        const size_t idx = ((size_t)(zb + k) * p.Y + y) * p.X + x;
         if (FINALIZE) {
             float o = __fdiv_rn(acc[k].x, acc[k].y);
             if (p.apply_ct) o = ct_number(o, p.ct_scale, p.ct_norm1);
@@ -243,12 +247,12 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, int bx, int by
 
 // One CTA = one 32 x 8 x ZPT voxel tile of one launch's grid.
 template <int ZPT, bool FINALIZE, bool EXACT, bool WZ>
-__global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_kernel(BPParams p) {
+__global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_kernel(BPParams p) {
     bp_block<ZPT, FINALIZE, EXACT, WZ>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 template <int ZPT, bool FINALIZE, bool WZ>
-__global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_mixed_kernel(BPParams p) {
+__global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_mixed_kernel(BPParams p) {
     bp_mixed_block<ZPT, FINALIZE, WZ>(p, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
@@ -258,7 +262,7 @@ __global__ void __launch_bounds__(256, bp_min_blocks(ZPT)) bp_mixed_kernel(BPPar
 // scan runs beside the start of the next.  The scan's parameters are copied
 // to shared memory per tile.
 template <bool MIXED>
-__global__ void __launch_bounds__(256, 4) bp_batch_kernel(const BatchScan* __restrict__ scans, int nscans,
+__global__ void __launch_bounds__(kBPThreads, bp_min_blocks(8)) bp_batch_kernel(const BatchScan* __restrict__ scans, int nscans,
                                                           unsigned* __restrict__ counter, unsigned total) {
     __shared__ BPParams sp;
     __shared__ unsigned s_item;
@@ -276,6 +280,7 @@ __global__ void __launch_bounds__(256, 4) bp_batch_kernel(const BatchScan* __res
         const unsigned it = s_item;
         if (it >= total) break;
         const BatchScan& b = scans[s_scan];
+        static_assert(sizeof(BPParams) % 4 == 0 && sizeof(BPParams) / 4 <= kBPThreads, "one word per thread");
         if (tid < (int)(sizeof(BPParams) / 4)) reinterpret_cast<int*>(&sp)[tid] = reinterpret_cast<const int*>(&b.p)[tid];
         __syncthreads();
         const unsigned local = it - b.first_tile;
@@ -421,8 +426,8 @@ __global__ void zfilter_kernel(float* frames, int nv, int rows, int width, long 
 template <int ZPT, bool F, bool E, bool WZ>
 cudaError_t go(const BPParams& p, cudaStream_t s) {
     const int nz = p.z_end - p.z_begin;
-    dim3 grid((p.X + 31) / 32, (p.Y + 7) / 8, (nz + ZPT - 1) / ZPT);
-    bp_kernel<ZPT, F, E, WZ><<<grid, dim3(32, 8), 0, s>>>(p);
+    dim3 grid((p.X + 31) / 32, (p.Y + kBPTileY - 1) / kBPTileY, (nz + ZPT - 1) / ZPT);
+    bp_kernel<ZPT, F, E, WZ><<<grid, dim3(32, kBPTileY), 0, s>>>(p);
     return cudaGetLastError();
 }
 
@@ -434,8 +439,8 @@ cudaError_t go2(const BPParams& p, bool wz, cudaStream_t s) {
 template <int ZPT, bool F, bool WZ>
 cudaError_t go_mixed(const BPParams& p, cudaStream_t s) {
     const int nz = p.z_end - p.z_begin;
-    dim3 grid((p.X + 31) / 32, (p.Y + 7) / 8, (nz + ZPT - 1) / ZPT);
-    bp_mixed_kernel<ZPT, F, WZ><<<grid, dim3(32, 8), 0, s>>>(p);
+    dim3 grid((p.X + 31) / 32, (p.Y + kBPTileY - 1) / kBPTileY, (nz + ZPT - 1) / ZPT);
+    bp_mixed_kernel<ZPT, F, WZ><<<grid, dim3(32, kBPTileY), 0, s>>>(p);
     return cudaGetLastError();
 }
 
@@ -474,9 +479,9 @@ cudaError_t launch_bp_batch(const BatchScan* d_scans, int nscans, unsigned total
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     if (mixed_form)
-        bp_batch_kernel<true><<<ctas, dim3(32, 8), 0, s>>>(d_scans, nscans, counter, total_tiles);
+        bp_batch_kernel<true><<<ctas, dim3(32, kBPTileY), 0, s>>>(d_scans, nscans, counter, total_tiles);
     else
-        bp_batch_kernel<false><<<ctas, dim3(32, 8), 0, s>>>(d_scans, nscans, counter, total_tiles);
+        bp_batch_kernel<false><<<ctas, dim3(32, kBPTileY), 0, s>>>(d_scans, nscans, counter, total_tiles);
     return cudaGetLastError();
 }
 
@@ -485,8 +490,8 @@ cudaError_t bp_batch_ctas(bool mixed_form, int* ctas) {
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-        e = mixed_form ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bp_batch_kernel<true>, 256, 0)
-                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bp_batch_kernel<false>, 256, 0);
+        e = mixed_form ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bp_batch_kernel<true>, kBPThreads, 0)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bp_batch_kernel<false>, kBPThreads, 0);
     *ctas = sms * (per > 0 ? per : 1);
     return e;
 }

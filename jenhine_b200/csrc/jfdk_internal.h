@@ -32,6 +32,10 @@ std::string build_host_operators(const jfdk_scan_params& scan, const jfdk_recon_
                                  int in_w, int out_w, int rows, int mirror, float hsr,
                                  HostOperators& ops);
 
+// Backprojection CTA: 32 x kBPTileY threads over (x, y), each thread a run of
+// slices in z (4 or 8 per thread).
+constexpr int kBPTileY = 4;
+
 // Parameters of the backprojection kernel (bp.cu).
 struct BPParams {
     const float4* q4;        // quads, [slots][rows][U]: (p[r][c], p[r+1][c], p[r][c+1], p[r+1][c+1])
