@@ -139,13 +139,14 @@ __device__ __forceinline__ void bp_block(const BPParams& p, int bx, int by, int 
 // p00 = p[r][c], p01 = p[r][c+1], p10 = p[r+1][c], p11 = p[r+1][c+1],
 // divided by the view's power-of-two scale s, as the coefficients of the
 // bilinear form  val = p00 + fx dx + fy (dy + fx dxy):
-//   .x  half2 (p00, dx = p01 - p00) / s
-//   .y  half2 (dy = p10 - p00, dxy = p11 - p10 - p01 + p00) / s
-//   .z  float w[c]                 the taper at c
-//   .w  float w[c+1] - w[c]        and its step to c+1
+//   .x  float p00 / s                  (exact)
+//   .y  half2 (dx = p01 - p00, dxy = p11 - p10 - p01 + p00) / s
+//   .z  half2 (dy = p10 - p00) / s, w[c+1] - w[c]   (the taper's step)
+//   .w  float w[c]                     the taper at c
 // so one 16-byte load per sample fetches everything the sample needs, and
-// the interpolation is two FP16 x FP16 + FP32 fused multiply-adds
-// (fma.rn.f32.f16, products exact in FP32) and one FP32 one.
+// the interpolation is three FP16 x FP16 + FP32 fused multiply-adds
+// (fma.rn.f32.f16, products exact in FP32; the FP32 addends p00 and w[c]
+// need no conversion) and one FP32 one.
 // The coordinates use an approximate reciprocal of W and fused
 // multiply-adds; when W does not depend on z the slices of a thread are
 // equally spaced on the detector and u, v advance by a constant per slice.
@@ -217,15 +218,15 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, int bx, int by
             const bool in = (iu < um1) & (iv < vm1);                  // negative / NaN wrap to large
             const unsigned idx = in ? iv * uu + iu : 0u;
             const uint4 rec = __ldg(q + idx);
-            float v1, inner;   // p00 + fx dx, dy + fx dxy (fx rounded to FP16)
-            asm("{\n .reg .f16 a, dx, dy, dxy, fh;\n .reg .f32 af, dyf;\n"
-                " mov.b32 {a, dx}, %2;\n mov.b32 {dy, dxy}, %3;\n"
-                " cvt.rn.f16.f32 fh, %4;\n cvt.f32.f16 af, a;\n cvt.f32.f16 dyf, dy;\n"
-                " fma.rn.f32.f16 %0, fh, dx, af;\n fma.rn.f32.f16 %1, fh, dxy, dyf;\n}"
-                : "=f"(v1), "=f"(inner)
-                : "r"(rec.x), "r"(rec.y), "f"(f.x));
+            float v1, inner, c;   // p00 + fx dx, dy + fx dxy, w + fx dw (fx rounded to FP16)
+            asm("{\n .reg .f16 dx, dxy, dy, dw, fh;\n .reg .f32 dyf;\n"
+                " mov.b32 {dx, dxy}, %4;\n mov.b32 {dy, dw}, %5;\n"
+                " cvt.rn.f16.f32 fh, %7;\n cvt.f32.f16 dyf, dy;\n"
+                " fma.rn.f32.f16 %0, fh, dx, %3;\n fma.rn.f32.f16 %1, fh, dxy, dyf;\n"
+                " fma.rn.f32.f16 %2, fh, dw, %6;\n}"
+                : "=f"(v1), "=f"(inner), "=f"(c)
+                : "f"(__uint_as_float(rec.x)), "r"(rec.y), "r"(rec.z), "f"(__uint_as_float(rec.w)), "f"(f.x));
             const float val = fmaf(f.y, inner, v1);
-            const float c = fmaf(f.x, __uint_as_float(rec.w), __uint_as_float(rec.z));
             if (in) acc[k] = pfma(f2(s, 1.0f), f2(val, c), acc[k]);
         }
     }
@@ -346,22 +347,20 @@ __global__ void __launch_bounds__(256) pack_mixed_kernel(const float* __restrict
     const float2 w = tw[(size_t)view * U + c];
     const float p00 = src[0] * w.x, p10 = down ? src[U] * w.x : 0.0f;
     const float p01 = right ? src[1] * w.y : 0.0f, p11 = (right && down) ? src[U + 1] * w.y : 0.0f;
-    // Each coefficient is rounded against the already rounded ones, so every
-    // corner the form reproduces carries the rounding of one coefficient
-    // only: p00 that of a, p01 that of dx (a difference, usually far smaller
-    // than the values), p10 that of dy, p11 that of dxy.
+    // p00 is kept in FP32; each difference is rounded against the already
+    // rounded ones, so every corner the form reproduces carries the rounding
+    // of one coefficient only: p01 that of dx (a difference, usually far
+    // smaller than the values), p10 that of dy, p11 that of dxy.
     const float a = p00 * inv, b = p01 * inv, cc = p10 * inv, d = p11 * inv;   // exact: inv a power of two
-    const __half ha = __float2half_rn(a);
-    const float ra = __half2float(ha);
-    const __half hdx = __float2half_rn(b - ra), hdy = __float2half_rn(cc - ra);
-    const __half hdxy = __float2half_rn(d - (ra + __half2float(hdx) + __half2float(hdy)));
-    const __half2 lo = __halves2half2(ha, hdx);
-    const __half2 hi = __halves2half2(hdy, hdxy);
+    const __half hdx = __float2half_rn(b - a), hdy = __float2half_rn(cc - a);
+    const __half hdxy = __float2half_rn(d - (a + __half2float(hdx) + __half2float(hdy)));
+    const __half2 d1 = __halves2half2(hdx, hdxy);
+    const __half2 d2 = __halves2half2(hdy, __float2half_rn(w.y - w.x));
     uint4 rec;
-    rec.x = *reinterpret_cast<const unsigned*>(&lo);
-    rec.y = *reinterpret_cast<const unsigned*>(&hi);
-    rec.z = __float_as_uint(w.x);
-    rec.w = __float_as_uint(w.y - w.x);
+    rec.x = __float_as_uint(a);
+    rec.y = *reinterpret_cast<const unsigned*>(&d1);
+    rec.z = *reinterpret_cast<const unsigned*>(&d2);
+    rec.w = __float_as_uint(w.x);
     qh[(size_t)(slot0 + f) * q_frame + (size_t)r * U + c] = rec;
 }
 
