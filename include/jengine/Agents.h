@@ -141,12 +141,26 @@ private:
     std::shared_ptr<Pipe<DeviceMemory<float>>> pipeOut;
 };
 
+// The volume is reconstructed in numReconParts parts of numSlicesPerRecon
+// slices (the last part may be shorter): shot i of the input pipe is
+// backprojected into part i mod numReconParts only, and that part's slices
+// are written out at its end, the last slice of the volume marking the shot
+// end (BPCUDAAgent/BPCUDAAgent.cpp:88-110, 244-290); the input agent repeats
+// the views once per part.  The accumulators hold one part; GetReady
+// allocates them, so a volume that does not fit fails there with "CUDA failed
+// to malloc ", which the application's retry loop answers with more parts
+// (PrepareAgentsWithRetry).  deviceMemoryBudget (an addition: 0 = no bound)
+// bounds the device memory the backprojection may take on top of its
+// context's fixed tables: the accumulators of one part and the packed store
+// of one chunk of views.  The reference's cache file
+// of precomputed weights has no counterpart: the weights are accumulated in
+// the same pass as the values.
 class BPCUDAAgent : public SequentialAgentBase {
 public:
     BPCUDAAgent(const std::vector<ProjectionMatrix>& projectionMatrices, size_t numDetectorsU, size_t numDetectorsV,
                 size_t volumeSizeX, size_t volumeSizeY, size_t volumeSizeZ, float pitchXY, float pitchZ,
                 size_t numSlicesPerRecon, size_t numReconParts, const std::filesystem::path& tempFileFolder,
-                size_t viewsPerChunk = 16);
+                size_t viewsPerChunk = 16, size_t deviceMemoryBudget = 0);
     ~BPCUDAAgent() override;
     void GetReady() override;
 
@@ -157,7 +171,9 @@ private:
     const std::vector<ProjectionMatrix> projectionMatrices;
     const size_t numDetectorsU, numDetectorsV, volumeSizeX, volumeSizeY, volumeSizeZ;
     const float pitchXY, pitchZ;
-    const size_t viewsPerChunk;
+    const size_t numSlicesPerRecon, numReconParts;
+    const size_t viewsPerChunk, deviceMemoryBudget;
+    size_t shot = 0;
     std::unique_ptr<StageContext> stage;
     std::unique_ptr<DeviceMemory<float>> staging;
     std::shared_ptr<Pipe<DeviceMemory<float>>> pipeIn, pipeOut;

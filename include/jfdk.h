@@ -159,6 +159,22 @@ jfdk_status jfdk_zfilter_frames(jfdk_ctx* ctx, float* d_frames, int nv);
  * accumulated into the context's sum and weight volumes.  d_proj: nv x rows
  * x filter_out_w float.  A view with IsShotStart first calls jfdk_bp_reset. */
 jfdk_status jfdk_bp_reset(jfdk_ctx* ctx);
+/* Restrict jfdk_bp_reset, jfdk_bp_accumulate and jfdk_finalize to slices
+ * [z_begin, z_begin + z_count) of the volume: one part of a volume
+ * reconstructed in numReconParts parts of numSlicesPerRecon slices, all
+ * views backprojected once per part (BPCUDAAgent/BPCUDAAgent.cpp:244-290,
+ * BPCUDACore.cpp:17-38, JEngine/JEngine.cpp:167-175).  The accumulators are
+ * sized to z_count slices here, so an out-of-memory failure surfaces at this
+ * call (JFDK_ERR_OOM, "CUDA failed to malloc ..."), where JEngine's retry
+ * loop expects it.  jfdk_finalize then takes slices of the slab only.  The
+ * default slab is the whole volume; the derivatives need the whole volume. */
+jfdk_status jfdk_bp_set_slab(jfdk_ctx* ctx, int z_begin, int z_count);
+/* Allocate now the packed store jfdk_bp_accumulate needs for calls of up to
+ * `views` views (otherwise the first such call allocates it), so that every
+ * allocation of the accumulating backprojection happens before the first
+ * frame arrives: with jfdk_bp_set_slab, at the agent's GetReady, where
+ * JEngine's retry loop catches an out-of-memory failure. */
+jfdk_status jfdk_bp_reserve(jfdk_ctx* ctx, int views);
 jfdk_status jfdk_bp_accumulate(jfdk_ctx* ctx, const float* d_proj, int v0, int nv);
 
 /* BPCore::DoneSlice + CTNumCore::Process for slices [z0, z0+nz)
@@ -201,7 +217,13 @@ enum {
     JFDK_OPT_FILTER_SIMT = 5, /* 1: ramp product on FP32 CUDA cores (same as
                                  JFDK_OPT_RAMP_PRODUCT = JFDK_RAMP_FP32_SIMT);
                                  0: the form's default                          */
-    JFDK_OPT_RAMP_PRODUCT = 6 /* how the ramp product runs, a jfdk_ramp_product */
+    JFDK_OPT_RAMP_PRODUCT = 6,/* how the ramp product runs, a jfdk_ramp_product */
+    JFDK_OPT_DEVICE_MEMORY_LIMIT = 7 /* bytes of device memory the context may hold
+                                 in all (0, default: no limit).  An allocation
+                                 that would exceed it fails like cudaMalloc:
+                                 JFDK_ERR_OOM, "CUDA failed to malloc ...".  Lets
+                                 a caller sharing the GPU bound the engine, and
+                                 choose the z-parts of jfdk_bp_set_slab ahead  */
 };
 /* Ramp products (JFDK_OPT_RAMP_PRODUCT).  The split products run on the
  * tcgen05 tensor cores as hi*hi + hi*lo + lo*hi with FP32 accumulation. */
@@ -293,6 +315,9 @@ jfdk_status jfdk_get_uweights(const jfdk_ctx* ctx, float* h_out);
 jfdk_status jfdk_get_ramp_operator(const jfdk_ctx* ctx, float* h_T, float* h_c);
 /* Number of kernels this context has launched (a counter, for benchmarks). */
 long long jfdk_kernel_launches(const jfdk_ctx* ctx);
+/* Bytes of device memory the context holds now (what
+ * JFDK_OPT_DEVICE_MEMORY_LIMIT bounds). */
+long long jfdk_device_bytes(const jfdk_ctx* ctx);
 
 /* jfdk_sync also reports JFDK_ERR_CUDA when a kernel's bounded wait gave up
  * (the device status word is then cleared). */

@@ -28,6 +28,7 @@ OPT_STAGE_TIMING = 3
 OPT_BP_ZPT = 4
 OPT_FILTER_SIMT = 5
 OPT_RAMP_PRODUCT = 6
+OPT_DEVICE_MEMORY_LIMIT = 7
 AUTOTUNE_FORCE = 1
 BATCH_AUTOTUNE, BATCH_GRAPH = 1, 2
 RAMP_DEFAULT, RAMP_TF32X3, RAMP_BF16X3, RAMP_FP16X3, RAMP_FP32_SIMT = 0, 1, 2, 3, 4
@@ -81,6 +82,8 @@ _SIGS = {
     "jfdk_zfilter_frames": ([_P, _P, C.c_int], C.c_int),
     "jfdk_composite_frames": ([_P, _P, _P, C.c_int, C.c_int, _P], C.c_int),
     "jfdk_bp_reset": ([_P], C.c_int),
+    "jfdk_bp_set_slab": ([_P, C.c_int, C.c_int], C.c_int),
+    "jfdk_bp_reserve": ([_P, C.c_int], C.c_int),
     "jfdk_bp_accumulate": ([_P, _P, C.c_int, C.c_int], C.c_int),
     "jfdk_finalize": ([_P, C.c_int, C.c_int, C.c_int, _P, _P], C.c_int),
     "jfdk_ctnum": ([_P, _P, C.c_size_t], C.c_int),
@@ -89,6 +92,7 @@ _SIGS = {
     "jfdk_get_uweights": ([_P, _P], C.c_int),
     "jfdk_get_ramp_operator": ([_P, _P, _P], C.c_int),
     "jfdk_kernel_launches": ([_P], C.c_longlong),
+    "jfdk_device_bytes": ([_P], C.c_longlong),
     "jfdk_device_check": ([C.c_char_p, C.c_int], C.c_int),
     "jfdk_set_bp_geometry": ([_P, _P], C.c_int),
     "jfdk_bp_adjoint": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),

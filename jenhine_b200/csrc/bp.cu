@@ -69,7 +69,7 @@ __device__ __forceinline__ void bp_block(const BPParams& p, int bx, int by, int 
         az[k] = bp_axis(zb + k, p.Z, p.pz);
         acc[k] = f2(0.0f, 0.0f);
         if (!FINALIZE && p.load_acc && zb + k < p.z_end) {
-            const size_t i = ((size_t)(zb + k) * p.Y + y) * p.X + x;
+            const size_t i = ((size_t)(zb + k - p.acc_z0) * p.Y + y) * p.X + x;
             acc[k] = f2(p.sum[i], p.cnt[i]);
         }
     }
@@ -121,13 +121,14 @@ __device__ __forceinline__ void bp_block(const BPParams& p, int bx, int by, int 
 #pragma unroll
     for (int k = 0; k < ZPT; ++k) {
         if (zb + k >= p.z_end) break;
-        const size_t idx = ((size_t)(zb + k) * p.Y + y) * p.X + x;
         if (FINALIZE) {
+            const size_t idx = ((size_t)(zb + k) * p.Y + y) * p.X + x;
             float o = __fdiv_rn(acc[k].x, acc[k].y);   // BPCore::DoneSlice
             if (p.apply_ct) o = ct_number(o, p.ct_scale, p.ct_norm1);
             if (p.out) p.out[idx] = o;
             if (p.out16) p.out16[idx] = to_i16(o);
         } else {
+            const size_t idx = ((size_t)(zb + k - p.acc_z0) * p.Y + y) * p.X + x;
             p.sum[idx] = acc[k].x;
             p.cnt[idx] = acc[k].y;
         }
@@ -174,7 +175,7 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, int bx, int by
     for (int k = 0; k < ZPT; ++k) {
         acc[k] = f2(0.0f, 0.0f);
         if (!FINALIZE && p.load_acc && zb + k < p.z_end) {
-            const size_t i = ((size_t)(zb + k) * p.Y + y) * p.X + x;
+            const size_t i = ((size_t)(zb + k - p.acc_z0) * p.Y + y) * p.X + x;
             acc[k] = f2(p.sum[i], p.cnt[i]);
         }
     }
@@ -233,13 +234,14 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, int bx, int by
 #pragma unroll
     for (int k = 0; k < ZPT; ++k) {
         if (zb + k >= p.z_end) break;
-        const size_t idx = ((size_t)(zb + k) * p.Y + y) * p.X + x;
         if (FINALIZE) {
+            const size_t idx = ((size_t)(zb + k) * p.Y + y) * p.X + x;
             float o = __fdiv_rn(acc[k].x, acc[k].y);
             if (p.apply_ct) o = ct_number(o, p.ct_scale, p.ct_norm1);
             if (p.out) p.out[idx] = o;
             if (p.out16) p.out16[idx] = to_i16(o);
         } else {
+            const size_t idx = ((size_t)(zb + k - p.acc_z0) * p.Y + y) * p.X + x;
             p.sum[idx] = acc[k].x;
             p.cnt[idx] = acc[k].y;
         }

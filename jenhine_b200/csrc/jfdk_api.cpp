@@ -45,23 +45,37 @@ jfdk_status cuda_fail(jfdk_ctx* c, cudaError_t e, const char* what) {
         ++(ctx)->launches;                                  \
     } while (0)
 
+// Every device allocation of a context goes through dev_alloc / dev_free,
+// which keep the context's total; a request that would take the total past
+// JFDK_OPT_DEVICE_MEMORY_LIMIT fails exactly like a failed cudaMalloc.
 template <class T>
 jfdk_status dev_alloc(jfdk_ctx* c, T** p, size_t count, const char* what) {
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
     void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    cudaError_t e = cudaErrorMemoryAllocation;
+    if (c->mem_limit <= 0 || c->dev_bytes + (long long)bytes <= c->mem_limit) e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(c, e == cudaErrorMemoryAllocation ? JFDK_ERR_OOM : JFDK_ERR_CUDA,
                     std::string("CUDA failed to malloc ") + std::to_string(count * sizeof(T)) +
                         " bytes for " + what);
     }
+    c->alloc_bytes[q] = bytes;
+    c->dev_bytes += (long long)bytes;
     *p = static_cast<T*>(q);
     return JFDK_OK;
 }
 
 template <class T>
-void dev_free(T*& p) {
-    if (p) cudaFree(p);
+void dev_free(jfdk_ctx* c, T*& p) {
+    if (p) {
+        auto it = c->alloc_bytes.find(p);
+        if (it != c->alloc_bytes.end()) {
+            c->dev_bytes -= (long long)it->second;
+            c->alloc_bytes.erase(it);
+        }
+        cudaFree(p);
+    }
     p = nullptr;
 }
 
@@ -71,9 +85,9 @@ long long frame_px(const jfdk_ctx* c) { return (long long)c->rows * c->out_w; }
 
 jfdk_status ensure_A(jfdk_ctx* c, size_t rows) {
     if (c->a_rows >= rows) return JFDK_OK;
-    dev_free(c->d_A);
-    dev_free(c->d_e);
-    dev_free(c->d_arow);
+    dev_free(c, c->d_A);
+    dev_free(c, c->d_e);
+    dev_free(c, c->d_arow);
     c->a_rows = 0;
     // room for a high and a low part of up to 4 bytes each
     jfdk_status st = dev_alloc(c, reinterpret_cast<float**>(&c->d_A), rows * a_pitch(c) * 2, "the weighted rows");
@@ -109,8 +123,8 @@ AOperand a_operand(const jfdk_ctx* c) {
 
 jfdk_status ensure_plain(jfdk_ctx* c, int views) {
     if (c->plain_views >= views) return JFDK_OK;
-    dev_free(c->d_plain); dev_free(c->d_Tt); dev_free(c->d_rt); dev_free(c->d_qadj); dev_free(c->d_partial);
-    dev_free(c->d_dptm);
+    dev_free(c, c->d_plain); dev_free(c, c->d_Tt); dev_free(c, c->d_rt); dev_free(c, c->d_qadj); dev_free(c, c->d_partial);
+    dev_free(c, c->d_dptm);
     c->plain_views = 0;
     jfdk_status st = dev_alloc(c, &c->d_plain, (size_t)views * frame_px(c), "the filtered frames");
     if (st) return st;
@@ -120,7 +134,7 @@ jfdk_status ensure_plain(jfdk_ctx* c, int views) {
 
 jfdk_status ensure_Q4(jfdk_ctx* c, int views) {
     if (c->q4_views >= views) return JFDK_OK;
-    dev_free(c->d_q4);
+    dev_free(c, c->d_q4);
     c->q4_views = 0;
     jfdk_status st = dev_alloc(c, &c->d_q4, (size_t)views * frame_px(c), "the backprojection quad store");
     if (st) return st;
@@ -130,7 +144,7 @@ jfdk_status ensure_Q4(jfdk_ctx* c, int views) {
 
 jfdk_status ensure_absmax(jfdk_ctx* c, int n) {
     if (c->absmax_n >= n) return JFDK_OK;
-    dev_free(c->d_absmax);
+    dev_free(c, c->d_absmax);
     c->absmax_n = 0;
     jfdk_status st = dev_alloc(c, &c->d_absmax, (size_t)n, "the per-view maxima");
     if (st) return st;
@@ -138,12 +152,27 @@ jfdk_status ensure_absmax(jfdk_ctx* c, int n) {
     return JFDK_OK;
 }
 
+// The accumulating backprojection's slab: slices [slab_z0, slab_z0 + n).
+int slab_slices(const jfdk_ctx* c) { return c->slab_nz > 0 ? c->slab_nz : c->Z; }
+bool whole_volume(const jfdk_ctx* c) { return c->slab_z0 == 0 && slab_slices(c) == c->Z; }
+
+// Accumulators for the slab's slices (BPCUDACore's accumulatedVol of
+// numSlicesEachPart planes, BPCUDAAgent/BPCUDACore.cpp:38).
 jfdk_status ensure_acc(jfdk_ctx* c) {
-    if (c->d_sum) return JFDK_OK;
-    const size_t n = (size_t)c->X * c->Y * c->Z;
+    const int need = slab_slices(c);
+    if (c->d_sum && c->acc_slices >= need) return JFDK_OK;
+    dev_free(c, c->d_sum);
+    dev_free(c, c->d_cnt);
+    c->acc_slices = 0;
+    const size_t n = (size_t)c->X * c->Y * need;
     jfdk_status st = dev_alloc(c, &c->d_sum, n, "the backprojection sum volume");
-    if (st) return st;
-    return dev_alloc(c, &c->d_cnt, n, "the backprojection weight volume");
+    if (!st) st = dev_alloc(c, &c->d_cnt, n, "the backprojection weight volume");
+    if (st) {
+        dev_free(c, c->d_sum);
+        return st;
+    }
+    c->acc_slices = need;
+    return JFDK_OK;
 }
 
 // Conjugate-view compositing is on when the filter reads rows twice the
@@ -381,17 +410,18 @@ jfdk_status jfdk_device_check(char* msg, int msg_len) {
 const char* jfdk_last_error(const jfdk_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
 long long jfdk_kernel_launches(const jfdk_ctx* c) { return c ? c->launches : 0; }
+long long jfdk_device_bytes(const jfdk_ctx* c) { return c ? c->dev_bytes : 0; }
 
 void jfdk_destroy(jfdk_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
-    dev_free(c->d_ptm); dev_free(c->d_tw); dev_free(c->d_tinv); dev_free(c->d_dmin); dev_free(c->d_pw);
-    dev_free(c->d_tinv_view); dev_free(c->d_cmask);
-    dev_free(c->d_T); dev_free(c->d_Th); dev_free(c->d_Tl); dev_free(c->d_Tb); dev_free(c->d_Tf);
-    dev_free(c->d_status); dev_free(c->d_c); dev_free(c->d_A); dev_free(c->d_e); dev_free(c->d_arow);
-    dev_free(c->d_plain);
-    dev_free(c->d_q4); dev_free(c->d_qscale); dev_free(c->d_absmax);
-    dev_free(c->d_sum); dev_free(c->d_cnt); dev_free(c->d_raw_stage); dev_free(c->d_hu_stage);
+    dev_free(c, c->d_ptm); dev_free(c, c->d_tw); dev_free(c, c->d_tinv); dev_free(c, c->d_dmin); dev_free(c, c->d_pw);
+    dev_free(c, c->d_tinv_view); dev_free(c, c->d_cmask);
+    dev_free(c, c->d_T); dev_free(c, c->d_Th); dev_free(c, c->d_Tl); dev_free(c, c->d_Tb); dev_free(c, c->d_Tf);
+    dev_free(c, c->d_status); dev_free(c, c->d_c); dev_free(c, c->d_A); dev_free(c, c->d_e); dev_free(c, c->d_arow);
+    dev_free(c, c->d_plain);
+    dev_free(c, c->d_q4); dev_free(c, c->d_qscale); dev_free(c, c->d_absmax);
+    dev_free(c, c->d_sum); dev_free(c, c->d_cnt); dev_free(c, c->d_raw_stage); dev_free(c, c->d_hu_stage);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -582,6 +612,10 @@ jfdk_status jfdk_set_option(jfdk_ctx* c, int key, long long value) {
                 for (auto& e : c->ev) JFDK_CUDA(c, cudaEventCreate(&e), "cudaEventCreate");
             c->opt_stage_timing = value ? 1 : 0;
             return JFDK_OK;
+        case JFDK_OPT_DEVICE_MEMORY_LIMIT:
+            if (value < 0) return fail(c, JFDK_ERR_INVALID, "negative memory limit");
+            c->mem_limit = value;
+            return JFDK_OK;
         default: return fail(c, JFDK_ERR_INVALID, "unknown option");
     }
 }
@@ -666,11 +700,27 @@ jfdk_status jfdk_zfilter_frames(jfdk_ctx* c, float* d, int nv) {
     return JFDK_OK;
 }
 
+jfdk_status jfdk_bp_set_slab(jfdk_ctx* c, int z_begin, int z_count) {
+    if (!c || z_begin < 0 || z_count < 1 || z_begin > c->Z - z_count)
+        return fail(c, JFDK_ERR_INVALID, "bp_set_slab: slices outside the volume");
+    c->slab_z0 = z_begin;
+    c->slab_nz = z_count;
+    c->bp_has_views = false;
+    return ensure_acc(c);
+}
+
+jfdk_status jfdk_bp_reserve(jfdk_ctx* c, int views) {
+    if (!c || views < 1 || views > c->nviews) return fail(c, JFDK_ERR_INVALID, "bp_reserve: bad view count");
+    jfdk_status st = ensure_Q4(c, views);
+    if (!st && mixed(c)) st = ensure_absmax(c, views);
+    return st;
+}
+
 jfdk_status jfdk_bp_reset(jfdk_ctx* c) {
     if (!c) return JFDK_ERR_INVALID;
     jfdk_status st = ensure_acc(c);
     if (st) return st;
-    const size_t n = (size_t)c->X * c->Y * c->Z * sizeof(float);
+    const size_t n = (size_t)c->X * c->Y * slab_slices(c) * sizeof(float);
     JFDK_CUDA(c, cudaMemsetAsync(c->d_sum, 0, n, c->stream), "clearing the sum volume");
     JFDK_CUDA(c, cudaMemsetAsync(c->d_cnt, 0, n, c->stream), "clearing the weight volume");
     c->bp_has_views = true;
@@ -688,7 +738,8 @@ jfdk_status jfdk_bp_accumulate(jfdk_ctx* c, const float* d_proj, int v0, int nv)
     if ((st = pack_frames(c, d_proj, nv, v0, 0))) return st;
     BPParams b = bp_params(c);
     b.view_base = v0; b.v0 = v0; b.nv = nv;
-    b.sum = c->d_sum; b.cnt = c->d_cnt; b.load_acc = 1;
+    b.z_begin = c->slab_z0; b.z_end = c->slab_z0 + slab_slices(c);
+    b.sum = c->d_sum; b.cnt = c->d_cnt; b.acc_z0 = c->slab_z0; b.load_acc = 1;
     return run_bp(c, b, false);
 }
 
@@ -696,8 +747,11 @@ jfdk_status jfdk_finalize(jfdk_ctx* c, int z0, int nz, int apply_ct, float* d_ou
     if (!c || z0 < 0 || nz < 0 || z0 + nz > c->Z || (!d_out && !d_out16))
         return fail(c, JFDK_ERR_INVALID, "finalize: bad argument");
     if (!c->d_sum) return fail(c, JFDK_ERR_STATE, "finalize before any backprojection");
+    if (z0 < c->slab_z0 || z0 + nz > c->slab_z0 + slab_slices(c))
+        return fail(c, JFDK_ERR_INVALID, "finalize: slices outside the slab set by bp_set_slab");
     const size_t plane = (size_t)c->X * c->Y;
-    JFDK_LAUNCH(c, launch_finalize(c->d_sum + z0 * plane, c->d_cnt + z0 * plane, nz * plane, apply_ct, c->ct_scale,
+    const size_t off = (size_t)(z0 - c->slab_z0) * plane;
+    JFDK_LAUNCH(c, launch_finalize(c->d_sum + off, c->d_cnt + off, nz * plane, apply_ct, c->ct_scale,
                                    c->recon.ct_norm1, d_out, d_out16, c->stream),
                 "finalize");
     return JFDK_OK;
@@ -729,13 +783,13 @@ jfdk_status jfdk_reconstruct_host(jfdk_ctx* c, const uint16_t* h_raw, float* h_h
     const size_t hu_bytes = (size_t)c->X * c->Y * c->Z * sizeof(float);
     jfdk_status st;
     if (c->raw_stage_bytes < raw_bytes) {
-        dev_free(c->d_raw_stage);
+        dev_free(c, c->d_raw_stage);
         c->raw_stage_bytes = 0;
         if ((st = dev_alloc(c, &c->d_raw_stage, raw_bytes / sizeof(uint16_t), "the raw frames"))) return st;
         c->raw_stage_bytes = raw_bytes;
     }
     if (c->hu_stage_bytes < hu_bytes) {
-        dev_free(c->d_hu_stage);
+        dev_free(c, c->d_hu_stage);
         c->hu_stage_bytes = 0;
         if ((st = dev_alloc(c, &c->d_hu_stage, hu_bytes / sizeof(float), "the output volume"))) return st;
         c->hu_stage_bytes = hu_bytes;
@@ -757,6 +811,8 @@ jfdk_status deriv_check(jfdk_ctx* c, const char* what) {
     if (mixed(c)) return fail(c, JFDK_ERR_UNSUPPORTED, std::string(what) + ": derivatives are of the FP32 form");
     if (!c->d_cnt || !c->bp_has_views)
         return fail(c, JFDK_ERR_STATE, std::string(what) + ": needs the weights of a backprojection (bp_accumulate)");
+    if (!whole_volume(c))
+        return fail(c, JFDK_ERR_STATE, std::string(what) + ": needs the weights of the whole volume, not a slab");
     return JFDK_OK;
 }
 
@@ -805,7 +861,7 @@ jfdk_status jfdk_bp_adjoint(jfdk_ctx* c, const float* d_vol_bar, int v0, int nv,
     jfdk_status st = deriv_check(c, "bp_adjoint");
     if (st || nv == 0) return st;
     if (c->qadj_views < nv) {
-        dev_free(c->d_qadj);
+        dev_free(c, c->d_qadj);
         c->qadj_views = 0;
         if ((st = dev_alloc(c, &c->d_qadj, (size_t)nv * frame_px(c), "the quad-space adjoint"))) return st;
         c->qadj_views = nv;
@@ -860,7 +916,7 @@ jfdk_status jfdk_geometry_gradient(jfdk_ctx* c, const float* d_q, int v0, int nv
     a.dptm = d_dptm;
     const size_t need = geometry_gradient_ctas(a) * 6 * (size_t)nv;
     if (c->partial_n < need) {
-        dev_free(c->d_partial);
+        dev_free(c, c->d_partial);
         c->partial_n = 0;
         if ((st = dev_alloc(c, &c->d_partial, need, "the gradient partial sums"))) return st;
         c->partial_n = need;
@@ -973,7 +1029,7 @@ extern "C" jfdk_status jfdk_autotune(jfdk_ctx* c, int flags) {
         if (st) break;
         if (t < best_t) { best_t = t; best_z = zpt; }
     }
-    dev_free(slab);
+    dev_free(c, slab);
     if (st) return st;
     c->opt_bp_zpt = best_z;
     // views per chunk: the filter stage over the first views of zero frames
@@ -993,7 +1049,7 @@ extern "C" jfdk_status jfdk_autotune(jfdk_ctx* c, int flags) {
             if (t < best_t) { best_t = t; best_c = ch; }
         }
         cudaStreamSynchronize(c->stream);
-        dev_free(raw);
+        dev_free(c, raw);
         if (st) return st;
     }
     c->opt_view_chunk = best_c;

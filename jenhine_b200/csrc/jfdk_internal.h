@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/jfdk.h"
@@ -50,8 +51,9 @@ struct BPParams {
     int X, Y, Z;
     float pxy, pz;
     int z_begin, z_end;      // slices handled by this launch
-    float* sum;              // [Z][Y][X] accumulators (chunked mode)
+    float* sum;              // accumulators (chunked mode): [slices][Y][X] from slice acc_z0
     float* cnt;
+    int acc_z0;
     int load_acc;            // add to sum/cnt already in memory
     float* out;              // finalize: [Z][Y][X] float or null
     int16_t* out16;          // finalize: int16 HU or null
@@ -265,8 +267,10 @@ struct jfdk_ctx {
     float4* d_q4 = nullptr; int q4_views = 0;       // quad store (mixed: uint4 records)
     float* d_qscale = nullptr;                      // mixed: [views] scales
     unsigned* d_absmax = nullptr; int absmax_n = 0; // mixed: per-frame maxima
-    float* d_sum = nullptr;
-    float* d_cnt = nullptr;
+    float* d_sum = nullptr;                          // accumulators of the slab:
+    float* d_cnt = nullptr;                          // [acc_slices][Y][X]
+    int acc_slices = 0;                              // planes allocated
+    int slab_z0 = 0, slab_nz = 0;                    // jfdk_bp_set_slab (nz 0: every slice)
     uint16_t* d_raw_stage = nullptr; size_t raw_stage_bytes = 0;
     float* d_hu_stage = nullptr; size_t hu_stage_bytes = 0;
     bool bp_has_views = false;
@@ -285,6 +289,9 @@ struct jfdk_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
     long long launches = 0;
+    // device memory held (dev_alloc / dev_free) and the JFDK_OPT_DEVICE_MEMORY_LIMIT
+    long long dev_bytes = 0, mem_limit = 0;
+    std::unordered_map<const void*, size_t> alloc_bytes;
     std::string err;
 };
 

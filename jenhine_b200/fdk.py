@@ -154,6 +154,11 @@ class FDKEngine:
     def kernel_launches(self) -> int:
         return self.lib.jfdk_kernel_launches(self.ctx)
 
+    @property
+    def device_bytes(self) -> int:
+        """Device memory the context holds now."""
+        return self.lib.jfdk_device_bytes(self.ctx)
+
     def autotune(self, force: bool = False):
         """Pick slices per thread and views per chunk for this shape (timed on
         the device; cached per shape)."""
@@ -225,6 +230,11 @@ class FDKEngine:
 
     def bp_reset(self):
         self._check(self.lib.jfdk_bp_reset(self.ctx))
+
+    def bp_set_slab(self, z0: int, nz: int):
+        """Accumulate (and finalize) slices [z0, z0 + nz) only: one z-part of a
+        volume reconstructed in parts."""
+        self._check(self.lib.jfdk_bp_set_slab(self.ctx, int(z0), int(nz)))
 
     def bp_accumulate(self, frames, v0: int):
         self._check(self.lib.jfdk_bp_accumulate(self.ctx, _ptr(frames), v0, frames.shape[0]))

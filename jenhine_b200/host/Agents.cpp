@@ -51,7 +51,11 @@ public:
         for (void* b : buf) DeviceFree(b);
         cudaStreamDestroy(stream);
     }
+    // An out-of-memory failure keeps its "CUDA failed to malloc " message
+    // unprefixed: the application's retry loop matches it
+    // (JEngine/JEngine.cpp:413-421).
     void Check(jfdk_status st) const {
+        if (st == JFDK_ERR_OOM) ThrowExceptionAndLog(jfdk_last_error(ctx));
         if (st != JFDK_OK) ThrowExceptionAndLog(std::string("jfdk: ") + jfdk_last_error(ctx));
     }
     void Sync() const { Check(jfdk_sync(ctx)); }
@@ -438,11 +442,18 @@ void DeviceUploadAgent::WorkFlow0() {
 
 BPCUDAAgent::BPCUDAAgent(const std::vector<ProjectionMatrix>& ptms, size_t numDetectorsU, size_t numDetectorsV,
                          size_t volumeSizeX, size_t volumeSizeY, size_t volumeSizeZ, float pitchXY, float pitchZ,
-                         size_t /*numSlicesPerRecon*/, size_t /*numReconParts*/,
-                         const std::filesystem::path& /*tempFileFolder*/, size_t viewsPerChunk)
+                         size_t numSlicesPerRecon, size_t numReconParts,
+                         const std::filesystem::path& /*tempFileFolder*/, size_t viewsPerChunk,
+                         size_t deviceMemoryBudget)
     : SequentialAgentBase("BPCUDAAgent", 1), projectionMatrices(ptms), numDetectorsU(numDetectorsU),
       numDetectorsV(numDetectorsV), volumeSizeX(volumeSizeX), volumeSizeY(volumeSizeY), volumeSizeZ(volumeSizeZ),
-      pitchXY(pitchXY), pitchZ(pitchZ), viewsPerChunk(std::max<size_t>(1, viewsPerChunk)) {}
+      pitchXY(pitchXY), pitchZ(pitchZ),
+      numSlicesPerRecon(std::min(std::max<size_t>(1, numSlicesPerRecon), volumeSizeZ)),
+      numReconParts(std::max<size_t>(1, numReconParts)), viewsPerChunk(std::max<size_t>(1, viewsPerChunk)),
+      deviceMemoryBudget(deviceMemoryBudget) {
+    if (this->numSlicesPerRecon * this->numReconParts < volumeSizeZ)
+        ThrowExceptionAndLog("BPCUDAAgent: numReconParts x numSlicesPerRecon does not cover the volume");
+}
 BPCUDAAgent::~BPCUDAAgent() = default;
 
 void BPCUDAAgent::SetPipesImpl() {
@@ -460,7 +471,14 @@ void BPCUDAAgent::GetReady() {
     r.pitch_xy = pitchXY;
     r.pitch_z = pitchZ;
     stage.reset(new StageContext(s, r, flatten(projectionMatrices)));
+    if (deviceMemoryBudget)
+        stage->Check(jfdk_set_option(stage->ctx, JFDK_OPT_DEVICE_MEMORY_LIMIT,
+                                     jfdk_device_bytes(stage->ctx) + (long long)deviceMemoryBudget));
+    // the accumulators of one part (BPCUDACore's accumulatedVol)
+    stage->Check(jfdk_bp_set_slab(stage->ctx, 0, (int)numSlicesPerRecon));
+    stage->Check(jfdk_bp_reserve(stage->ctx, (int)std::min(viewsPerChunk, projectionMatrices.size())));
     staging.reset(new DeviceMemory<float>(viewsPerChunk * numDetectorsU * numDetectorsV));
+    shot = 0;
 }
 
 void BPCUDAAgent::WorkFlow0() {
@@ -469,7 +487,13 @@ void BPCUDAAgent::WorkFlow0() {
         while (true) {
             auto rt = pipeIn->GetReadToken();
             ThreadOccupiedScope occupied(this);
-            if (rt.IsShotStart()) stage->Check(jfdk_bp_reset(stage->ctx));
+            const size_t part = shot % numReconParts;
+            const size_t z0 = std::min(part * numSlicesPerRecon, volumeSizeZ - 1);
+            const size_t nz = std::min(numSlicesPerRecon, volumeSizeZ - z0);
+            if (rt.IsShotStart()) {
+                stage->Check(jfdk_bp_set_slab(stage->ctx, (int)z0, (int)nz));
+                stage->Check(jfdk_bp_reset(stage->ctx));
+            }
             const size_t n = rt.GetSize();
             const int view = (int)(rt.GetStartIndex() % projectionMatrices.size());
             for (size_t i = 0; i < n; ++i)
@@ -482,11 +506,12 @@ void BPCUDAAgent::WorkFlow0() {
                 stage->Sync();   // the read token (frames) is released only after the kernels read it
             }
             if (rt.IsShotEnd()) {
-                for (size_t z = 0; z < volumeSizeZ; ++z) {  // BPCore::DoneSlice per slice
+                for (size_t z = z0; z < z0 + nz; ++z) {  // the part's slices, one token each
                     auto wt = pipeOut->GetWriteToken(1, z + 1 == volumeSizeZ);
                     stage->Check(jfdk_finalize(stage->ctx, (int)z, 1, 0, wt.GetBuffer(0).Data(), nullptr));
                     stage->Sync();
                 }
+                ++shot;
             }
         }
     } catch (PipeClosedAndEmptySignal&) {

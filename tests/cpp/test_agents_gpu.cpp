@@ -3,10 +3,12 @@
 // DeviceUploadAgent -> BPCUDAAgent -> DeviceMemoryDownloadAgent -> CTNumAgent
 // -> Sink (the order of JEngine/JEngine.cpp:186-314).
 //
-// usage: test_agents_gpu <case.bin> <out.bin> [folder]
+// usage: test_agents_gpu <case.bin> <out.bin> [folder|-] [parts|retry]
 //   With a folder, the frames come from its Proj_%d.prj files and the
 //   orbit from its PTM.dat (InputAgent, ReadPTMFile), and the slices go to
 //   slice_%d.slc files there (OutputAgent) -- the application's file chain.
+//   parts: the volume in that many z-parts; retry: the application's part
+//   loop under a device-memory budget that only 3 or more parts fit.
 //   case.bin: int32 header [views, detU, detV, X, Y, Z, comp] (comp: -1 no
 //   compositing, else 1 when the detector is on the right), float32 [dso, hsr,
 //   bright, bhc0, bhc1, bhc2, pitchXY, pitchZ, norm0, norm1, cutStart,
@@ -19,6 +21,7 @@
 
 #include "jengine/Agents.h"
 #include "jengine/IO.h"
+#include "jengine/ReconParts.h"
 
 using namespace JEngine;
 
@@ -94,7 +97,7 @@ int main(int argc, char** argv) {
     std::vector<UINT16Vec> frames(V, UINT16Vec(U * H));
     for (auto& fr : frames) f.read((char*)fr.data(), 2 * U * H);
     if (!f) return 3;
-    const std::filesystem::path folder = argc > 3 ? argv[3] : "";
+    const std::filesystem::path folder = (argc > 3 && std::string(argv[3]) != "-") ? argv[3] : "";
     if (!folder.empty()) {
         try {
             auto fromFile = ReadPTMFile(folder / "PTM.dat", V);
@@ -110,33 +113,62 @@ int main(int argc, char** argv) {
         }
     }
 
-    const int shots = 2;  // two scans back to back: the second must not see the first
-    std::vector<std::shared_ptr<AgentBase>> agents;
-    if (folder.empty())
-        agents.push_back(std::make_shared<FrameSource>(frames, U, H, shots, comp));
-    else
-        agents.push_back(std::make_shared<InputAgent>(U, H, V, shots, folder, "Proj_%d.prj", comp));
-    agents.push_back(std::make_shared<PreProcessingAgent>(2, 1, U, H, 0, 0, 0, 0, U, H, prm[2],
-                                                          FloatVec{prm[3], prm[4], prm[5]}));
-    if (comp) agents.push_back(std::make_shared<CompositeAgent>(2, U, H, detRight, prm[0], ptms));
-    agents.push_back(std::make_shared<FilterAgent>(2, 240, comp ? 2 * U : U, H, U, detRight, prm[1], prm[10], prm[11],
-                                                   adjP, adjL, ptms, prm[0]));
-    auto upload = std::make_shared<DeviceUploadAgent>("Proj", U, H);
-    agents.push_back(upload);
-    agents.push_back(std::make_shared<BPCUDAAgent>(ptms, U, H, X, Y, Z, prm[6], prm[7], Z, 1, "", 7));
-    auto download = std::make_shared<DeviceMemoryDownloadAgent>("Slice", X, Y);
-    agents.push_back(download);
-    agents.push_back(std::make_shared<CTNumAgent>(2, X, Y, prm[8], prm[9], 0.02f));
-    auto sink = std::make_shared<SliceSink>(Z);
-    if (folder.empty())
-        agents.push_back(sink);
-    else
-        agents.push_back(std::make_shared<OutputAgent>(X, Y, folder, "slice_%d.slc"));
+    // z-parts: a count, or "retry" -- the application's loop over part counts
+    // with the backprojection's device memory bounded so that the
+    // accumulators of ceil(Z / 3) slices fit and those of ceil(Z / 2) do not
+    const std::string partsArg = argc > 4 ? argv[4] : "1";
+    const bool retry = partsArg == "retry";
+    const size_t chunk = 7;
+    size_t budget = 0;
+    // (accumulators: 2 floats a voxel; packed store: 16 bytes a pixel a view;
+    // margin: half a slice of accumulators)
+    if (retry) budget = 2 * X * Y * ((Z + 2) / 3) * 4 + chunk * H * U * 16 + X * Y * 4;
 
+    const int scans = 2;  // two scans back to back: the second must not see the first
+    std::shared_ptr<SliceSink> sink;
+    std::shared_ptr<DeviceUploadAgent> upload;
+    std::shared_ptr<DeviceMemoryDownloadAgent> download;
+    auto makeAgents = [&](const ReconPartPlan& plan) {
+        std::vector<std::shared_ptr<AgentBase>> agents;
+        const int shots = scans * (int)plan.numReconParts;  // the views once per part
+        if (folder.empty())
+            agents.push_back(std::make_shared<FrameSource>(frames, U, H, shots, comp));
+        else
+            agents.push_back(std::make_shared<InputAgent>(U, H, V, shots, folder, "Proj_%d.prj", comp));
+        agents.push_back(std::make_shared<PreProcessingAgent>(2, 1, U, H, 0, 0, 0, 0, U, H, prm[2],
+                                                              FloatVec{prm[3], prm[4], prm[5]}));
+        if (comp) agents.push_back(std::make_shared<CompositeAgent>(2, U, H, detRight, prm[0], ptms));
+        agents.push_back(std::make_shared<FilterAgent>(2, 240, comp ? 2 * U : U, H, U, detRight, prm[1], prm[10],
+                                                       prm[11], adjP, adjL, ptms, prm[0]));
+        upload = std::make_shared<DeviceUploadAgent>("Proj", U, H);
+        agents.push_back(upload);
+        agents.push_back(std::make_shared<BPCUDAAgent>(ptms, U, H, X, Y, Z, prm[6], prm[7], plan.numSlicesPerRecon,
+                                                       plan.numReconParts, "", chunk, budget));
+        download = std::make_shared<DeviceMemoryDownloadAgent>("Slice", X, Y);
+        agents.push_back(download);
+        agents.push_back(std::make_shared<CTNumAgent>(2, X, Y, prm[8], prm[9], 0.02f));
+        sink = std::make_shared<SliceSink>(Z);
+        if (folder.empty())
+            agents.push_back(sink);
+        else
+            agents.push_back(std::make_shared<OutputAgent>(X, Y, folder, "slice_%d.slc"));
+        return agents;
+    };
+
+    std::vector<std::shared_ptr<AgentBase>> agents;
     std::vector<std::shared_ptr<PipeBase>> trunk;
     try {
-        for (auto& a : agents) a->SetPipes(trunk);
-        for (auto& a : agents) a->GetReady();
+        ReconPartPlan plan{1, Z};
+        if (retry) {
+            plan = PrepareAgentsWithRetry(Z, makeAgents, agents, trunk);
+        } else {
+            const size_t parts = std::stoul(partsArg);
+            plan = {parts, (Z - 1) / parts + 1};
+            agents = makeAgents(plan);
+            for (auto& a : agents) a->SetPipes(trunk);
+            for (auto& a : agents) a->GetReady();
+        }
+        std::printf("plan: %zu parts of %zu slices\n", plan.numReconParts, plan.numSlicesPerRecon);
         std::printf("pinned slots: upload %zu, download %zu\n", upload->NumPinnedSlots(), download->NumPinnedSlots());
         if (upload->NumPinnedSlots() == 0 || download->NumPinnedSlots() == 0) return 8;
         for (auto& a : agents) a->Start();
@@ -145,6 +177,7 @@ int main(int argc, char** argv) {
         std::printf("exception: %s\n", e.what());
         return 4;
     }
+    const size_t shots = scans;
     if (!folder.empty()) {  // the slice files, numbered on across both scans
         for (size_t s = 0; s < shots * Z; ++s) {
             std::ifstream in(folder / FormatName("slice_%d.slc", s), std::ios::binary);

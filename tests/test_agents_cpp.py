@@ -43,6 +43,17 @@ def test_file_format_agents_cpu(tmp_path):
     assert "OK (0 failures)" in r.stdout
 
 
+def test_recon_parts_retry_cpu(tmp_path):
+    """z-part plans and the retry on "CUDA failed to malloc " (include/jengine/ReconParts.h)."""
+    exe = str(tmp_path / "test_recon_parts")
+    host = os.path.join(ROOT, "jenhine_b200", "host")
+    _build(exe, [os.path.join(CPP, "test_recon_parts.cpp"), os.path.join(host, "Pipe.cpp"),
+                 os.path.join(host, "Agent.cpp"), os.path.join(host, "ReconParts.cpp")])
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "OK (0 failures)" in r.stdout
+
+
 def _write_case(path, g):
     raw = g["raw"]
     V, H, U = raw.shape
@@ -92,6 +103,33 @@ def test_agent_chain_gpu(tmp_path, name, files):
     r = subprocess.run(args, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     X, Y, Z = (int(v) for v in g["vol"])
+    hu = np.fromfile(out, np.float32).reshape(Z, Y, X)
+    assert rel_l2(hu + 1000.0, g["hu"] + 1000.0) <= 1e-5
+    assert np.max(np.abs(hu - g["hu"])) < 0.5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("parts", ["3", "retry"])
+@pytest.mark.parametrize("name", ["mini_c1", "mini_comp"])
+def test_agent_chain_zparts_gpu(tmp_path, name, parts):
+    """The volume in z-parts (BPCUDAAgent numReconParts / numSlicesPerRecon):
+    3 parts given, or found by the application's retry loop under a
+    device-memory budget that only 3 or more parts fit."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from jenhine_b200 import build
+    lib = build.build()
+    exe = str(tmp_path / "test_agents_gpu")
+    _build(exe, [os.path.join(CPP, "test_agents_gpu.cpp")],
+           ["-L", os.path.dirname(lib), "-ljfdk", f"-Wl,-rpath,{os.path.dirname(lib)}"])
+    g = load_golden(name)
+    case, out = str(tmp_path / "case.bin"), str(tmp_path / "out.bin")
+    _write_case(case, g)
+    r = subprocess.run([exe, case, out, "-", parts], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    X, Y, Z = (int(v) for v in g["vol"])
+    assert f"plan: 3 parts of {(Z + 2) // 3} slices" in r.stdout, r.stdout
     hu = np.fromfile(out, np.float32).reshape(Z, Y, X)
     assert rel_l2(hu + 1000.0, g["hu"] + 1000.0) <= 1e-5
     assert np.max(np.abs(hu - g["hu"])) < 0.5
