@@ -123,8 +123,7 @@ AOperand a_operand(const jfdk_ctx* c) {
 
 jfdk_status ensure_plain(jfdk_ctx* c, int views) {
     if (c->plain_views >= views) return JFDK_OK;
-    dev_free(c, c->d_plain); dev_free(c, c->d_Tt); dev_free(c, c->d_rt); dev_free(c, c->d_qadj); dev_free(c, c->d_partial);
-    dev_free(c, c->d_dptm);
+    dev_free(c, c->d_plain);
     c->plain_views = 0;
     jfdk_status st = dev_alloc(c, &c->d_plain, (size_t)views * frame_px(c), "the filtered frames");
     if (st) return st;
@@ -422,6 +421,8 @@ void jfdk_destroy(jfdk_ctx* c) {
     dev_free(c, c->d_plain);
     dev_free(c, c->d_q4); dev_free(c, c->d_qscale); dev_free(c, c->d_absmax);
     dev_free(c, c->d_sum); dev_free(c, c->d_cnt); dev_free(c, c->d_raw_stage); dev_free(c, c->d_hu_stage);
+    dev_free(c, c->d_Tt); dev_free(c, c->d_rt); dev_free(c, c->d_qadj); dev_free(c, c->d_partial);
+    dev_free(c, c->d_dptm);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);

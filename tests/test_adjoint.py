@@ -97,6 +97,25 @@ def test_filter_adjoint_against_tensor_core_forward(torch_cuda, name):
     assert check_filter_dot(torch_cuda, engine_for(g), g["raw"].shape[0], 2) <= 1e-5
 
 
+def test_derivatives_after_reconstruct(torch_cuda):
+    """A whole reconstruction first (it allocates the filter stage's working
+    buffers) must leave the derivative operators intact: the same adjoint
+    filter and adjoint backprojection as on a fresh context."""
+    torch = torch_cuda
+    g = load_golden("mini_c2")
+    nv = g["raw"].shape[0]
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    fresh, used = fp32_product(engine_for(g)), fp32_product(engine_for(g))
+    used.reconstruct(to_dev(torch, g["raw"]))
+    y = torch.rand((nv, fresh.rows, fresh.filter_out_w), generator=gen, device="cuda")
+    assert torch.equal(fresh.filter_adjoint(y, v0=0), used.filter_adjoint(y, v0=0))
+    q = torch.rand((nv, fresh.rows, fresh.filter_out_w), generator=gen, device="cuda")
+    vols = [bp_forward(e, q)[0] for e in (fresh, used)]
+    assert torch.equal(torch.nan_to_num(vols[0]), torch.nan_to_num(vols[1]))
+    vb = torch.rand(vols[0].shape, generator=gen, device="cuda")
+    assert torch.equal(torch.nan_to_num(fresh.bp_adjoint(vb, 0, nv)), torch.nan_to_num(used.bp_adjoint(vb, 0, nv)))
+
+
 def test_fdk_adjoint_dot_product(torch_cuda):
     """<B F x, y> = <x, F^T B^T y> through the autograd binding's backward."""
     import torch
