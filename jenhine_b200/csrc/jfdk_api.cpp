@@ -270,17 +270,19 @@ jfdk_status pack_frames(jfdk_ctx* c, const float* plain, int nv, int view0, int 
     return JFDK_OK;
 }
 
-jfdk_status run_bp(jfdk_ctx* c, BPParams b, bool finalize) {
+jfdk_status run_bp_on(jfdk_ctx* c, BPParams b, bool finalize, cudaStream_t s) {
     if (mixed(c)) {
         b.qh = reinterpret_cast<const uint4*>(c->d_q4);
         b.qscale = c->d_qscale;
-        JFDK_LAUNCH(c, launch_bp_mixed(b, finalize, c->w_depends_on_z, bp_zpt(c), c->stream), "backprojection");
+        JFDK_LAUNCH(c, launch_bp_mixed(b, finalize, c->w_depends_on_z, bp_zpt(c), s), "backprojection");
         return JFDK_OK;
     }
-    JFDK_LAUNCH(c, launch_bp(b, finalize, c->opt_bp_exact != 0, c->w_depends_on_z, bp_zpt(c), c->stream),
+    JFDK_LAUNCH(c, launch_bp(b, finalize, c->opt_bp_exact != 0, c->w_depends_on_z, bp_zpt(c), s),
                 "backprojection");
     return JFDK_OK;
 }
+
+jfdk_status run_bp(jfdk_ctx* c, BPParams b, bool finalize) { return run_bp_on(c, b, finalize, c->stream); }
 
 cudaError_t launch_ramp(jfdk_ctx* c, RampParams r) {
     const AOperand a = a_operand(c);
@@ -321,7 +323,7 @@ namespace jfdk {
 // Everything jfdk_reconstruct does before the backprojection, for the first
 // nviews views: per chunk of views raw -> weighted rows -> filtered frames
 // (L2-sized buffers) -> [z-filter] -> the BP store of the rotation.
-jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nviews) {
+jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nviews, const cudaEvent_t* chunk_ready) {
     if (nviews < 0 || nviews > c->nviews) nviews = c->nviews;
     if (c->in_w != c->used_u && !compositing(c))
         return fail(c, JFDK_ERR_UNSUPPORTED,
@@ -334,6 +336,7 @@ jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nvi
     const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;
     for (int v0 = 0; v0 < nviews; v0 += chunk) {
         const int nv = std::min(chunk, nviews - v0);
+        if (chunk_ready) JFDK_CUDA(c, cudaStreamWaitEvent(c->stream, chunk_ready[v0 / chunk], 0), "frame transfer");
         PrepParams pp = prep_params(c, d_raw + (size_t)v0 * frame);
         if (compositing(c)) {
             pp.width = c->in_w;
@@ -425,6 +428,12 @@ void jfdk_destroy(jfdk_ctx* c) {
     dev_free(c, c->d_dptm);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
+    for (cudaStream_t s : {c->copy_stream, c->aux_stream}) {
+        if (!s) continue;
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
+    for (auto& e : c->xfer_ev) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -778,6 +787,63 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, in
     return JFDK_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Slabs the host path backprojects and downloads one after another.
+constexpr int kHostSlabs = 8;
+
+jfdk_status ensure_overlap(jfdk_ctx* c, size_t events) {
+    if (!c->copy_stream)
+        JFDK_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking), "creating the copy stream");
+    if (!c->aux_stream)
+        JFDK_CUDA(c, cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking), "creating a compute stream");
+    while (c->xfer_ev.size() < events) {
+        cudaEvent_t e = nullptr;
+        JFDK_CUDA(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "creating an event");
+        c->xfer_ev.push_back(e);
+    }
+    return JFDK_OK;
+}
+
+// Uploads the frames chunk k of the filter stage reads that are not on the
+// device yet (its views and, when compositing, their conjugates), as
+// contiguous runs, on the copy stream.
+jfdk_status upload_chunk(jfdk_ctx* c, const uint16_t* h_raw, int v0, int nv, std::vector<char>& up) {
+    const int N = c->nviews;
+    const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;
+    std::vector<int> need;
+    for (int v = v0; v < v0 + nv; ++v) {
+        need.push_back(v);
+        if (compositing(c)) need.push_back((v + N / 2) % N);
+    }
+    std::sort(need.begin(), need.end());
+    for (size_t i = 0; i < need.size();) {
+        if (up[need[i]]) { ++i; continue; }
+        size_t j = i;
+        while (j + 1 < need.size() && need[j + 1] == need[j] + 1 && !up[need[j + 1]]) ++j;
+        const int a = need[i], n = need[j] - need[i] + 1;
+        JFDK_CUDA(c, cudaMemcpyAsync(c->d_raw_stage + (size_t)a * frame, h_raw + (size_t)a * frame,
+                                     (size_t)n * frame * sizeof(uint16_t), cudaMemcpyHostToDevice, c->copy_stream),
+                  "raw upload");
+        for (int v = a; v < a + n; ++v) up[v] = 1;
+        i = j + 1;
+    }
+    return JFDK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Host buffers in and out, with the transfers overlapped: the frames go up
+// chunk by chunk on a copy stream, each chunk of the filter stage waiting
+// only for its own frames; the backprojection runs as slabs of slices on
+// two compute streams (no launch tail between slabs), and each slab goes
+// down as soon as it is done.  The results equal jfdk_reconstruct's bit for
+// bit: the slabs start at multiples of the tile depth, so every thread
+// covers the slices it covers in one launch.
 jfdk_status jfdk_reconstruct_host(jfdk_ctx* c, const uint16_t* h_raw, float* h_hu) {
     if (!c || !h_raw || !h_hu) return fail(c, JFDK_ERR_INVALID, "reconstruct_host: bad argument");
     const size_t raw_bytes = (size_t)c->nviews * c->scan.num_dets_u * c->scan.num_dets_v * sizeof(uint16_t);
@@ -795,9 +861,58 @@ jfdk_status jfdk_reconstruct_host(jfdk_ctx* c, const uint16_t* h_raw, float* h_h
         if ((st = dev_alloc(c, &c->d_hu_stage, hu_bytes / sizeof(float), "the output volume"))) return st;
         c->hu_stage_bytes = hu_bytes;
     }
-    JFDK_CUDA(c, cudaMemcpyAsync(c->d_raw_stage, h_raw, raw_bytes, cudaMemcpyHostToDevice, c->stream), "raw upload");
-    if ((st = jfdk_reconstruct(c, c->d_raw_stage, c->d_hu_stage, nullptr))) return st;
-    JFDK_CUDA(c, cudaMemcpyAsync(h_hu, c->d_hu_stage, hu_bytes, cudaMemcpyDeviceToHost, c->stream), "volume download");
+    const int chunk = std::min(c->opt_view_chunk, c->nviews);
+    const int nchunks = (c->nviews + chunk - 1) / chunk;
+    const int zpt = bp_zpt(c);
+    const int slab = (int)round_up((c->Z + kHostSlabs - 1) / kHostSlabs, zpt);
+    const int nslabs = (c->Z + slab - 1) / slab;
+    if ((st = ensure_overlap(c, (size_t)nchunks + nslabs + 3))) return st;
+    cudaEvent_t* ev = c->xfer_ev.data();   // [chunks][slabs] start, filtered, copies done
+    cudaEvent_t ev_start = ev[nchunks + nslabs], ev_filtered = ev[nchunks + nslabs + 1],
+                ev_done = ev[nchunks + nslabs + 2];
+    // on any failure below, wait for what is queued before returning: the
+    // copies still reference the caller's host buffers
+    auto drain = [c](jfdk_status s) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamSynchronize(c->aux_stream);
+        cudaStreamSynchronize(c->stream);
+        return s;
+    };
+    const bool timing = c->opt_stage_timing != 0;
+    if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[0], c->stream), "event");
+    // the transfers start after the work already queued on the context's stream
+    JFDK_CUDA(c, cudaEventRecord(ev_start, c->stream), "event");
+    JFDK_CUDA(c, cudaStreamWaitEvent(c->copy_stream, ev_start, 0), "event");
+    std::vector<char> up((size_t)c->nviews, 0);
+    for (int k = 0; k < nchunks; ++k) {
+        const int v0 = k * chunk;
+        if ((st = upload_chunk(c, h_raw, v0, std::min(chunk, c->nviews - v0), up))) return drain(st);
+        JFDK_CUDA(c, cudaEventRecord(ev[k], c->copy_stream), "event");
+    }
+    if ((st = jfdk::reconstruct_filter_stage(c, c->d_raw_stage, c->nviews, ev))) return drain(st);
+    if (timing) {
+        JFDK_CUDA(c, cudaEventRecord(c->ev[1], c->stream), "event");
+        JFDK_CUDA(c, cudaEventRecord(c->ev[2], c->stream), "event");
+    }
+    JFDK_CUDA(c, cudaEventRecord(ev_filtered, c->stream), "event");
+    JFDK_CUDA(c, cudaStreamWaitEvent(c->aux_stream, ev_filtered, 0), "event");
+    const size_t plane = (size_t)c->X * c->Y;
+    for (int sl = 0; sl < nslabs; ++sl) {
+        const int z0 = sl * slab, z1 = std::min(c->Z, z0 + slab);
+        cudaStream_t s = (sl & 1) ? c->aux_stream : c->stream;
+        BPParams b = jfdk::reconstruct_bp_params(c, c->d_hu_stage, nullptr);
+        b.z_begin = z0;
+        b.z_end = z1;
+        if ((st = run_bp_on(c, b, true, s))) return drain(st);
+        JFDK_CUDA(c, cudaEventRecord(ev[nchunks + sl], s), "event");
+        JFDK_CUDA(c, cudaStreamWaitEvent(c->copy_stream, ev[nchunks + sl], 0), "event");
+        JFDK_CUDA(c, cudaMemcpyAsync(h_hu + z0 * plane, c->d_hu_stage + z0 * plane, (size_t)(z1 - z0) * plane * 4,
+                                     cudaMemcpyDeviceToHost, c->copy_stream),
+                  "volume download");
+    }
+    JFDK_CUDA(c, cudaEventRecord(ev_done, c->copy_stream), "event");
+    JFDK_CUDA(c, cudaStreamWaitEvent(c->stream, ev_done, 0), "event");
+    if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[3], c->stream), "event");
     JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "reconstruct_host");
     return JFDK_OK;
 }

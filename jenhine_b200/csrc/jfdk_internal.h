@@ -287,6 +287,10 @@ struct jfdk_ctx {
     int opt_bp_zpt = 0;          // 0: default (bp_zpt() in jfdk_api.cpp)
     int opt_ramp = 0;            // JFDK_OPT_RAMP_PRODUCT (0: the form's default)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // jfdk_reconstruct_host: a copy stream and a second compute stream, and
+    // their events (created on first use)
+    cudaStream_t copy_stream = nullptr, aux_stream = nullptr;
+    std::vector<cudaEvent_t> xfer_ev;
 
     long long launches = 0;
     // device memory held (dev_alloc / dev_free) and the JFDK_OPT_DEVICE_MEMORY_LIMIT
@@ -298,7 +302,10 @@ struct jfdk_ctx {
 namespace jfdk {
 // Stages of jfdk_reconstruct, shared with the batch (batch.cpp).
 // nviews: the first views only (the autotuner), or all when out of range.
-jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nviews);
+// chunk_ready (optional): one event per chunk of views; the stage waits for
+// chunk k's event before its first kernel (frames still in transfer).
+jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nviews,
+                                     const cudaEvent_t* chunk_ready = nullptr);
 BPParams reconstruct_bp_params(const jfdk_ctx* c, float* d_hu, int16_t* d_hu16);
 int bp_slices_per_thread(const jfdk_ctx* c);
 bool mixed_form(const jfdk_ctx* c);

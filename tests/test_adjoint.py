@@ -113,7 +113,9 @@ def test_derivatives_after_reconstruct(torch_cuda):
     vols = [bp_forward(e, q)[0] for e in (fresh, used)]
     assert torch.equal(torch.nan_to_num(vols[0]), torch.nan_to_num(vols[1]))
     vb = torch.rand(vols[0].shape, generator=gen, device="cuda")
-    assert torch.equal(torch.nan_to_num(fresh.bp_adjoint(vb, 0, nv)), torch.nan_to_num(used.bp_adjoint(vb, 0, nv)))
+    # the adjoint scatters with float atomics: equal up to the order of additions
+    a, b = fresh.bp_adjoint(vb, 0, nv), used.bp_adjoint(vb, 0, nv)
+    assert ((a - b).norm() / a.norm()).item() <= 1e-6
 
 
 def test_fdk_adjoint_dot_product(torch_cuda):

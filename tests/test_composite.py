@@ -55,6 +55,17 @@ def test_reconstruct_with_compositing(torch_cuda, comp_case, exact):
     assert np.max(np.abs(hu - g["hu"])) < 0.5
 
 
+def test_reconstruct_host_with_compositing(torch_cuda, comp_case):
+    """The host path uploads each chunk's views and their conjugates before
+    the chunk's compositing pass: the same volume as the device path."""
+    from jenhine_b200 import _lib
+    g = comp_case
+    e = engine_for(g)
+    e.set_option(_lib.OPT_VIEW_CHUNK, 5)
+    hu = e.reconstruct(to_dev(torch_cuda, g["raw"])).cpu().numpy()
+    np.testing.assert_array_equal(e.reconstruct_host(g["raw"]), hu)
+
+
 def test_reconstruct_with_compositing_mixed(torch_cuda, comp_case):
     g = comp_case
     hu = engine_for(g, precision="mixed").reconstruct(to_dev(torch_cuda, g["raw"])).cpu().numpy()

@@ -129,6 +129,22 @@ def test_reconstruct_end_to_end(torch_cuda, case, exact):
     np.testing.assert_array_equal(hu_host, hu)
 
 
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_reconstruct_host_overlapped_equals_device(torch_cuda, case, precision):
+    """jfdk_reconstruct_host uploads chunk by chunk and backprojects and
+    downloads slab by slab on two compute streams: the same volume as
+    jfdk_reconstruct, bit for bit, in both forms and for several chunk and
+    tile choices."""
+    from jenhine_b200 import _lib
+    e = engine_for(case, precision=precision)
+    raw = to_dev(torch_cuda, case["raw"])
+    for chunk, zpt in ((32, 8), (7, 4), (16, 8)):
+        e.set_option(_lib.OPT_VIEW_CHUNK, chunk)
+        e.set_option(_lib.OPT_BP_ZPT, zpt)
+        hu = e.reconstruct(raw).cpu().numpy()
+        np.testing.assert_array_equal(e.reconstruct_host(case["raw"]), hu)
+
+
 def test_reconstruct_int16_output(torch_cuda, case, oracle):
     e = engine_for(case)
     import torch
