@@ -54,6 +54,27 @@ def test_recon_parts_retry_cpu(tmp_path):
     assert "OK (0 failures)" in r.stdout
 
 
+def test_cmake_build_cpu(tmp_path):
+    """The CMake build (CMakeLists.txt) compiles libjfdk.so for sm_100a and the
+    C++ test programs; the CPU ones run."""
+    import shutil
+    cmake = shutil.which("cmake")
+    if cmake is None or shutil.which("ninja") is None:
+        pytest.skip("cmake / ninja not installed")
+    b = str(tmp_path / "build")
+    r = subprocess.run([cmake, "-S", ROOT, "-B", b, "-G", "Ninja", "-DCMAKE_CUDA_COMPILER=/usr/local/cuda/bin/nvcc"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    r = subprocess.run([cmake, "--build", b, "-j", "16"], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    assert os.path.exists(os.path.join(b, "libjfdk.so"))
+    for t in ("test_pipeline", "test_recon_parts"):
+        r = subprocess.run([os.path.join(b, t)], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0 and "OK (0 failures)" in r.stdout, r.stdout + r.stderr
+    r = subprocess.run([os.path.join(b, "test_io"), str(tmp_path / "io")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "OK (0 failures)" in r.stdout, r.stdout + r.stderr
+
+
 def _write_case(path, g):
     raw = g["raw"]
     V, H, U = raw.shape
