@@ -399,6 +399,80 @@ def run_batch(a, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_grad(a, rank, world, local):
+    """--workload grad: the differentiation case (c3: 256^3 at 0.4 mm from 360
+    views of 512^2).  One step = the loss ||FDK(p; theta) - V_target||^2 and
+    its gradient with respect to the preprocessed projections p and the 6
+    rigid parameters per view theta: forward filter + backprojection under
+    the moved geometry, then per chunk of views the adjoint backprojection,
+    the adjoint filter and the geometry gradient (jenhine_b200.autograd).
+    value = voxel-view updates of the three backprojection-sized passes
+    (forward, adjoint, gradient) per second."""
+    import numpy as np
+    import torch
+    from jenhine_b200.autograd import FDKFunction
+    from jenhine_b200.fdk import FDKEngine
+    from jenhine_b200.motion import seeded_motion
+    from jenhine_b200.workloads import c3
+    if a.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no derivatives "
+                                                                  "(no adjoint backprojector, filter or geometry "
+                                                                  "gradient)"}), flush=True)
+        return
+    torch.cuda.set_device(local)
+    w = c3()
+    w.geom.seed += 1000 * rank
+    P0 = np.asarray(w.geom.ptms(), np.float32)
+    eng = FDKEngine(w.scan, w.recon, P0)
+    p = eng.preprocess(w.raw_torch()).contiguous()
+    nv = p.shape[0]
+    target = FDKFunction.apply(p, torch.zeros((nv, 6), dtype=torch.float64), eng, P0).detach().clone()
+    seen = torch.isfinite(target)
+    target = torch.nan_to_num(target)
+    theta = torch.from_numpy(seeded_motion(nv, 303)).requires_grad_()
+    pp = p.clone().requires_grad_()
+
+    def step():
+        vol = FDKFunction.apply(pp, theta, eng, P0)
+        loss = torch.where(seen & torch.isfinite(vol), vol - target, 0.0).square().sum()
+        pp.grad = None
+        theta.grad = None
+        loss.backward()
+        return loss
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.5)
+    l0 = eng.kernel_launches
+    s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(a.steps):
+        loss = step()
+    e0.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = s0.elapsed_time(e0) / a.steps
+    g_theta = theta.grad.detach().cpu().numpy()
+    if rank == 0:
+        upd = 3 * w.updates
+        print(json.dumps({
+            "metric": "gradient of ||FDK(p; theta) - V_target||^2 w.r.t. projections and 6 rigid parameters "
+                      "per view: voxel-view updates/s of forward + adjoint + geometry-gradient passes",
+            "value": upd / (ms / 1000.0) / 1e9, "unit": "GUPS", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": DATA,
+            "config": {"workload": "c3: 256x256x256 at 0.4 mm from 360 views of 512x512, seeded rigid motion "
+                                   "+/-0.5 mm / +/-0.3 deg", "updates_per_pass": w.updates, "passes": 3,
+                       "l2": "inputs larger than L2 (projections 377 MB, quad store 1.5 GB)"},
+            "loss": float(loss.item()), "grad_theta_norm": float(np.linalg.norm(g_theta)),
+            "gpu_launches": eng.kernel_launches - l0, "clocks": clk}), flush=True)
+    eng.close()
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -407,6 +481,9 @@ def main():
     from jenhine_b200.workloads import WORKLOADS
     if a.workload == "batch":
         run_batch(a, rank, world, local)
+        return
+    if a.workload == "grad":
+        run_grad(a, rank, world, local)
         return
     w = WORKLOADS[a.workload]()
     if a.impl == "reference":

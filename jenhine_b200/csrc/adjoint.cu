@@ -73,11 +73,13 @@ __global__ void __launch_bounds__(256) bp_adjoint_kernel(AdjParams p) {
             const float2 uv = bp_uv(xy, bp_w_r<WZ>(xy, rxy, az[k], r2.z), az[k], r0.z, r1.z);
             const bool in = (uv.x >= 0.0f) & (uv.x <= umax) & (uv.y >= 0.0f) & (uv.y <= vmax);
             if (in && rt[k] != 0.0f) {
-                const float fu = floorf(uv.x), fv = floorf(uv.y);
-                const float fx = uv.x - fu, fy = uv.y - fv;
-                const float a = rt[k] * (1.0f - fx), b = rt[k] * fx;
-                red_add_v4(qb + (size_t)fv * p.U + (size_t)fu,
-                           make_float4(a * (1.0f - fy), a * fy, b * (1.0f - fy), b * fy));
+                // floor by the 2^23 add rounded toward -inf (exact for 0 <= u, v < 2^23)
+                const float2 t = padd_rm(uv, f2(kMagic, kMagic));
+                const float2 f = psub(uv, psub(t, f2(kMagic, kMagic)));
+                const unsigned iu = __float_as_uint(t.x) - (unsigned)kMagicBits;
+                const unsigned iv = __float_as_uint(t.y) - (unsigned)kMagicBits;
+                const float a = rt[k] * (1.0f - f.x), b = rt[k] * f.x;
+                red_add_v4(qb + (size_t)iv * p.U + iu, make_float4(a * (1.0f - f.y), a * f.y, b * (1.0f - f.y), b * f.y));
             }
         }
     }
@@ -101,6 +103,16 @@ __global__ void __launch_bounds__(256) unpack_adjoint_kernel(const float4* __res
 }
 
 // Geometry gradient: per (CTA, view) partial sums of the 6 components.
+//
+// For a sample with a_u = rt (dS/du - vol dC/du) / W, a_v = rt dS/dv / W and
+// s = a_u u + a_v v, the contribution to component j is
+// a_u dU_j + a_v dV_j - s dW_j with (dU_j, dV_j, dW_j) = dP_j (x, y, z, 1).
+// That is linear in dP_j, so a thread only sums, over its slices, the six
+// moments a_u, a_u z, a_v, a_v z, s, s z; per view they become the twelve
+// coefficients m of the 3x4 matrix dP_j (m = (x A, y A, A_z, A) for the U
+// row, likewise B for V and -C for W); the CTA sums m over its threads
+// (a transposing butterfly in each warp, then shared memory), and six
+// threads form sum_i dP_j[i] m[i].  dP is read once per CTA and view.
 template <int ZPT, bool WZ>
 __global__ void __launch_bounds__(256) geometry_gradient_kernel(AdjParams p) {
     const int x = blockIdx.x * 32 + threadIdx.x;
@@ -122,60 +134,76 @@ __global__ void __launch_bounds__(256) geometry_gradient_kernel(AdjParams p) {
     const int tid = threadIdx.y * 32 + threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const size_t cta = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
     const size_t ncta = (size_t)gridDim.x * gridDim.y * gridDim.z;
-    __shared__ float red[2][8][6];
+    __shared__ float red[2][8][16];
     const float4* P4 = reinterpret_cast<const float4*>(p.ptm + (size_t)p.v0 * 12);
 #pragma unroll 1
     for (int n = 0; n < p.nv; ++n, P4 += 3) {
-        float g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        float A0 = 0.f, A1 = 0.f, B0 = 0.f, B1 = 0.f, C0 = 0.f, C1 = 0.f;
         if (valid) {
             const float4 r0 = __ldg(P4), r1 = __ldg(P4 + 1), r2 = __ldg(P4 + 2);
             const XYTerms xy = bp_xy_terms(ax, ay, r0, r1, r2);
             const float rxy = WZ ? 0.0f : __frcp_rn(xy.W);
             const float4* __restrict__ q = p.q4 + (size_t)n * p.q_frame;
             const float2* __restrict__ tw = p.tw + (size_t)((p.v0 + n) % p.num_views) * p.U;
-            const float* dP = p.dptm + (size_t)n * 72;
 #pragma unroll
             for (int k = 0; k < ZPT; ++k) {
                 const float2 wr = bp_w_r<WZ>(xy, rxy, az[k], r2.z);
                 const float2 uv = bp_uv(xy, wr, az[k], r0.z, r1.z);
                 const bool in = (uv.x >= 0.0f) & (uv.x <= umax) & (uv.y >= 0.0f) & (uv.y <= vmax);
                 if (in && rt[k] != 0.0f) {
-                    const float fu = floorf(uv.x), fv = floorf(uv.y);
-                    const float fx = uv.x - fu, fy = uv.y - fv;
-                    const int iu = (int)fu, iv = (int)fv;
+                    const float2 t = padd_rm(uv, f2(kMagic, kMagic));          // 2^23 + floor
+                    const float2 f = psub(uv, psub(t, f2(kMagic, kMagic)));
+                    const float fx = f.x, fy = f.y;
+                    const unsigned iu = __float_as_uint(t.x) - (unsigned)kMagicBits;
+                    const unsigned iv = __float_as_uint(t.y) - (unsigned)kMagicBits;
                     const float4 Q = q[(size_t)iv * p.U + iu];
                     const float2 w = tw[iu];
                     const float dSu = (1.0f - fy) * (Q.z - Q.x) + fy * (Q.w - Q.y);
                     const float dSv = (1.0f - fx) * (Q.y - Q.x) + fx * (Q.w - Q.z);
-                    const float iw = 1.0f / wr.x;
+                    const float iw = wr.y;                                 // RN(1 / W)
                     const float au = rt[k] * (dSu - vo[k] * (w.y - w.x)) * iw;
                     const float av = rt[k] * dSv * iw;
-                    const float u0 = uv.x - 0.5f, v0 = uv.y - 0.5f;   // U / W, V / W
-#pragma unroll
-                    for (int j = 0; j < 6; ++j) {
-                        const float* d = dP + j * 12;
-                        const float dU = fmaf(ax, d[0], fmaf(ay, d[1], fmaf(az[k], d[2], d[3])));
-                        const float dV = fmaf(ax, d[4], fmaf(ay, d[5], fmaf(az[k], d[6], d[7])));
-                        const float dW = fmaf(ax, d[8], fmaf(ay, d[9], fmaf(az[k], d[10], d[11])));
-                        g[j] += au * (dU - u0 * dW) + av * (dV - v0 * dW);
-                    }
+                    const float sk = au * (uv.x - 0.5f) + av * (uv.y - 0.5f);   // u = U / W, v = V / W
+                    A0 += au; A1 = fmaf(au, az[k], A1);
+                    B0 += av; B1 = fmaf(av, az[k], B1);
+                    C0 += sk; C1 = fmaf(sk, az[k], C1);
                 }
             }
         }
+        // the coefficients of dP_j's twelve entries (padded to 16)
+        float m[16] = {ax * A0, ay * A0, A1, A0, ax * B0, ay * B0, B1, B0,
+                       -ax * C0, -ay * C0, -C1, -C0, 0.f, 0.f, 0.f, 0.f};
+        // transposing butterfly: after the steps at 16, 8, 4, 2 lanes apart
+        // lane l holds one coefficient, index (l >> 1) & 15, summed over 16
+        // lanes; the step at 1 completes the warp's sum
 #pragma unroll
-        for (int j = 0; j < 6; ++j) {
+        for (int o = 16, h = 8; o >= 2; o >>= 1, h >>= 1) {
+            const bool upper = (lane & o) != 0;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) g[j] += __shfl_xor_sync(0xffffffffu, g[j], o);
+            for (int i = 0; i < h; ++i) {
+                const float send = upper ? m[i] : m[i + h];
+                const float keep = upper ? m[i + h] : m[i];
+                m[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+            }
         }
+        m[0] += __shfl_xor_sync(0xffffffffu, m[0], 1);
         const int buf = n & 1;
-        if (lane == 0)
-#pragma unroll
-            for (int j = 0; j < 6; ++j) red[buf][warp][j] = g[j];
+        if ((lane & 1) == 0) red[buf][warp][lane >> 1] = m[0];
         __syncthreads();
         if (tid < 6) {
-            float s = 0.0f;
-            for (int w = 0; w < 8; ++w) s += red[buf][w][tid];
-            p.partial[((size_t)n * ncta + cta) * 6 + tid] = s;
+            float mc[12];
+#pragma unroll
+            for (int i = 0; i < 12; ++i) {
+                float t = 0.0f;
+#pragma unroll
+                for (int w = 0; w < 8; ++w) t += red[buf][w][i];
+                mc[i] = t;
+            }
+            const float* d = p.dptm + (size_t)n * 72 + tid * 12;
+            float g = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 12; ++i) g = fmaf(__ldg(d + i), mc[i], g);
+            p.partial[((size_t)n * ncta + cta) * 6 + tid] = g;
         }
     }
 }

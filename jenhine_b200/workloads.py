@@ -125,6 +125,18 @@ def c2_slab() -> Workload:
     return w
 
 
+def c2_chunks() -> Workload:
+    """c2's detector, orbit and voxels with 96 views (three 32-view chunks)
+    into a 16-slice slab: the per-chunk kernels (preprocess + pre-weight,
+    ramp product, packing) at c2's sizes with ~1.2 GB on the device, for
+    multi-pass profiling."""
+    w = c2()
+    w.name = "c2_chunks"
+    w.geom.n_views = 96
+    w.recon.num_pixels_z = 16
+    return w
+
+
 def mini_c1() -> Workload:
     return Workload("mini_c1", ScanGeometry(48, 500.0, 800.0, 64, 56, 2.0, 2.0, seed=5),
                     ReconConfig(40, 40, 32, 1.6, 1.6, ct_norm0=1.2, ct_norm1=1.0), 10, 0, 1e5)
@@ -137,4 +149,5 @@ def mini_c2() -> Workload:
                     beam_hardening=(1.0, 0.05, 0.01))
 
 
-WORKLOADS = {"c1": c1, "c2": c2, "c2_slab": c2_slab, "c3": c3, "mini_c1": mini_c1, "mini_c2": mini_c2}
+WORKLOADS = {"c1": c1, "c2": c2, "c2_slab": c2_slab, "c2_chunks": c2_chunks, "c3": c3, "mini_c1": mini_c1,
+             "mini_c2": mini_c2}
