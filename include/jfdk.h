@@ -284,9 +284,17 @@ enum { JFDK_AUTOTUNE_FORCE = 1 };  /* re-time even when the shape is cached */
 jfdk_status jfdk_autotune(jfdk_ctx* ctx, int flags);
 
 /* A batch of scans (one context each, all of the same form) reconstructed
- * together: every scan's filter stage, then ONE persistent backprojection
- * launch over the tiles of all scans (scans in order; a CTA takes the next
- * tile when it finishes one, so scans of uneven size leave no tail).  With
+ * together, on one of two schedules:
+ *  - persistent: every scan's filter stage, then ONE persistent
+ *    backprojection launch over the tiles of up to 8 scans (scans in order;
+ *    a CTA takes the next tile when it finishes one, so scans of uneven size
+ *    leave no tail; consecutive scans of another tile depth or W(z) start a
+ *    new launch);
+ *  - pipelined: each scan's own backprojection launch, the filter stage of
+ *    the next scan running beside it on a second stream.
+ * JFDK_BATCH_AUTOTUNE tunes each context (jfdk_autotune) and, on the first
+ * run, times both schedules and keeps the faster; JFDK_BATCH_PERSISTENT or
+ * JFDK_BATCH_PIPELINED fixes one (default: persistent).  With
  * JFDK_BATCH_GRAPH the first jfdk_batch_run with a set of buffers runs the
  * pipeline directly and records it as a CUDA graph; later runs with the same
  * buffers replay the graph (one launch from the host).  The batch runs on
@@ -294,7 +302,12 @@ jfdk_status jfdk_autotune(jfdk_ctx* ctx, int flags);
  * stream); the contexts' own streams are restored after each run.  Each
  * volume equals the scan's own jfdk_reconstruct bit for bit. */
 typedef struct jfdk_batch jfdk_batch;
-enum { JFDK_BATCH_AUTOTUNE = 1, JFDK_BATCH_GRAPH = 2 };
+enum {
+    JFDK_BATCH_AUTOTUNE = 1,
+    JFDK_BATCH_GRAPH = 2,
+    JFDK_BATCH_PERSISTENT = 4,
+    JFDK_BATCH_PIPELINED = 8
+};
 jfdk_status jfdk_batch_create(jfdk_batch** out, jfdk_ctx* const* ctxs, int n, int flags, void* cuda_stream);
 void jfdk_batch_destroy(jfdk_batch* batch);
 const char* jfdk_batch_last_error(const jfdk_batch* batch);
@@ -304,6 +317,9 @@ jfdk_status jfdk_batch_run(jfdk_batch* batch, const uint16_t* const* d_raw, floa
  * each graph replay (a direct run's filter-stage kernels are counted by the
  * contexts, jfdk_kernel_launches). */
 long long jfdk_batch_launches(const jfdk_batch* batch);
+/* The schedule in use: 0 not chosen yet (before the first run),
+ * JFDK_BATCH_PERSISTENT or JFDK_BATCH_PIPELINED. */
+int jfdk_batch_schedule(const jfdk_batch* batch);
 
 /* ---- introspection (tests, autotuner) ------------------------------------ */
 

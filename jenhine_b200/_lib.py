@@ -30,7 +30,7 @@ OPT_FILTER_SIMT = 5
 OPT_RAMP_PRODUCT = 6
 OPT_DEVICE_MEMORY_LIMIT = 7
 AUTOTUNE_FORCE = 1
-BATCH_AUTOTUNE, BATCH_GRAPH = 1, 2
+BATCH_AUTOTUNE, BATCH_GRAPH, BATCH_PERSISTENT, BATCH_PIPELINED = 1, 2, 4, 8
 RAMP_DEFAULT, RAMP_TF32X3, RAMP_BF16X3, RAMP_FP16X3, RAMP_FP32_SIMT = 0, 1, 2, 3, 4
 
 
@@ -104,6 +104,7 @@ _SIGS = {
     "jfdk_batch_last_error": ([_P], C.c_char_p),
     "jfdk_batch_run": ([_P, _P, _P], C.c_int),
     "jfdk_batch_launches": ([_P], C.c_longlong),
+    "jfdk_batch_schedule": ([_P], C.c_int),
 }
 
 

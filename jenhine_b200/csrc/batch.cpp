@@ -1,6 +1,10 @@
-// batch.cpp -- several scans through one pipeline: every scan's filter stage,
-// then one persistent backprojection launch over the tiles of all scans
-// (bp_batch_kernel), optionally recorded once as a CUDA graph and replayed.
+// batch.cpp -- several scans through one pipeline, on one of two schedules:
+// persistent (every scan's filter stage, then persistent backprojection
+// launches over the tiles of all scans -- bp_batch_kernel, one launch per run
+// of up to 8 consecutive scans that share the tile depth and W's
+// z-dependence) or pipelined (each scan's own backprojection, the next
+// scan's filter stage beside it on a second stream); optionally recorded
+// once as a CUDA graph and replayed.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -19,9 +23,17 @@ struct jfdk_batch {
     int mixed = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    BatchScan* d_scans = nullptr;
-    unsigned* d_counter = nullptr;
-    int ctas = 0;
+    struct Group {                      // one persistent launch
+        BatchSlots slots;
+        int n, zpt, wz, ctas;
+        unsigned total;
+    };
+    std::vector<Group> groups;
+    unsigned* d_counter = nullptr;      // one work cursor per group
+    int schedule = 0;                   // JFDK_BATCH_PERSISTENT / _PIPELINED, 0 not chosen
+    cudaStream_t aux = nullptr;         // the pipelined schedule's filter stream
+    std::vector<cudaEvent_t> ev;        // [scans] filtered, fork, join, two timing events
+    std::vector<float*> hu;             // the outputs of the run being enqueued
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::vector<const uint16_t*> raw;   // the buffers the graph was recorded with
@@ -54,13 +66,14 @@ void drop_graph(jfdk_batch* b) {
 }
 
 // Scan descriptors for the given outputs: each scan's finalizing BP params,
-// its grid of 32 x 8 x ZPT tiles and its first tile in the work list.
-jfdk_status upload_scans(jfdk_batch* b, float* const* d_hu, unsigned* total) {
-    std::vector<BatchScan> h(b->ctx.size());
-    unsigned first = 0;
+// its grid of 32 x kBPTileY x ZPT tiles and its first tile in its group's
+// work list; consecutive scans with the same tile depth and W(z) share a
+// group of up to kBatchSlots.
+jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
+    b->groups.clear();
     for (size_t i = 0; i < b->ctx.size(); ++i) {
         jfdk_ctx* c = b->ctx[i];
-        BatchScan& s = h[i];
+        BatchScan s;
         std::memset(&s, 0, sizeof s);
         s.p = reconstruct_bp_params(c, d_hu[i], nullptr);
         s.zpt = bp_slices_per_thread(c) == 4 ? 4 : 8;
@@ -68,17 +81,26 @@ jfdk_status upload_scans(jfdk_batch* b, float* const* d_hu, unsigned* total) {
         s.gx = (c->X + 31) / 32;
         s.gy = (c->Y + kBPTileY - 1) / kBPTileY;
         s.gz = (c->Z + s.zpt - 1) / s.zpt;
-        s.first_tile = first;
-        first += (unsigned)s.gx * s.gy * s.gz;
+        if (b->groups.empty() || b->groups.back().n == kBatchSlots || b->groups.back().zpt != s.zpt ||
+            b->groups.back().wz != s.wz) {
+            jfdk_batch::Group g;
+            std::memset(&g, 0, sizeof g);
+            g.zpt = s.zpt;
+            g.wz = s.wz;
+            BATCH_CUDA(b, bp_batch_ctas(b->mixed != 0, g.zpt, g.wz != 0, &g.ctas), "occupancy query");
+            b->groups.push_back(g);
+        }
+        jfdk_batch::Group& g = b->groups.back();
+        s.first_tile = g.total;
+        g.total += (unsigned)s.gx * s.gy * s.gz;
+        g.slots.s[g.n++] = s;
     }
-    BATCH_CUDA(b, cudaMemcpy(b->d_scans, h.data(), sizeof(BatchScan) * h.size(), cudaMemcpyHostToDevice),
-               "uploading the scan table");
-    *total = first;
     return JFDK_OK;
 }
 
-// Every scan's filter stage on the batch stream, then the persistent BP.
-jfdk_status enqueue(jfdk_batch* b, const uint16_t* const* d_raw, unsigned total) {
+// Persistent: every scan's filter stage on the batch stream, then the
+// persistent BP launches.
+jfdk_status enqueue_persistent(jfdk_batch* b, const uint16_t* const* d_raw) {
     for (size_t i = 0; i < b->ctx.size(); ++i) {
         jfdk_ctx* c = b->ctx[i];
         cudaStream_t saved = c->stream;
@@ -87,10 +109,67 @@ jfdk_status enqueue(jfdk_batch* b, const uint16_t* const* d_raw, unsigned total)
         c->stream = saved;
         if (st) return berr(b, st, std::string("scan ") + std::to_string(i) + ": " + c->err);
     }
-    BATCH_CUDA(b, launch_bp_batch(b->d_scans, (int)b->ctx.size(), total, b->mixed != 0, b->d_counter, b->ctas,
-                                  b->stream),
-               "batched backprojection");
-    ++b->launches;
+    for (size_t k = 0; k < b->groups.size(); ++k) {
+        const jfdk_batch::Group& g = b->groups[k];
+        BATCH_CUDA(b, launch_bp_batch(g.slots, g.n, g.total, b->mixed != 0, g.zpt, g.wz != 0, b->d_counter + k, g.ctas,
+                                      b->stream),
+                   "batched backprojection");
+        ++b->launches;
+    }
+    return JFDK_OK;
+}
+
+// Pipelined: the filter stages in order on the second stream, each scan's
+// backprojection on the batch stream once its own filter stage is done.
+jfdk_status enqueue_pipelined(jfdk_batch* b, const uint16_t* const* d_raw) {
+    const size_t n = b->ctx.size();
+    cudaEvent_t fork = b->ev[n], join = b->ev[n + 1];
+    BATCH_CUDA(b, cudaEventRecord(fork, b->stream), "event");
+    BATCH_CUDA(b, cudaStreamWaitEvent(b->aux, fork, 0), "event");
+    for (size_t i = 0; i < n; ++i) {
+        jfdk_ctx* c = b->ctx[i];
+        cudaStream_t saved = c->stream;
+        c->stream = b->aux;
+        jfdk_status st = reconstruct_filter_stage(c, d_raw[i], c->nviews);
+        c->stream = saved;
+        if (st) return berr(b, st, std::string("scan ") + std::to_string(i) + ": " + c->err);
+        BATCH_CUDA(b, cudaEventRecord(b->ev[i], b->aux), "event");
+        BATCH_CUDA(b, cudaStreamWaitEvent(b->stream, b->ev[i], 0), "event");
+        if ((st = reconstruct_bp(c, b->hu[i], b->stream)))
+            return berr(b, st, std::string("scan ") + std::to_string(i) + ": " + c->err);
+    }
+    BATCH_CUDA(b, cudaEventRecord(join, b->aux), "event");
+    BATCH_CUDA(b, cudaStreamWaitEvent(b->stream, join, 0), "event");
+    return JFDK_OK;
+}
+
+jfdk_status enqueue(jfdk_batch* b, const uint16_t* const* d_raw) {
+    return b->schedule == JFDK_BATCH_PIPELINED ? enqueue_pipelined(b, d_raw) : enqueue_persistent(b, d_raw);
+}
+
+// The first run: with JFDK_BATCH_AUTOTUNE and no schedule fixed, both
+// schedules run (the outputs are the same) and the faster is kept.
+jfdk_status first_run(jfdk_batch* b, const uint16_t* const* d_raw) {
+    if (b->schedule) return enqueue(b, d_raw);
+    if (!(b->flags & JFDK_BATCH_AUTOTUNE)) {
+        b->schedule = JFDK_BATCH_PERSISTENT;
+        return enqueue(b, d_raw);
+    }
+    const size_t n = b->ctx.size();
+    cudaEvent_t t0 = b->ev[n + 2], t1 = b->ev[n + 3];
+    float ms[2] = {0.0f, 0.0f};
+    const int order[2] = {JFDK_BATCH_PERSISTENT, JFDK_BATCH_PIPELINED};
+    for (int k = 0; k < 2; ++k) {
+        b->schedule = order[k];
+        jfdk_status st = enqueue(b, d_raw);   // the first pass also allocates what the contexts still need
+        if (st) return st;
+        BATCH_CUDA(b, cudaEventRecord(t0, b->stream), "event");
+        if ((st = enqueue(b, d_raw))) return st;
+        BATCH_CUDA(b, cudaEventRecord(t1, b->stream), "event");
+        BATCH_CUDA(b, cudaEventSynchronize(t1), "timing the schedules");
+        BATCH_CUDA(b, cudaEventElapsedTime(&ms[k], t0, t1), "timing the schedules");
+    }
+    b->schedule = ms[0] <= ms[1] ? JFDK_BATCH_PERSISTENT : JFDK_BATCH_PIPELINED;
     return JFDK_OK;
 }
 
@@ -118,9 +197,14 @@ jfdk_status jfdk_batch_create(jfdk_batch** out, jfdk_ctx* const* ctxs, int n, in
         BATCH_CUDA(b, cudaStreamCreate(&b->stream), "creating the batch stream");   // ordered after the legacy stream
         b->own_stream = true;
     }
-    BATCH_CUDA(b, cudaMalloc(&b->d_scans, sizeof(BatchScan) * n), "CUDA failed to malloc the scan table");
-    BATCH_CUDA(b, cudaMalloc(&b->d_counter, sizeof(unsigned)), "CUDA failed to malloc the work counter");
-    BATCH_CUDA(b, bp_batch_ctas(b->mixed != 0, &b->ctas), "occupancy query");
+    BATCH_CUDA(b, cudaMalloc(&b->d_counter, sizeof(unsigned) * n), "CUDA failed to malloc the work counters");
+    if ((flags & JFDK_BATCH_PERSISTENT) && (flags & JFDK_BATCH_PIPELINED))
+        return berr(b, JFDK_ERR_INVALID, "one schedule at most");
+    b->schedule = (flags & JFDK_BATCH_PIPELINED) ? JFDK_BATCH_PIPELINED
+                  : (flags & JFDK_BATCH_PERSISTENT) ? JFDK_BATCH_PERSISTENT : 0;
+    BATCH_CUDA(b, cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking), "creating the filter stream");
+    b->ev.assign((size_t)n + 4, nullptr);
+    for (auto& e : b->ev) BATCH_CUDA(b, cudaEventCreate(&e), "creating an event");
     if (flags & JFDK_BATCH_AUTOTUNE)
         for (jfdk_ctx* c : b->ctx) {
             cudaStream_t saved = c->stream;
@@ -136,8 +220,11 @@ void jfdk_batch_destroy(jfdk_batch* b) {
     if (!b) return;
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graph(b);
-    if (b->d_scans) cudaFree(b->d_scans);
+    if (b->aux) cudaStreamSynchronize(b->aux);
     if (b->d_counter) cudaFree(b->d_counter);
+    for (cudaEvent_t e : b->ev)
+        if (e) cudaEventDestroy(e);
+    if (b->aux) cudaStreamDestroy(b->aux);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }
@@ -145,6 +232,8 @@ void jfdk_batch_destroy(jfdk_batch* b) {
 const char* jfdk_batch_last_error(const jfdk_batch* b) { return b ? b->err.c_str() : "null batch"; }
 
 long long jfdk_batch_launches(const jfdk_batch* b) { return b ? b->launches : 0; }
+
+int jfdk_batch_schedule(const jfdk_batch* b) { return b ? b->schedule : 0; }
 
 jfdk_status jfdk_batch_run(jfdk_batch* b, const uint16_t* const* d_raw, float* const* d_hu) {
     if (!b || !d_raw || !d_hu) return JFDK_ERR_INVALID;
@@ -159,11 +248,12 @@ jfdk_status jfdk_batch_run(jfdk_batch* b, const uint16_t* const* d_raw, float* c
         return JFDK_OK;
     }
     drop_graph(b);
-    unsigned total = 0;
-    jfdk_status st = upload_scans(b, d_hu, &total);
+    jfdk_status st = plan_groups(b, d_hu);
     if (st) return st;
-    // run directly (allocates whatever the contexts still need)
-    if ((st = enqueue(b, d_raw, total))) return st;
+    b->hu.assign(d_hu, d_hu + n);
+    // run directly (allocates whatever the contexts still need; picks the
+    // schedule on the first run)
+    if ((st = first_run(b, d_raw))) return st;
     if (!(b->flags & JFDK_BATCH_GRAPH)) return JFDK_OK;
     // record the same work as a graph for the next runs with these buffers
     BATCH_CUDA(b, cudaStreamSynchronize(b->stream), "batch run");
@@ -171,7 +261,7 @@ jfdk_status jfdk_batch_run(jfdk_batch* b, const uint16_t* const* d_raw, float* c
     for (size_t i = 0; i < n; ++i) counted[i] = b->ctx[i]->launches;
     const long long own = b->launches;
     BATCH_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "graph capture");
-    st = enqueue(b, d_raw, total);
+    st = enqueue(b, d_raw);
     cudaGraph_t g = nullptr;
     const cudaError_t ec = cudaStreamEndCapture(b->stream, &g);
     for (size_t i = 0; i < n; ++i) b->ctx[i]->launches = counted[i];   // recorded, not run

@@ -54,11 +54,56 @@ constexpr int kBPThreads = 32 * kBPTileY;
 // leaves fewer warps idle while the SM waits for the next.
 constexpr int bp_min_blocks(int zpt) { return zpt == 8 ? 1024 / kBPThreads : 1; }
 
-template <int ZPT, bool FINALIZE, bool EXACT, bool WZ>
-__device__ __forceinline__ void bp_block(const BPParams& p, int bx, int by, int bz) {
-    const int x = bx * 32 + threadIdx.x;
-    const int y = by * kBPTileY + threadIdx.y;
-    const int zb = p.z_begin + bz * ZPT;
+// Where a CTA's tile lies: the launch grid's block index for the per-scan
+// kernels, the current work item of the batch kernel.  The tile bodies ask
+// for it at the start and again after the view loop: the batch kernel's
+// tile is re-read from shared memory then rather than held in registers
+// through the loop (at the 64-register bound that made the FP32 body spill).
+struct GridTile {
+    __device__ int bx() const { return blockIdx.x; }
+    __device__ int by() const { return blockIdx.y; }
+    __device__ int bz() const { return blockIdx.z; }
+};
+
+__shared__ unsigned g_batch_tile;   // the batch kernel's current work item
+
+struct BatchTile {
+    const BatchScan& b;
+    __device__ unsigned local() const { return *static_cast<volatile unsigned*>(&g_batch_tile) - b.first_tile; }
+    __device__ int bx() const { return (int)(local() % (unsigned)b.gx); }
+    __device__ int by() const { return (int)((local() / (unsigned)b.gx) % (unsigned)b.gy); }
+    __device__ int bz() const { return (int)(local() / ((unsigned)b.gx * (unsigned)b.gy)); }
+};
+
+// The tile's (sum, weight) pairs: normalised, CT numbers, stored (FINALIZE),
+// or stored as accumulators.  The coordinates are asked for again here.
+template <int ZPT, bool FINALIZE, class Tile>
+__device__ __forceinline__ void epilogue(const BPParams& p, const Tile& tile, const float2 (&acc)[ZPT]) {
+    const int x = tile.bx() * 32 + threadIdx.x;
+    const int y = tile.by() * kBPTileY + threadIdx.y;
+    const int zb = p.z_begin + tile.bz() * ZPT;
+#pragma unroll
+    for (int k = 0; k < ZPT; ++k) {
+        if (zb + k >= p.z_end) break;
+        if (FINALIZE) {
+            const size_t idx = ((size_t)(zb + k) * p.Y + y) * p.X + x;
+            float o = __fdiv_rn(acc[k].x, acc[k].y);   // BPCore::DoneSlice
+            if (p.apply_ct) o = ct_number(o, p.ct_scale, p.ct_norm1);
+            if (p.out) p.out[idx] = o;
+            if (p.out16) p.out16[idx] = to_i16(o);
+        } else {
+            const size_t idx = ((size_t)(zb + k - p.acc_z0) * p.Y + y) * p.X + x;
+            p.sum[idx] = acc[k].x;
+            p.cnt[idx] = acc[k].y;
+        }
+    }
+}
+
+template <int ZPT, bool FINALIZE, bool EXACT, bool WZ, class Tile>
+__device__ __forceinline__ void bp_block(const BPParams& p, const Tile& tile) {
+    const int x = tile.bx() * 32 + threadIdx.x;
+    const int y = tile.by() * kBPTileY + threadIdx.y;
+    const int zb = p.z_begin + tile.bz() * ZPT;
     if (x >= p.X || y >= p.Y) return;
 
     const float ax = bp_axis(x, p.X, p.pxy), ay = bp_axis(y, p.Y, p.pxy);
@@ -118,21 +163,7 @@ __device__ __forceinline__ void bp_block(const BPParams& p, int bx, int by, int 
 
     // The output index is formed here, not before the view loop, so that it
     // holds no registers across the loop.
-#pragma unroll
-    for (int k = 0; k < ZPT; ++k) {
-        if (zb + k >= p.z_end) break;
-        if (FINALIZE) {
-            const size_t idx = ((size_t)(zb + k) * p.Y + y) * p.X + x;
-            float o = __fdiv_rn(acc[k].x, acc[k].y);   // BPCore::DoneSlice
-            if (p.apply_ct) o = ct_number(o, p.ct_scale, p.ct_norm1);
-            if (p.out) p.out[idx] = o;
-            if (p.out16) p.out16[idx] = to_i16(o);
-        } else {
-            const size_t idx = ((size_t)(zb + k - p.acc_z0) * p.Y + y) * p.X + x;
-            p.sum[idx] = acc[k].x;
-            p.cnt[idx] = acc[k].y;
-        }
-    }
+    epilogue<ZPT, FINALIZE>(p, tile, acc);
 }
 
 // ---- mixed precision ---------------------------------------------------------
@@ -161,11 +192,11 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return r;
 }
 
-template <int ZPT, bool FINALIZE, bool WZ>
-__device__ __forceinline__ void bp_mixed_block(const BPParams& p, int bx, int by, int bz) {
-    const int x = bx * 32 + threadIdx.x;
-    const int y = by * kBPTileY + threadIdx.y;
-    const int zb = p.z_begin + bz * ZPT;
+template <int ZPT, bool FINALIZE, bool WZ, class Tile>
+__device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& tile) {
+    const int x = tile.bx() * 32 + threadIdx.x;
+    const int y = tile.by() * kBPTileY + threadIdx.y;
+    const int zb = p.z_begin + tile.bz() * ZPT;
     if (x >= p.X || y >= p.Y) return;
     const float ax = (x - 0.5f * (p.X - 1)) * p.pxy;
     const float ay = (y - 0.5f * (p.Y - 1)) * p.pxy;
@@ -231,77 +262,66 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, int bx, int by
             if (in) acc[k] = pfma(f2(s, 1.0f), f2(val, c), acc[k]);
         }
     }
-#pragma unroll
-    for (int k = 0; k < ZPT; ++k) {
-        if (zb + k >= p.z_end) break;
-        if (FINALIZE) {
-            const size_t idx = ((size_t)(zb + k) * p.Y + y) * p.X + x;
-            float o = __fdiv_rn(acc[k].x, acc[k].y);
-            if (p.apply_ct) o = ct_number(o, p.ct_scale, p.ct_norm1);
-            if (p.out) p.out[idx] = o;
-            if (p.out16) p.out16[idx] = to_i16(o);
-        } else {
-            const size_t idx = ((size_t)(zb + k - p.acc_z0) * p.Y + y) * p.X + x;
-            p.sum[idx] = acc[k].x;
-            p.cnt[idx] = acc[k].y;
-        }
-    }
+    epilogue<ZPT, FINALIZE>(p, tile, acc);
 }
 
 // One CTA = one 32 x 8 x ZPT voxel tile of one launch's grid.
 template <int ZPT, bool FINALIZE, bool EXACT, bool WZ>
 __global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_kernel(BPParams p) {
-    bp_block<ZPT, FINALIZE, EXACT, WZ>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    bp_block<ZPT, FINALIZE, EXACT, WZ>(p, GridTile{});
 }
 
 template <int ZPT, bool FINALIZE, bool WZ>
 __global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_mixed_kernel(BPParams p) {
-    bp_mixed_block<ZPT, FINALIZE, WZ>(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    bp_mixed_block<ZPT, FINALIZE, WZ>(p, GridTile{});
 }
 
-// Persistent backprojection over the tiles of several scans: each CTA takes
-// the next tile of the batch's work list (scans in order, tiles of a scan in
-// the grid order x, y, z) until the list is exhausted, so the tail of one
-// scan runs beside the start of the next.  The scan's parameters are copied
-// to shared memory per tile.
-template <bool MIXED>
-__global__ void __launch_bounds__(kBPThreads, bp_min_blocks(8)) bp_batch_kernel(const BatchScan* __restrict__ scans, int nscans,
-                                                          unsigned* __restrict__ counter, unsigned total) {
-    __shared__ BPParams sp;
-    __shared__ unsigned s_item;
-    __shared__ int s_scan;
+// Persistent backprojection over the tiles of up to kBatchSlots scans: each
+// CTA takes the next tile of the launch's work list (scans in order, tiles
+// of a scan in the grid order x, y, z) until the list is exhausted, so the
+// tail of one scan runs beside the start of the next.  Each scan's
+// parameters sit at a fixed offset of the kernel's parameter space (slot S,
+// a compile-time index), so the tile body reads them as constant operands
+// exactly as the single-scan kernels do; a shared-memory or indexed copy of
+// them measured 16-27 % slower at the 64-register bound.  The next tile's
+// index is fetched while the current one runs.
+template <int S, bool MIXED, int ZPT, bool WZ>
+__device__ __forceinline__ void batch_slot_tile(const BatchSlots& t) {
+    const BatchTile tile{t.s[S]};
+    if (MIXED)
+        bp_mixed_block<ZPT, true, WZ>(t.s[S].p, tile);
+    else
+        bp_block<ZPT, true, false, WZ>(t.s[S].p, tile);
+}
+
+template <bool MIXED, int ZPT, bool WZ>
+__global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT))
+    bp_batch_kernel(const __grid_constant__ BatchSlots t, int nscans, unsigned* __restrict__ counter,
+                    unsigned total) {
+    static_assert(kBatchSlots == 8, "one case per slot below");
+    __shared__ unsigned s_next;
     const int tid = threadIdx.y * 32 + threadIdx.x;
+    if (tid == 0) g_batch_tile = atomicAdd(counter, 1u);
+    __syncthreads();
     for (;;) {
-        if (tid == 0) {
-            const unsigned it = atomicAdd(counter, 1u);
-            int s = 0;
-            while (s + 1 < nscans && it >= scans[s + 1].first_tile) ++s;
-            s_item = it;
-            s_scan = s;
-        }
-        __syncthreads();
-        const unsigned it = s_item;
+        const unsigned it = *static_cast<volatile unsigned*>(&g_batch_tile);
         if (it >= total) break;
-        const BatchScan& b = scans[s_scan];
-        static_assert(sizeof(BPParams) % 4 == 0 && sizeof(BPParams) / 4 <= kBPThreads, "one word per thread");
-        if (tid < (int)(sizeof(BPParams) / 4)) reinterpret_cast<int*>(&sp)[tid] = reinterpret_cast<const int*>(&b.p)[tid];
-        __syncthreads();
-        const unsigned local = it - b.first_tile;
-        const int bx = (int)(local % b.gx), by = (int)((local / b.gx) % b.gy), bz = (int)(local / (b.gx * b.gy));
-        if (MIXED) {
-            if (b.zpt == 4) {
-                if (b.wz) bp_mixed_block<4, true, true>(sp, bx, by, bz); else bp_mixed_block<4, true, false>(sp, bx, by, bz);
-            } else {
-                if (b.wz) bp_mixed_block<8, true, true>(sp, bx, by, bz); else bp_mixed_block<8, true, false>(sp, bx, by, bz);
-            }
-        } else {
-            if (b.zpt == 4) {
-                if (b.wz) bp_block<4, true, false, true>(sp, bx, by, bz); else bp_block<4, true, false, false>(sp, bx, by, bz);
-            } else {
-                if (b.wz) bp_block<8, true, false, true>(sp, bx, by, bz); else bp_block<8, true, false, false>(sp, bx, by, bz);
-            }
+        if (tid == 0) s_next = atomicAdd(counter, 1u);   // the next tile, while this one runs
+        int si = 0;
+        while (si + 1 < nscans && it >= t.s[si + 1].first_tile) ++si;
+        switch (si) {
+            case 0: batch_slot_tile<0, MIXED, ZPT, WZ>(t); break;
+            case 1: batch_slot_tile<1, MIXED, ZPT, WZ>(t); break;
+            case 2: batch_slot_tile<2, MIXED, ZPT, WZ>(t); break;
+            case 3: batch_slot_tile<3, MIXED, ZPT, WZ>(t); break;
+            case 4: batch_slot_tile<4, MIXED, ZPT, WZ>(t); break;
+            case 5: batch_slot_tile<5, MIXED, ZPT, WZ>(t); break;
+            case 6: batch_slot_tile<6, MIXED, ZPT, WZ>(t); break;
+            default: batch_slot_tile<7, MIXED, ZPT, WZ>(t); break;
         }
-        __syncthreads();   // sp and s_item are rewritten for the next tile
+        __syncthreads();   // every thread is done with the current tile
+        if (tid == 0) g_batch_tile = s_next;
+        __syncthreads();
     }
 }
 
@@ -475,24 +495,52 @@ cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_
     return w_depends_on_z ? go_mixed2<false, true>(p, zpt, s) : go_mixed2<false, false>(p, zpt, s);
 }
 
-cudaError_t launch_bp_batch(const BatchScan* d_scans, int nscans, unsigned total_tiles, bool mixed_form,
-                            unsigned* counter, int ctas, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), s);
-    if (e != cudaSuccess) return e;
-    if (mixed_form)
-        bp_batch_kernel<true><<<ctas, dim3(32, kBPTileY), 0, s>>>(d_scans, nscans, counter, total_tiles);
-    else
-        bp_batch_kernel<false><<<ctas, dim3(32, kBPTileY), 0, s>>>(d_scans, nscans, counter, total_tiles);
+namespace {
+
+template <bool M, int Z, bool W>
+cudaError_t batch_go(const BatchSlots& t, int nscans, unsigned total, unsigned* counter, int ctas, cudaStream_t s) {
+    bp_batch_kernel<M, Z, W><<<ctas, dim3(32, kBPTileY), 0, s>>>(t, nscans, counter, total);
     return cudaGetLastError();
 }
 
-cudaError_t bp_batch_ctas(bool mixed_form, int* ctas) {
+template <bool M, int Z, bool W>
+cudaError_t batch_occ(int* per) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, bp_batch_kernel<M, Z, W>, kBPThreads, 0);
+}
+
+}  // namespace
+
+cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tiles, bool mixed_form, int zpt, bool wz,
+                            unsigned* counter, int ctas, cudaStream_t s) {
+    if (nscans < 1 || nscans > kBatchSlots || (zpt != 4 && zpt != 8)) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    const bool z8 = zpt == 8;
+    if (mixed_form) {
+        if (z8) return wz ? batch_go<true, 8, true>(t, nscans, total_tiles, counter, ctas, s)
+                          : batch_go<true, 8, false>(t, nscans, total_tiles, counter, ctas, s);
+        return wz ? batch_go<true, 4, true>(t, nscans, total_tiles, counter, ctas, s)
+                  : batch_go<true, 4, false>(t, nscans, total_tiles, counter, ctas, s);
+    }
+    if (z8) return wz ? batch_go<false, 8, true>(t, nscans, total_tiles, counter, ctas, s)
+                      : batch_go<false, 8, false>(t, nscans, total_tiles, counter, ctas, s);
+    return wz ? batch_go<false, 4, true>(t, nscans, total_tiles, counter, ctas, s)
+              : batch_go<false, 4, false>(t, nscans, total_tiles, counter, ctas, s);
+}
+
+cudaError_t bp_batch_ctas(bool mixed_form, int zpt, bool wz, int* ctas) {
     int dev = 0, sms = 0, per = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess)
-        e = mixed_form ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bp_batch_kernel<true>, kBPThreads, 0)
-                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, bp_batch_kernel<false>, kBPThreads, 0);
+    if (e == cudaSuccess) {
+        const bool z8 = zpt == 8;
+        if (mixed_form)
+            e = z8 ? (wz ? batch_occ<true, 8, true>(&per) : batch_occ<true, 8, false>(&per))
+                   : (wz ? batch_occ<true, 4, true>(&per) : batch_occ<true, 4, false>(&per));
+        else
+            e = z8 ? (wz ? batch_occ<false, 8, true>(&per) : batch_occ<false, 8, false>(&per))
+                   : (wz ? batch_occ<false, 4, true>(&per) : batch_occ<false, 4, false>(&per));
+    }
     *ctas = sms * (per > 0 ? per : 1);
     return e;
 }

@@ -376,6 +376,10 @@ BPParams reconstruct_bp_params(const jfdk_ctx* c, float* d_hu, int16_t* d_hu16) 
     return b;
 }
 
+jfdk_status reconstruct_bp(jfdk_ctx* c, float* d_hu, cudaStream_t s) {
+    return run_bp_on(c, reconstruct_bp_params(c, d_hu, nullptr), true, s);
+}
+
 int bp_slices_per_thread(const jfdk_ctx* c) { return bp_zpt(c); }
 bool mixed_form(const jfdk_ctx* c) { return mixed(c); }
 

@@ -76,12 +76,19 @@ struct BatchScan {
 // Launchers (return cudaError_t of the launch).
 // zpt: slices per thread (4, 8 or 16).
 cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, cudaStream_t s);
+// A batched backprojection launch covers up to kBatchSlots scans that share
+// the tile depth and whether W depends on z; their parameters travel in the
+// kernel's parameter space.
+constexpr int kBatchSlots = 8;
+struct BatchSlots {
+    BatchScan s[kBatchSlots];
+};
 // All tiles of nscans scans in one persistent launch of `ctas` CTAs (the
 // SMs' resident CTAs); *counter is the work-list cursor (cleared here).
-cudaError_t launch_bp_batch(const BatchScan* d_scans, int nscans, unsigned total_tiles, bool mixed_form,
+cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tiles, bool mixed_form, int zpt, bool wz,
                             unsigned* counter, int ctas, cudaStream_t s);
 // CTAs of a full persistent wave: SMs x resident CTAs per SM.
-cudaError_t bp_batch_ctas(bool mixed_form, int* ctas);
+cudaError_t bp_batch_ctas(bool mixed_form, int zpt, bool wz, int* ctas);
 // Mixed-precision form: FP16 footprints with a per-view scale (qh, qscale).
 cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, cudaStream_t s);
 // absmax[f] = bit pattern of max |plain[f][...]| over each of nv frames.
@@ -307,6 +314,8 @@ namespace jfdk {
 jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nviews,
                                      const cudaEvent_t* chunk_ready = nullptr);
 BPParams reconstruct_bp_params(const jfdk_ctx* c, float* d_hu, int16_t* d_hu16);
+// The finalizing backprojection of every view into d_hu, on stream s.
+jfdk_status reconstruct_bp(jfdk_ctx* c, float* d_hu, cudaStream_t s);
 int bp_slices_per_thread(const jfdk_ctx* c);
 bool mixed_form(const jfdk_ctx* c);
 }  // namespace jfdk

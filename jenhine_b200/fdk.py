@@ -306,15 +306,19 @@ class FDKEngine:
 
 
 class FDKBatch:
-    """Scans of uneven size reconstructed together: each scan's filter stage,
-    then one persistent backprojection launch over all scans' tiles, recorded
-    as a CUDA graph on the first run with a set of buffers and replayed after.
+    """Scans of uneven size reconstructed together, recorded as a CUDA graph on
+    the first run with a set of buffers and replayed after.  schedule:
+    "persistent" (each scan's filter stage, then one persistent backprojection
+    launch over the tiles of up to 8 scans), "pipelined" (each scan's own
+    backprojection beside the next scan's filter stage), or None: the faster
+    of the two, timed on the first run when autotune is on (else persistent).
 
         batch = FDKBatch([engine_0, ..., engine_n], autotune=True)
         batch.run([raw_0, ...], [vol_0, ...])   # torch CUDA tensors
     """
 
-    def __init__(self, engines, autotune: bool = True, graph: bool = True, stream=None):
+    def __init__(self, engines, autotune: bool = True, graph: bool = True, stream=None,
+                 schedule: Optional[str] = None):
         import torch
         self.lib = _lib.load()
         self.h = None
@@ -323,6 +327,7 @@ class FDKBatch:
         arr = (C.c_void_p * len(self.engines))(*[e.ctx for e in self.engines])
         h = C.c_void_p()
         flags = (_lib.BATCH_AUTOTUNE if autotune else 0) | (_lib.BATCH_GRAPH if graph else 0)
+        flags |= {None: 0, "persistent": _lib.BATCH_PERSISTENT, "pipelined": _lib.BATCH_PIPELINED}[schedule]
         st = self.lib.jfdk_batch_create(C.byref(h), arr, len(self.engines), flags,
                                         C.c_void_p(self.stream.cuda_stream))
         self.h = h.value
@@ -348,6 +353,12 @@ class FDKBatch:
     @property
     def launches(self) -> int:
         return self.lib.jfdk_batch_launches(self.h)
+
+    @property
+    def schedule(self) -> Optional[str]:
+        """The schedule in use (None before the first run picks one)."""
+        return {0: None, _lib.BATCH_PERSISTENT: "persistent",
+                _lib.BATCH_PIPELINED: "pipelined"}[self.lib.jfdk_batch_schedule(self.h)]
 
     def close(self):
         if getattr(self, "h", None):

@@ -41,13 +41,14 @@ def same(torch, a, b):
     return torch.equal(torch.nan_to_num(a, 1e30), torch.nan_to_num(b, 1e30))
 
 
+@pytest.mark.parametrize("schedule", [None, "persistent", "pipelined"])
 @pytest.mark.parametrize("precision", ["fp32", "mixed"])
-def test_batch_equals_single_reconstructions(torch_cuda, precision):
+def test_batch_equals_single_reconstructions(torch_cuda, precision, schedule):
     torch = torch_cuda
     from jenhine_b200.fdk import FDKBatch
     scans = make_scans(precision)
     untuned = [e.reconstruct(raw).clone() for _, e, raw in scans]
-    batch = FDKBatch([e for _, e, _ in scans], autotune=True, graph=True)
+    batch = FDKBatch([e for _, e, _ in scans], autotune=True, graph=True, schedule=schedule)
     refs = [e.reconstruct(raw).clone() for _, e, raw in scans]   # with the tuned options
     if precision == "fp32":
         assert all(same(torch, u, r) for u, r in zip(untuned, refs))
@@ -56,6 +57,7 @@ def test_batch_equals_single_reconstructions(torch_cuda, precision):
     batch.run(raws, outs)            # direct run, recorded as a graph
     torch.cuda.synchronize()
     assert all(same(torch, o, r) for o, r in zip(outs, refs))
+    assert batch.schedule == (schedule or batch.schedule) and batch.schedule in ("persistent", "pipelined")
     for o in outs:
         o.fill_(-7.0)
     n0 = batch.launches
