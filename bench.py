@@ -54,7 +54,33 @@ def parse():
     ap.add_argument("--zpt", type=int, default=0, help="slices per backprojection thread (0: form default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--split", default="scans", choices=["scans", "zslab"],
+                    help="scans: one independent scan per GPU (weak scaling); zslab: one volume, each GPU "
+                         "filters 1/N of the views and backprojects 1/N of the slices (strong scaling)")
     return ap.parse_args()
+
+
+def init_dist(world, local, backend="nccl"):
+    """The job's process group (None for one process); a short timeout so
+    ranks that wait for one another end with an error."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
+    return dist
+
+
+def max_over_ranks(dist, value: float, device="cuda") -> float:
+    """The largest of every rank's value (the job's time is its slowest rank's)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
 
 
 def workload_config(w):
@@ -196,6 +222,44 @@ def _ref_bp_slab(ref, filt, ptms, r, nz, z0, cores):
     return ref.bp(filt, p, r.num_pixels_x, r.num_pixels_y, nz, r.pitch_xy, r.pitch_z, nthreads=cores)
 
 
+def time_zslab(a, w, raw, ptms, precision, dist, rank, world, local):
+    """One volume over the job's GPUs (jenhine_b200.zslab): per step each rank
+    filters its share of the views, the projection stores are completed by
+    broadcasts over NVLink, and each rank backprojects its slab.  Device-timed,
+    max over ranks; value = one volume's updates per second."""
+    import torch
+    from jenhine_b200.fdk import FDKEngine
+    from jenhine_b200.zslab import reconstruct_zslab, slab_ranges
+    eng = FDKEngine(w.scan, w.recon, ptms, precision=precision, bp_exact=a.exact)
+    r = w.recon
+    z0, nz = slab_ranges(r.num_pixels_z, world)[rank]
+    out = torch.empty((max(nz, 1), r.num_pixels_y, r.num_pixels_x), dtype=torch.float32, device="cuda")
+    for _ in range(a.warmup):
+        reconstruct_zslab(eng, raw, rank, world, out=out[:nz] if nz else None)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.5)
+    l0 = eng.kernel_launches
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(a.steps):
+        reconstruct_zslab(eng, raw, rank, world, out=out[:nz] if nz else None)
+    end.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(dist, start.elapsed_time(end) / a.steps)
+    launches = eng.kernel_launches - l0
+    eng.close()
+    return {"value": w.updates / (ms / 1000.0) / 1e9, "ms_per_step": ms, "s_per_volume": ms / 1000.0,
+            "gpu_launches": launches, "clocks": clk}
+
+
 def run_reference(a, w, rank, world):
     """--impl reference: the reference CPU implementation, rank 0 only."""
     if rank != 0:
@@ -265,10 +329,7 @@ def time_form(a, w, raw, ptms, precision, dist, world, local):
         dist.barrier()
     launches = eng.kernel_launches - launches0
     clk = clocks.stop()
-    ms_t = torch.tensor([start.elapsed_time(end) / a.steps], device="cuda")
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms = ms_t.item()
+    ms = max_over_ranks(dist, start.elapsed_time(end) / a.steps)
     out = {"value": w.updates * world / (ms / 1000.0) / 1e9, "ms_per_step": ms, "s_per_volume": ms / 1000.0,
            "stages_ms": {"preprocess_weight_filter": statistics.mean(s[0] for s in stage_ms),
                          "backprojection_hu": statistics.mean(s[2] for s in stage_ms)},
@@ -292,12 +353,10 @@ def time_form(a, w, raw, ptms, precision, dist, world, local):
         e2.record()
         torch.cuda.synchronize()
         out["gpu_launches"] += eng.kernel_launches - l0
-        ems = torch.tensor([s2.elapsed_time(e2) / a.steps], device="cuda")
-        if dist:
-            dist.all_reduce(ems, op=dist.ReduceOp.MAX)
-        out["e2e"] = {"value": w.updates * world / (ems.item() / 1000.0) / 1e9, "unit": "GUPS",
+        ems = max_over_ranks(dist, s2.elapsed_time(e2) / a.steps)
+        out["e2e"] = {"value": w.updates * world / (ems / 1000.0) / 1e9, "unit": "GUPS",
                       "h2d_bytes_per_step": int(raw.numel() * 2), "d2h_bytes_per_step": int(vol.numel() * 4),
-                      "ms_per_step": ems.item()}
+                      "ms_per_step": ems}
     eng.close()
     return out
 
@@ -331,6 +390,7 @@ def run_batch(a, rank, world, local):
                                                                   "the reference arm runs the c2 workload"}), flush=True)
         return
     torch.cuda.set_device(local)
+    dist = init_dist(world, local)
     scans = batch()
     for w in scans:
         w.geom.seed += 1000 * rank
@@ -348,7 +408,7 @@ def run_batch(a, rank, world, local):
             b.run(raws, outs)
         e1.record()
         torch.cuda.synchronize()
-        return s1.elapsed_time(e1) / a.steps
+        return max_over_ranks(dist, s1.elapsed_time(e1) / a.steps)
 
     for form in forms:
         engines = [FDKEngine(w.scan, w.recon, w.geom.ptms(), precision=form) for w in scans]
@@ -368,7 +428,7 @@ def run_batch(a, rank, world, local):
                 e.reconstruct(r, o)
         e0.record()
         torch.cuda.synchronize()
-        single_ms = s0.elapsed_time(e0) / a.steps
+        single_ms = max_over_ranks(dist, s0.elapsed_time(e0) / a.steps)
         # one batch: direct run + graph recording, then replays
         for _ in range(a.warmup):
             b.run(raws, outs)
@@ -384,7 +444,7 @@ def run_batch(a, rank, world, local):
         e1.record()
         torch.cuda.synchronize()
         clk = clocks.stop()
-        batch_ms = s1.elapsed_time(e1) / a.steps
+        batch_ms = max_over_ranks(dist, s1.elapsed_time(e1) / a.steps)
         chosen = b.schedule
         launched = b.launches - l0
         b.close()
@@ -393,11 +453,12 @@ def run_batch(a, rank, world, local):
         for name in ("persistent", "pipelined"):
             bs = FDKBatch(engines, autotune=False, graph=True, schedule=name)
             ms = time_schedule(bs, outs)
-            sched[name] = {"value": updates / (ms / 1000.0) / 1e9, "ms_per_step": ms}
+            sched[name] = {"value": updates * world / (ms / 1000.0) / 1e9, "ms_per_step": ms}
             bs.close()
-        res[form] = {"value": updates / (batch_ms / 1000.0) / 1e9, "ms_per_step": batch_ms,
+        res[form] = {"value": updates * world / (batch_ms / 1000.0) / 1e9, "ms_per_step": batch_ms,
                      "schedule": chosen, "schedules": sched,
-                     "one_launch_each": {"value": updates / (single_ms / 1000.0) / 1e9, "ms_per_step": single_ms},
+                     "one_launch_each": {"value": updates * world / (single_ms / 1000.0) / 1e9,
+                                         "ms_per_step": single_ms},
                      "speedup_vs_one_launch_each": single_ms / batch_ms,
                      "gpu_launches": launched, "clocks": clk}
         for e in engines:
@@ -421,6 +482,9 @@ def run_batch(a, rank, world, local):
         if len(forms) == 2:
             line["forms"] = res
         print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_grad(a, rank, world, local):
@@ -445,6 +509,7 @@ def run_grad(a, rank, world, local):
                                                                   "gradient)"}), flush=True)
         return
     torch.cuda.set_device(local)
+    dist = init_dist(world, local)
     w = c3()
     w.geom.seed += 1000 * rank
     P0 = np.asarray(w.geom.ptms(), np.float32)
@@ -479,10 +544,10 @@ def run_grad(a, rank, world, local):
     e0.record()
     torch.cuda.synchronize()
     clk = clocks.stop()
-    ms = s0.elapsed_time(e0) / a.steps
+    ms = max_over_ranks(dist, s0.elapsed_time(e0) / a.steps)
     g_theta = theta.grad.detach().cpu().numpy()
     if rank == 0:
-        upd = 3 * w.updates
+        upd = 3 * w.updates * world
         print(json.dumps({
             "metric": "gradient of ||FDK(p; theta) - V_target||^2 w.r.t. projections and 6 rigid parameters "
                       "per view: voxel-view updates/s of forward + adjoint + geometry-gradient passes",
@@ -495,6 +560,9 @@ def run_grad(a, rank, world, local):
             "loss": float(loss.item()), "grad_theta_norm": float(np.linalg.norm(g_theta)),
             "gpu_launches": eng.kernel_launches - l0, "clocks": clk}), flush=True)
     eng.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def main():
@@ -515,19 +583,35 @@ def main():
         return
 
     import torch
-    import datetime
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    dist = init_dist(world, local)
+    forms = ["fp32", "mixed"] if a.precision == "both" else [a.precision]
+    if a.split == "zslab":
+        # one volume shared by all ranks
+        raw = w.raw_torch()
+        ptms = w.geom.ptms()
+        res = {f: time_zslab(a, w, raw, ptms, f, dist, rank, world, local) for f in forms}
+        if rank == 0:
+            head = res[forms[0]]
+            line = {"metric": METRIC, "value": head["value"], "unit": "GUPS", "n_gpus": world,
+                    "steps": a.steps, "warmup": a.warmup, "ms_per_step": head["ms_per_step"],
+                    "s_per_volume": head["s_per_volume"], "higher_is_better": True, "scaling": "strong",
+                    "vs_baseline": None, "dtype": "f32", "data": DATA,
+                    "config": dict(workload_config(w), precision=forms[0],
+                                   parallelism=f"one volume in z-slabs over {world} GPUs"),
+                    "gpu_launches": sum(r["gpu_launches"] for r in res.values()), "clocks": head["clocks"]}
+            if len(forms) == 2:
+                line["forms"] = res
+            print(json.dumps(line), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     # each rank reconstructs its own scan
     w.geom.seed += 1000 * rank
     raw = w.raw_torch()
     ptms = w.geom.ptms()
-    forms = ["fp32", "mixed"] if a.precision == "both" else [a.precision]
     res = {f: time_form(a, w, raw, ptms, f, dist, world, local) for f in forms}
 
     if rank == 0:

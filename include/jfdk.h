@@ -201,6 +201,29 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* ctx, const uint16_t* d_raw, float* d_hu, 
  * copied in, h_hu (Z x Y x X float) copied out; synchronous. */
 jfdk_status jfdk_reconstruct_host(jfdk_ctx* ctx, const uint16_t* h_raw, float* h_hu);
 
+/* ---- one volume over several GPUs: z-slabs ------------------------------- */
+/* The stages of jfdk_reconstruct, split so that GPUs can share a volume: each
+ * filters a part of the views into its context's projection store
+ * (jfdk_filter_to_store), the stores are completed by an all-gather of the
+ * ranges jfdk_store_range names (one NCCL all-gather over NVLink; no
+ * counterpart in the reference), and each GPU backprojects its own slab of
+ * slices from every view (jfdk_backproject_store).  Results equal
+ * jfdk_reconstruct's bit for bit when the slabs start at multiples of the
+ * tile depth (JFDK_OPT_BP_ZPT; 8 by default). */
+/* Filter views [v0, v0+nv) into the store.  d_raw: the rotation's frames
+ * (num_views x NumDetsV x NumDetsU uint16); only the frames of these views
+ * (and, when compositing, of their conjugates) are read. */
+jfdk_status jfdk_filter_to_store(jfdk_ctx* ctx, const uint16_t* d_raw, int v0, int nv);
+/* Device address and size of the store's records of views [v0, v0+nv)
+ * (contiguous, views in order) and, in the mixed form, of their per-view
+ * scales (4 bytes a view; *d_scales = NULL in the FP32 form). */
+jfdk_status jfdk_store_range(jfdk_ctx* ctx, int v0, int nv, void** d_records, size_t* record_bytes,
+                             float** d_scales);
+/* The finalizing backprojection of every view in the store, with CT numbers,
+ * into slices [z0, z0+nz): d_hu / d_hu16 hold those slices only
+ * (nz x Y x X); either may be NULL. */
+jfdk_status jfdk_backproject_store(jfdk_ctx* ctx, int z0, int nz, float* d_hu, int16_t* d_hu16);
+
 /* ---- options --------------------------------------------------------------- */
 enum {
     JFDK_OPT_BP_EXACT = 1,    /* FP32 form.  1: backprojection rounds every

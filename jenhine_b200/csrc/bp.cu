@@ -86,7 +86,7 @@ __device__ __forceinline__ void epilogue(const BPParams& p, const Tile& tile, co
     for (int k = 0; k < ZPT; ++k) {
         if (zb + k >= p.z_end) break;
         if (FINALIZE) {
-            const size_t idx = ((size_t)(zb + k) * p.Y + y) * p.X + x;
+            const size_t idx = ((size_t)(zb + k - p.out_z0) * p.Y + y) * p.X + x;
             float o = __fdiv_rn(acc[k].x, acc[k].y);   // BPCore::DoneSlice
             if (p.apply_ct) o = ct_number(o, p.ct_scale, p.ct_norm1);
             if (p.out) p.out[idx] = o;

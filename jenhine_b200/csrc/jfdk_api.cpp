@@ -325,6 +325,10 @@ namespace jfdk {
 // (L2-sized buffers) -> [z-filter] -> the BP store of the rotation.
 jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nviews, const cudaEvent_t* chunk_ready) {
     if (nviews < 0 || nviews > c->nviews) nviews = c->nviews;
+    return filter_stage_range(c, d_raw, 0, nviews, chunk_ready);
+}
+
+jfdk_status filter_stage_range(jfdk_ctx* c, const uint16_t* d_raw, int vbeg, int vend, const cudaEvent_t* chunk_ready) {
     if (c->in_w != c->used_u && !compositing(c))
         return fail(c, JFDK_ERR_UNSUPPORTED,
                     "reconstruct: filter input width must be the frame width or twice it (compositing)");
@@ -334,9 +338,10 @@ jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nvi
     if ((st = ensure_A(c, (size_t)chunk * c->rows))) return st;
     if ((st = ensure_plain(c, chunk))) return st;
     const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;
-    for (int v0 = 0; v0 < nviews; v0 += chunk) {
-        const int nv = std::min(chunk, nviews - v0);
-        if (chunk_ready) JFDK_CUDA(c, cudaStreamWaitEvent(c->stream, chunk_ready[v0 / chunk], 0), "frame transfer");
+    for (int v0 = vbeg; v0 < vend; v0 += chunk) {
+        const int nv = std::min(chunk, vend - v0);
+        if (chunk_ready)
+            JFDK_CUDA(c, cudaStreamWaitEvent(c->stream, chunk_ready[(v0 - vbeg) / chunk], 0), "frame transfer");
         PrepParams pp = prep_params(c, d_raw + (size_t)v0 * frame);
         if (compositing(c)) {
             pp.width = c->in_w;
@@ -789,6 +794,35 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, in
     if ((st = run_bp(c, jfdk::reconstruct_bp_params(c, d_hu, d_hu16), true))) return st;
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[3], c->stream), "event");
     return JFDK_OK;
+}
+
+jfdk_status jfdk_filter_to_store(jfdk_ctx* c, const uint16_t* d_raw, int v0, int nv) {
+    if (!c || !d_raw || v0 < 0 || nv < 0 || v0 > c->nviews - nv)
+        return fail(c, JFDK_ERR_INVALID, "filter_to_store: bad argument");
+    if (nv == 0) return JFDK_OK;
+    return jfdk::filter_stage_range(c, d_raw, v0, v0 + nv);
+}
+
+jfdk_status jfdk_store_range(jfdk_ctx* c, int v0, int nv, void** d_records, size_t* record_bytes, float** d_scales) {
+    if (!c || !d_records || !record_bytes || !d_scales || v0 < 0 || nv < 0 || v0 > c->nviews - nv)
+        return fail(c, JFDK_ERR_INVALID, "store_range: bad argument");
+    jfdk_status st = ensure_Q4(c, c->nviews);
+    if (st) return st;
+    *d_records = c->d_q4 + (size_t)v0 * frame_px(c);
+    *record_bytes = (size_t)nv * frame_px(c) * sizeof(float4);
+    *d_scales = mixed(c) ? c->d_qscale + v0 : nullptr;
+    return JFDK_OK;
+}
+
+jfdk_status jfdk_backproject_store(jfdk_ctx* c, int z0, int nz, float* d_hu, int16_t* d_hu16) {
+    if (!c || z0 < 0 || nz < 1 || z0 > c->Z - nz || (!d_hu && !d_hu16))
+        return fail(c, JFDK_ERR_INVALID, "backproject_store: bad argument");
+    if (!c->d_q4 || c->q4_views < c->nviews) return fail(c, JFDK_ERR_STATE, "backproject_store: the store is empty");
+    BPParams b = jfdk::reconstruct_bp_params(c, d_hu, d_hu16);
+    b.z_begin = z0;
+    b.z_end = z0 + nz;
+    b.out_z0 = z0;
+    return run_bp(c, b, true);
 }
 
 }  // extern "C"

@@ -55,8 +55,9 @@ struct BPParams {
     float* cnt;
     int acc_z0;
     int load_acc;            // add to sum/cnt already in memory
-    float* out;              // finalize: [Z][Y][X] float or null
-    int16_t* out16;          // finalize: int16 HU or null
+    float* out;              // finalize: [slices][Y][X] float from slice out_z0, or null
+    int16_t* out16;          // finalize: int16 HU, the same layout, or null
+    int out_z0;
     int apply_ct;
     float ct_scale, ct_norm1;
 };
@@ -313,6 +314,9 @@ namespace jfdk {
 // chunk k's event before its first kernel (frames still in transfer).
 jfdk_status reconstruct_filter_stage(jfdk_ctx* c, const uint16_t* d_raw, int nviews,
                                      const cudaEvent_t* chunk_ready = nullptr);
+// The same for views [vbeg, vend) only (d_raw: the rotation's frames).
+jfdk_status filter_stage_range(jfdk_ctx* c, const uint16_t* d_raw, int vbeg, int vend,
+                               const cudaEvent_t* chunk_ready = nullptr);
 BPParams reconstruct_bp_params(const jfdk_ctx* c, float* d_hu, int16_t* d_hu16);
 // The finalizing backprojection of every view into d_hu, on stream s.
 jfdk_status reconstruct_bp(jfdk_ctx* c, float* d_hu, cudaStream_t s);

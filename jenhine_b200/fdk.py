@@ -270,6 +270,29 @@ class FDKEngine:
         return out
 
     # -- derivatives of the FP32 form (torch CUDA tensors) ------------------------
+    # -- one volume over several GPUs (z-slabs; jenhine_b200.zslab) -------------
+    def filter_to_store(self, raw, v0: int, nv: int):
+        """Filter views [v0, v0 + nv) of raw (the rotation's frames, device) into
+        the projection store."""
+        self._check(self.lib.jfdk_filter_to_store(self.ctx, _ptr(raw), int(v0), int(nv)))
+
+    def store_range(self, v0: int, nv: int):
+        """(device address, bytes) of the store's records of views [v0, v0+nv),
+        and (address, bytes) of their scales (mixed form) or None."""
+        rec, nbytes, sc = C.c_void_p(), C.c_size_t(), C.c_void_p()
+        self._check(self.lib.jfdk_store_range(self.ctx, int(v0), int(nv), C.byref(rec), C.byref(nbytes),
+                                              C.byref(sc)))
+        return (rec.value, nbytes.value), ((sc.value, 4 * int(nv)) if sc.value else None)
+
+    def backproject_store(self, z0: int, nz: int, out=None, device="cuda"):
+        """HU of slices [z0, z0 + nz) from every view in the store."""
+        import torch
+        if out is None:
+            out = torch.empty((nz, self.recon.num_pixels_y, self.recon.num_pixels_x), dtype=torch.float32,
+                              device=device)
+        self._check(self.lib.jfdk_backproject_store(self.ctx, int(z0), int(nz), _ptr(out), None))
+        return out
+
     def set_bp_geometry(self, ptms):
         """Projection matrices the backprojector uses from now on (the filter's
         pre-weight and the u-taper keep the creation geometry)."""
