@@ -158,10 +158,11 @@ __global__ void __launch_bounds__(256) geometry_gradient_kernel(AdjParams p) {
                     const unsigned iv = __float_as_uint(t.y) - (unsigned)kMagicBits;
                     const float4 Q = q[(size_t)iv * p.U + iu];
                     const float2 w = tw[iu];
-                    const float dSu = (1.0f - fy) * (Q.z - Q.x) + fy * (Q.w - Q.y);
-                    const float dSv = (1.0f - fx) * (Q.y - Q.x) + fx * (Q.w - Q.z);
+                    // quads: (t00, t10, t01 - t00, t11 - t10); taper pairs (w0, w1 - w0)
+                    const float dSu = (1.0f - fy) * Q.z + fy * Q.w;
+                    const float dSv = (Q.y - Q.x) + fx * (Q.w - Q.z);
                     const float iw = wr.y;                                 // RN(1 / W)
-                    const float au = rt[k] * (dSu - vo[k] * (w.y - w.x)) * iw;
+                    const float au = rt[k] * (dSu - vo[k] * w.y) * iw;
                     const float av = rt[k] * dSv * iw;
                     const float sk = au * (uv.x - 0.5f) + av * (uv.y - 0.5f);   // u = U / W, v = V / W
                     A0 += au; A1 = fmaf(au, az[k], A1);

@@ -16,11 +16,12 @@
 // samples the taper without interpolation, checks only u and clamps v.
 //
 // Data layout.  The filtered, tapered projections are stored as "quads": for
-// every view, row r and column c one float4 (p[r][c], p[r+1][c], p[r][c+1],
-// p[r+1][c+1]) -- the whole bilinear footprint of a sample point in one
-// 16-byte load -- with zeros past the last row and column (pack_quads_kernel
-// writes it).  The taper is stored as pairs (w[c], w[c+1]).  The volume is
-// [z][y][x], x fastest.
+// every view, row r and column c one float4 (p[r][c], p[r+1][c],
+// RN(p[r][c+1] - p[r][c]), RN(p[r+1][c+1] - p[r+1][c])) -- the whole bilinear
+// footprint of a sample point in one 16-byte load, with the column
+// differences BPCore's lerp rounds already formed -- with zeros past the last
+// row and column (pack_quads_kernel writes it).  The taper is stored as pairs
+// (w[c], RN(w[c+1] - w[c])), w[U] = 0.  The volume is [z][y][x], x fastest.
 //
 // Work split.  A CTA is 32 x kBPTileY threads over (x, y); each thread owns ZPT
 // consecutive slices of its (x, y) column and keeps (sum, weight) pairs in
@@ -118,8 +119,7 @@ __device__ __forceinline__ void bp_block(const BPParams& p, const Tile& tile) {
             acc[k] = f2(p.sum[i], p.cnt[i]);
         }
     }
-    const float umax = (float)(p.U - 1), vmax = (float)(p.V - 1);
-    const float2 neg1 = f2(-1.0f, -1.0f);
+    const unsigned umax_bits = __float_as_uint((float)(p.U - 1)), vmax_bits = __float_as_uint((float)(p.V - 1));
 
     // Pointers step from view to view (index arithmetic on v0 and view_base
     // inside the loop measured over 10% slower at the 64-register bound).
@@ -136,7 +136,10 @@ __device__ __forceinline__ void bp_block(const BPParams& p, const Tile& tile) {
             float2 uv = bp_uv(xy, bp_w_r<WZ>(xy, rxy, az[k], r2.z), az[k], r0.z, r1.z);
             // Branch-free so the loads of all ZPT slices can be in flight at
             // once: a point off the detector reads quad (0, 0) and adds nothing.
-            const bool in = (uv.x >= 0.0f) & (uv.x <= umax) & (uv.y >= 0.0f) & (uv.y <= vmax);
+            // 0 <= u <= umax on the bit patterns: non-negative floats order like
+            // their bits, negatives and NaN have larger unsigned patterns (u is
+            // never -0: RN(U / W) + 0.5 rounds an exact zero to +0)
+            const bool in = (__float_as_uint(uv.x) <= umax_bits) & (__float_as_uint(uv.y) <= vmax_bits);
             uv = in ? uv : f2(0.0f, 0.0f);
             const float2 t = padd_rm(uv, f2(kMagic, kMagic));         // 2^23 + floor(uv)
             const float2 fxy = psub(uv, psub(t, f2(kMagic, kMagic)));  // (u - fu, v - fv), exact
@@ -144,18 +147,17 @@ __device__ __forceinline__ void bp_block(const BPParams& p, const Tile& tile) {
             const int idx = (__float_as_int(t.y) - kMagicBits) * p.U + ix;
             const float4 Q = __ldg(q + idx);
             const float2 w = __ldg(tw + ix);
-            const float2 lo = f2(Q.x, Q.y), hi = f2(Q.z, Q.w);       // columns ix, ix + 1
-            const float2 d = pfma(lo, neg1, hi);                      // RN(hi - lo)
+            const float2 lo = f2(Q.x, Q.y), d = f2(Q.z, Q.w);        // column ix, RN(column ix+1 - ix)
             float val, c;
             if (EXACT) {
                 const float t0 = __fadd_rn(lo.x, __fmul_rn(fxy.x, d.x));
                 const float t1 = __fadd_rn(lo.y, __fmul_rn(fxy.x, d.y));
                 val = __fadd_rn(t0, __fmul_rn(fxy.y, __fsub_rn(t1, t0)));
-                c = __fadd_rn(w.x, __fmul_rn(fxy.x, __fsub_rn(w.y, w.x)));
+                c = __fadd_rn(w.x, __fmul_rn(fxy.x, w.y));
             } else {
                 const float2 t = pfma(f2(fxy.x, fxy.x), d, lo);
                 val = fmaf(fxy.y, t.y - t.x, t.x);
-                c = fmaf(fxy.x, w.y - w.x, w.x);
+                c = fmaf(fxy.x, w.y, w.x);
             }
             if (in) acc[k] = padd(acc[k], f2(val, c));
         }
@@ -366,9 +368,10 @@ __global__ void __launch_bounds__(256) pack_mixed_kernel(const float* __restrict
     if (r == 0 && c == 0) scale[view] = s;
     const float* src = plain + (size_t)f * plain_frame + (size_t)r * U + c;
     const bool right = c + 1 < U, down = r + 1 < rows;
-    const float2 w = tw[(size_t)view * U + c];
+    const float2 w = tw[(size_t)view * U + c];                      // (w[c], RN(w[c+1] - w[c]))
+    const float w1 = right ? tw[(size_t)view * U + c + 1].x : 0.0f;
     const float p00 = src[0] * w.x, p10 = down ? src[U] * w.x : 0.0f;
-    const float p01 = right ? src[1] * w.y : 0.0f, p11 = (right && down) ? src[U + 1] * w.y : 0.0f;
+    const float p01 = right ? src[1] * w1 : 0.0f, p11 = (right && down) ? src[U + 1] * w1 : 0.0f;
     // p00 is kept in FP32; each difference is rounded against the already
     // rounded ones, so every corner the form reproduces carries the rounding
     // of one coefficient only: p01 that of dx (a difference, usually far
@@ -377,7 +380,7 @@ __global__ void __launch_bounds__(256) pack_mixed_kernel(const float* __restrict
     const __half hdx = __float2half_rn(b - a), hdy = __float2half_rn(cc - a);
     const __half hdxy = __float2half_rn(d - (a + __half2float(hdx) + __half2float(hdy)));
     const __half2 d1 = __halves2half2(hdx, hdxy);
-    const __half2 d2 = __halves2half2(hdy, __float2half_rn(w.y - w.x));
+    const __half2 d2 = __halves2half2(hdy, __float2half_rn(w.y));
     uint4 rec;
     rec.x = __float_as_uint(a);
     rec.y = *reinterpret_cast<const unsigned*>(&d1);
@@ -387,8 +390,9 @@ __global__ void __launch_bounds__(256) pack_mixed_kernel(const float* __restrict
 }
 
 // Filtered frames -> tapered quads.  One thread per (row, column) of a frame:
-// (w[c] p[r][c], w[c] p[r+1][c], w[c+1] p[r][c+1], w[c+1] p[r+1][c+1]), the
-// products rounded as InitView's in-place multiply (BPCore.cpp:147-151).
+// the tapered values w[c] p[r][c], w[c] p[r+1][c], w[c+1] p[r][c+1],
+// w[c+1] p[r+1][c+1], each product rounded as InitView's in-place multiply
+// (BPCore.cpp:147-151), stored as (t00, t10, RN(t01 - t00), RN(t11 - t10)).
 __global__ void __launch_bounds__(256) pack_quads_kernel(const float* __restrict__ plain, long long plain_frame,
                                                          int rows, int U, const float2* __restrict__ tw,
                                                          int view0, int num_views, int apply_taper,
@@ -401,11 +405,13 @@ __global__ void __launch_bounds__(256) pack_quads_kernel(const float* __restrict
     float p00 = s[0], p01 = right ? s[1] : 0.0f;
     float p10 = down ? s[U] : 0.0f, p11 = (right && down) ? s[U + 1] : 0.0f;
     if (apply_taper) {
-        const float2 w = tw[(size_t)((view0 + f) % num_views) * U + c];
-        p00 = __fmul_rn(p00, w.x); p10 = __fmul_rn(p10, w.x);
-        p01 = __fmul_rn(p01, w.y); p11 = __fmul_rn(p11, w.y);
+        const float2* wv = tw + (size_t)((view0 + f) % num_views) * U;
+        const float w0 = wv[c].x, w1 = right ? wv[c + 1].x : 0.0f;
+        p00 = __fmul_rn(p00, w0); p10 = __fmul_rn(p10, w0);
+        p01 = __fmul_rn(p01, w1); p11 = __fmul_rn(p11, w1);
     }
-    q4[(size_t)(slot0 + f) * q4_frame + (size_t)r * U + c] = make_float4(p00, p10, p01, p11);
+    q4[(size_t)(slot0 + f) * q4_frame + (size_t)r * U + c] =
+        make_float4(p00, p10, __fsub_rn(p01, p00), __fsub_rn(p11, p10));
 }
 
 __global__ void finalize_kernel(const float* __restrict__ sum, const float* __restrict__ cnt, size_t n,

@@ -532,7 +532,7 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     for (int v = 0; v < c->nviews; ++v)
         for (int i = 0; i < c->out_w; ++i) {
             const float* w = &c->ops.uw[(size_t)v * c->out_w];
-            twp[(size_t)v * c->out_w + i] = make_float2(w[i], i + 1 < c->out_w ? w[i + 1] : 0.0f);
+            twp[(size_t)v * c->out_w + i] = make_float2(w[i], (i + 1 < c->out_w ? w[i + 1] : 0.0f) - w[i]);
         }
     std::vector<float> Tp((size_t)c->out_w * a_pitch(c), 0.0f);
     for (int j = 0; j < c->out_w; ++j)

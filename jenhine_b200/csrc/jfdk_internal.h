@@ -39,8 +39,8 @@ constexpr int kBPTileY = 4;
 
 // Parameters of the backprojection kernel (bp.cu).
 struct BPParams {
-    const float4* q4;        // quads, [slots][rows][U]: (p[r][c], p[r+1][c], p[r][c+1], p[r+1][c+1])
-    const float2* tw;        // [views][U] taper pairs (w[c], w[c+1]), w[U] = 0
+    const float4* q4;        // quads, [slots][rows][U]: (p[r][c], p[r+1][c], p[r][c+1] - p[r][c], p[r+1][c+1] - p[r+1][c])
+    const float2* tw;        // [views][U] taper pairs (w[c], RN(w[c+1] - w[c])), w[U] = 0
     const uint4* qh;         // mixed precision: records [slots][rows][U] (bp.cu)
     const float* qscale;     // mixed precision: [views] power-of-two scale of each view
     const float* ptm;        // [views][12]
@@ -204,7 +204,7 @@ struct AdjParams {
     float4* qbar;            // adjoint out: quad space [nv][V][U]
     long long q_frame;       // V * U
     const float4* q4;        // gradient: the forward's tapered quads [nv][V][U]
-    const float2* tw;        // [views][U] taper pairs
+    const float2* tw;        // [views][U] taper pairs (w[c], RN(w[c+1] - w[c]))
     const float* vol;        // gradient: the forward volume
     const float* dptm;       // gradient: [nv][6][12] dP / dtheta_j
     float* partial;          // gradient: [nv][ctas][6] scratch
@@ -250,7 +250,7 @@ struct jfdk_ctx {
 
     // device constants
     float* d_ptm = nullptr;
-    float2* d_tw = nullptr;      // [views][out_w] taper pairs
+    float2* d_tw = nullptr;      // [views][out_w] taper pairs (w[c], RN(w[c+1] - w[c]))
     float* d_tinv = nullptr;
     float* d_dmin = nullptr;
     float* d_pw = nullptr;       // [groups][rows][in_w] pre-weights
