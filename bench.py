@@ -151,6 +151,17 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
+def profile_figure(name: str, key: str):
+    """A figure of a committed ncu summary (profiles/<name>.md, line 'key: N')."""
+    try:
+        for line in open(os.path.join(ROOT, "profiles", f"{name}.md")):
+            if line.strip().startswith(key + ":"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
 def profile_traffic(name: str):
     """dram bytes per launch of the dominant kernel from the committed ncu
     summary (profiles/<name>.md, line 'dram_bytes_per_launch: N')."""
@@ -373,7 +384,12 @@ def roofline(w, bp_ms, kernel, prof, proj_bytes=4):
             "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs ({'of measured' if peak_kind == 'measured' else 'of fallback'})",
             "algorithmic_bytes_per_launch": alg, "traffic": profile_traffic(prof),
             "note": "the backprojector is bound by instruction issue and L1 traffic (its footprint reads "
-                    "hit L1/L2), not by HBM: frac shows the distance to the memory floor"}
+                    "hit L1/L2), not by HBM: frac shows the distance to the memory floor",
+            "sm_bound": {"issue_active": profile_figure(prof.replace("_c2", "_c2_slab"), "issue_active"),
+                         "l1_data_pipe_wavefronts": profile_figure(prof.replace("_c2", "_c2_slab"),
+                                                                   "l1_data_pipe_wavefronts"),
+                         "unit": "fraction of peak (ncu, c2 slab)",
+                         "source": f"profiles/{prof.replace('_c2', '_c2_slab')}.md"}}
 
 
 def run_batch(a, rank, world, local):
