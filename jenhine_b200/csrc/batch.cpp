@@ -66,7 +66,7 @@ void drop_graph(jfdk_batch* b) {
 }
 
 // Scan descriptors for the given outputs: each scan's finalizing BP params,
-// its grid of 32 x kBPTileY x ZPT tiles and its first tile in its group's
+// its grid of kBPTileX x kBPTileY x ZPT tiles and its first tile in its group's
 // work list; consecutive scans with the same tile depth and W(z) share a
 // group of up to kBatchSlots.
 jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
@@ -78,7 +78,7 @@ jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
         s.p = reconstruct_bp_params(c, d_hu[i], nullptr);
         s.zpt = bp_slices_per_thread(c) == 4 ? 4 : 8;
         s.wz = c->w_depends_on_z ? 1 : 0;
-        s.gx = (c->X + 31) / 32;
+        s.gx = (c->X + kBPTileX - 1) / kBPTileX;
         s.gy = (c->Y + kBPTileY - 1) / kBPTileY;
         s.gz = (c->Z + s.zpt - 1) / s.zpt;
         if (b->groups.empty() || b->groups.back().n == kBatchSlots || b->groups.back().zpt != s.zpt ||

@@ -33,9 +33,10 @@ std::string build_host_operators(const jfdk_scan_params& scan, const jfdk_recon_
                                  int in_w, int out_w, int rows, int mirror, float hsr,
                                  HostOperators& ops);
 
-// Backprojection CTA: 32 x kBPTileY threads over (x, y), each thread a run of
-// slices in z (4 or 8 per thread).
-constexpr int kBPTileY = 4;
+// Backprojection CTA: kBPTileX x kBPTileY threads over (x, y), each thread a
+// run of slices in z (4 or 8 per thread).
+constexpr int kBPTileX = 4;
+constexpr int kBPTileY = 32;
 
 // Parameters of the backprojection kernel (bp.cu).
 struct BPParams {
