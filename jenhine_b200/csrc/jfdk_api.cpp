@@ -390,9 +390,6 @@ bool mixed_form(const jfdk_ctx* c) { return mixed(c); }
 
 }  // namespace jfdk
 
-namespace {
-}  // namespace
-
 extern "C" {
 
 jfdk_status jfdk_device_check(char* msg, int msg_len) {
