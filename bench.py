@@ -659,7 +659,7 @@ def main():
                                      proj_bytes=2)
             m["speedup_vs_fp32"] = head["ms_per_step"] / m["ms_per_step"]
             line["forms"] = {"fp32": {k: v for k, v in head.items()}, "mixed": m}
-        if not a.no_cpu_baseline and world == 1:
+        if not a.no_cpu_baseline and world == 1 and not w.composite:
             from jenhine_b200.fdk import FDKEngine
             g = w.geom
             nvb = min(60, g.n_views)

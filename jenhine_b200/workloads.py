@@ -40,13 +40,19 @@ class Workload:
     gain_spread: float = 0.05
     offset_max: float = 50.0
     beam_hardening: tuple = (1.0, 0.0, 0.0)
+    composite: bool = False        # offset detector read with conjugate-view compositing
+    detector_on_right: bool = True
 
     @property
     def scan(self) -> ScanConfig:
         g = self.geom
-        return ScanConfig(num_views=g.n_views, dso=g.sid, dsd=g.sdd, num_dets_u=g.det_u,
-                          num_dets_v=g.det_v, detector_pixel_size=g.pixel_u,
-                          bright_field=self.bright_field, beam_hardening=self.beam_hardening)
+        sc = ScanConfig(num_views=g.n_views, dso=g.sid, dsd=g.sdd, num_dets_u=g.det_u,
+                        num_dets_v=g.det_v, detector_pixel_size=g.pixel_u,
+                        bright_field=self.bright_field, beam_hardening=self.beam_hardening)
+        if self.composite:   # the 2W-wide, mirrored filter input the compositing stage builds
+            sc.filter_input_width = 2 * g.det_u
+            sc.detector_on_right = self.detector_on_right
+        return sc
 
     def phantom(self):
         r = self.recon
@@ -137,6 +143,29 @@ def c2_chunks() -> Workload:
     return w
 
 
+def c2_offset() -> Workload:
+    """c2 with an offset detector: the principal point 100 columns from the
+    detector's left edge, read with conjugate-view compositing (2 x 768-wide
+    filter input) and the z-filter, as the reference application's offset
+    scans run (CompositeAgent, FilterAgent, ZFilterAgent)."""
+    w = c2()
+    w.name = "c2_offset"
+    w.geom.offset_u_px = 100.0 - (w.geom.det_u / 2.0 - 1.0)
+    w.composite = True
+    w.recon.z_filter = True
+    return w
+
+
+def c2_offset_chunks() -> Workload:
+    """c2_offset with 96 views into a 16-slice slab (multi-pass profiling of
+    the compositing filter stage at c2's frame size)."""
+    w = c2_offset()
+    w.name = "c2_offset_chunks"
+    w.geom.n_views = 96
+    w.recon.num_pixels_z = 16
+    return w
+
+
 def mini_c1() -> Workload:
     return Workload("mini_c1", ScanGeometry(48, 500.0, 800.0, 64, 56, 2.0, 2.0, seed=5),
                     ReconConfig(40, 40, 32, 1.6, 1.6, ct_norm0=1.2, ct_norm1=1.0), 10, 0, 1e5)
@@ -149,5 +178,5 @@ def mini_c2() -> Workload:
                     beam_hardening=(1.0, 0.05, 0.01))
 
 
-WORKLOADS = {"c1": c1, "c2": c2, "c2_slab": c2_slab, "c2_chunks": c2_chunks, "c3": c3, "mini_c1": mini_c1,
-             "mini_c2": mini_c2}
+WORKLOADS = {"c1": c1, "c2": c2, "c2_slab": c2_slab, "c2_chunks": c2_chunks, "c2_offset": c2_offset,
+             "c2_offset_chunks": c2_offset_chunks, "c3": c3, "mini_c1": mini_c1, "mini_c2": mini_c2}
