@@ -145,7 +145,7 @@ private:
 // slices (the last part may be shorter): shot i of the input pipe is
 // backprojected into part i mod numReconParts only, and that part's slices
 // are written out at its end, the last slice of the volume marking the shot
-// end (BPCUDAAgent/BPCUDAAgent.cpp:88-110, 244-290); the input agent repeats
+// end (BPCUDAAgent/BPCUDAAgent.cpp:84-111, 231-287); the input agent repeats
 // the views once per part.  The accumulators hold one part; GetReady
 // allocates them, so a volume that does not fit fails there with "CUDA failed
 // to malloc ", which the application's retry loop answers with more parts

@@ -13,7 +13,7 @@
  *    message of the last failure is jfdk_last_error(ctx).
  *  - One context per CUDA stream.  A context is not thread-safe: callers
  *    serialise on it (the reference issues all CUDA work of BPCUDAAgent from
- *    its single WorkFlow0 thread, BPCUDAAgent/BPCUDAAgent.cpp:160-187).
+ *    its single WorkFlow0 thread, BPCUDAAgent/BPCUDAAgent.cpp:84-111).
  *  - All work is enqueued on the context's stream; calls return without
  *    synchronising unless stated.  jfdk_sync waits for the stream.
  *  - An out-of-memory failure returns JFDK_ERR_OOM and a message starting with
@@ -162,7 +162,7 @@ jfdk_status jfdk_bp_reset(jfdk_ctx* ctx);
 /* Restrict jfdk_bp_reset, jfdk_bp_accumulate and jfdk_finalize to slices
  * [z_begin, z_begin + z_count) of the volume: one part of a volume
  * reconstructed in numReconParts parts of numSlicesPerRecon slices, all
- * views backprojected once per part (BPCUDAAgent/BPCUDAAgent.cpp:244-290,
+ * views backprojected once per part (BPCUDAAgent/BPCUDAAgent.cpp:231-287,
  * BPCUDACore.cpp:17-38, JEngine/JEngine.cpp:167-175).  The accumulators are
  * sized to z_count slices here, so an out-of-memory failure surfaces at this
  * call (JFDK_ERR_OOM, "CUDA failed to malloc ..."), where JEngine's retry

@@ -438,7 +438,7 @@ void DeviceUploadAgent::WorkFlow0() {
     }
 }
 
-// ---- BPCUDAAgent (BPCUDAAgent/BPCUDAAgent.cpp:88-363) ----------------------------
+// ---- BPCUDAAgent (BPCUDAAgent/BPCUDAAgent.cpp:49-287) ----------------------------
 
 BPCUDAAgent::BPCUDAAgent(const std::vector<ProjectionMatrix>& ptms, size_t numDetectorsU, size_t numDetectorsV,
                          size_t volumeSizeX, size_t volumeSizeY, size_t volumeSizeZ, float pitchXY, float pitchZ,
