@@ -252,7 +252,7 @@ int jo_preweight_source_view(int v, int numViews) {
 }
 
 /* ======================================================================
- * Real FFT with MKL CCS packing (Performance/RealFFT.cpp, RealFFT.h:73-79)
+ * Real FFT with MKL CCS packing (Performance/RealFFT.cpp, Performance/RealFFT.h:11-17)
  * computed in double.
  * ==================================================================== */
 static int is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
