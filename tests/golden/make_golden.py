@@ -42,6 +42,13 @@ CASES = {
                                 pixel_v=2.6, offset_u_px=-13.0, seed=44),
                       vol=(32, 32, 20, 2.5, 2.5), phantom=dict(n=10), i0=1e5, bf=50000.0,
                       bhc=(1.0, 0.0, 0.0), norm=(1.0, 1.0), composite=dict(det_right=True)),
+    # ragged sizes: an odd detector (33 x 17), a view count that is not a
+    # multiple of the 9-view pre-weight group, a volume that fills no BP tile
+    # (13 x 37 x 5 against tiles of 4 x 32 x 8)
+    "mini_odd": dict(geom=dict(n_views=11, sid=500.0, sdd=800.0, det_u=33, det_v=17, pixel_u=2.6,
+                               pixel_v=2.6, flex_shift_px=0.5, flex_tilt_deg=0.2, seed=55),
+                     vol=(13, 37, 5, 1.4, 2.5), phantom=dict(n=8, n_metal=1), i0=5e4, bf=50000.0,
+                     bhc=(1.0, 0.05, 0.01), norm=(1.2, 0.9)),
 }
 
 
