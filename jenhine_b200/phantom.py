@@ -34,6 +34,7 @@ class ScanGeometry:
     flex_tilt_deg: float = 0.0   # seeded per-view in-plane detector tilt, +/- deg
     seed: int = 0
     offset_u_px: float = 0.0     # detector offset: the principal point moves by this many columns
+    gantry_tilt_deg: float = 0.0  # orbit plane tilted about the x axis: W then depends on z (P[10] != 0)
 
     @property
     def half_sample_rate(self) -> float:
@@ -59,6 +60,10 @@ class ScanGeometry:
             ev = -st * eu0 + ct * ev0
             cu = self.det_u / 2.0 - 1.0 + shift[k, 0] + self.offset_u_px
             cv = self.det_v / 2.0 - 1.0 + shift[k, 1]
+            if self.gantry_tilt_deg:
+                g = math.radians(self.gantry_tilt_deg)
+                Rx = np.array([[1.0, 0.0, 0.0], [0.0, math.cos(g), -math.sin(g)], [0.0, math.sin(g), math.cos(g)]])
+                src, n_hat, eu, ev = Rx @ src, Rx @ n_hat, Rx @ eu, Rx @ ev
             out.append((src, n_hat, eu, ev, cu, cv))
         return out
 

@@ -11,6 +11,8 @@ c2  dental-CBCT size, plain FP32: 600 views over 360 deg, 768 x 768 detector
     case; it uses c1's SID 500 mm / SDD 800 mm.
 c3  differentiation: 360 views of 512 x 512 at 0.5 mm -> 256^3 at 0.4 mm
     (the detector pitch is not given for this case; 0.5 mm covers the volume).
+c2_tilt  c2 with the orbit tilted 1 deg (P[10] != 0, as in calibrated
+    projection matrices): the backprojectors' W(z) form.
 batch  16 seeded scans of uneven size for the batched launch (batch()).
 mini_*  reduced versions of c1 / c2 for parity tests.
 
@@ -166,6 +168,16 @@ def c2_offset_chunks() -> Workload:
     return w
 
 
+def c2_tilt() -> Workload:
+    """c2 with the orbit plane tilted 1 deg about x.  Projection matrices
+    from a calibration, like these, have P[10] != 0: W then depends on z and
+    the backprojectors take their W(z) form (a reciprocal per sample)."""
+    w = c2()
+    w.name = "c2_tilt"
+    w.geom.gantry_tilt_deg = 1.0
+    return w
+
+
 def mini_c1() -> Workload:
     return Workload("mini_c1", ScanGeometry(48, 500.0, 800.0, 64, 56, 2.0, 2.0, seed=5),
                     ReconConfig(40, 40, 32, 1.6, 1.6, ct_norm0=1.2, ct_norm1=1.0), 10, 0, 1e5)
@@ -179,4 +191,4 @@ def mini_c2() -> Workload:
 
 
 WORKLOADS = {"c1": c1, "c2": c2, "c2_slab": c2_slab, "c2_chunks": c2_chunks, "c2_offset": c2_offset,
-             "c2_offset_chunks": c2_offset_chunks, "c3": c3, "mini_c1": mini_c1, "mini_c2": mini_c2}
+             "c2_offset_chunks": c2_offset_chunks, "c2_tilt": c2_tilt, "c3": c3, "mini_c1": mini_c1, "mini_c2": mini_c2}

@@ -34,7 +34,7 @@ def load_golden(name):
     return dict(np.load(os.path.join(GOLDEN, f"{name}.npz")))
 
 
-@pytest.fixture(scope="session", params=["mini_c1", "mini_c2", "mini_odd"])
+@pytest.fixture(scope="session", params=["mini_c1", "mini_c2", "mini_odd", "mini_tilt"])
 def golden(request):
     return request.param, load_golden(request.param)
 

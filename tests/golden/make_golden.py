@@ -49,6 +49,12 @@ CASES = {
                                pixel_v=2.6, flex_shift_px=0.5, flex_tilt_deg=0.2, seed=55),
                      vol=(13, 37, 5, 1.4, 2.5), phantom=dict(n=8, n_metal=1), i0=5e4, bf=50000.0,
                      bhc=(1.0, 0.05, 0.01), norm=(1.2, 0.9)),
+    # orbit plane tilted 15 deg about x: the projection matrices' P[10] is
+    # not zero, so W depends on z (the backprojectors' W(z) instantiations)
+    "mini_tilt": dict(geom=dict(n_views=24, sid=500.0, sdd=800.0, det_u=40, det_v=36, pixel_u=2.6,
+                                pixel_v=2.6, flex_shift_px=0.5, gantry_tilt_deg=15.0, seed=66),
+                      vol=(24, 24, 16, 2.5, 2.5), phantom=dict(n=10, n_metal=1), i0=5e4, bf=50000.0,
+                      bhc=(1.0, 0.0, 0.0), norm=(1.0, 1.0)),
 }
 
 

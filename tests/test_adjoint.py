@@ -65,7 +65,7 @@ def check_filter_dot(torch, e, nv, seed):
     return abs(lhs - rhs) / max(abs(lhs), 1e-30)
 
 
-@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_odd"])
+@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_odd", "mini_tilt"])
 def test_bp_adjoint_dot_product(torch_cuda, name):
     g = load_golden(name)
     e = engine_for(g)
@@ -80,7 +80,7 @@ def fp32_product(e):
     return e
 
 
-@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_odd"])
+@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_odd", "mini_tilt"])
 def test_filter_adjoint_dot_product(torch_cuda, name):
     g = load_golden(name)
     e = fp32_product(engine_for(g))
@@ -89,7 +89,7 @@ def test_filter_adjoint_dot_product(torch_cuda, name):
     assert r <= 1e-6
 
 
-@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_odd"])
+@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_odd", "mini_tilt"])
 def test_filter_adjoint_against_tensor_core_forward(torch_cuda, name):
     """The default (TF32x3) forward against the same adjoint: within its
     split's rounding."""

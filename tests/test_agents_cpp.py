@@ -103,7 +103,7 @@ def _write_files(folder, g):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("files", [False, True], ids=["pipes", "files"])
-@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_comp", "mini_odd"])
+@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_comp", "mini_odd", "mini_tilt"])
 def test_agent_chain_gpu(tmp_path, name, files):
     import torch
     if not torch.cuda.is_available():

@@ -41,7 +41,7 @@ def engine_for(g, **kw):
     return FDKEngine(scan, recon, g["ptms"], **kw)
 
 
-@pytest.fixture(scope="module", params=["mini_c1", "mini_c2", "mini_odd"])
+@pytest.fixture(scope="module", params=["mini_c1", "mini_c2", "mini_odd", "mini_tilt"])
 def case(request):
     return load_golden(request.param)
 

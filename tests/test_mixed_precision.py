@@ -36,7 +36,7 @@ def torch_cuda():
     return torch
 
 
-@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_odd"])
+@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_odd", "mini_tilt"])
 def test_mixed_vs_fp64_oracle_mini(torch_cuda, oracle, name):
     g = load_golden(name)
     X, Y, Z = (int(v) for v in g["vol"])

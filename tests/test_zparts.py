@@ -25,7 +25,7 @@ def accumulate(e, filt, chunk=7):
         e.bp_accumulate(filt[v0:v0 + chunk].contiguous(), v0)
 
 
-@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_odd"])
+@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_odd", "mini_tilt"])
 def test_parts_equal_whole_volume(torch_cuda, name):
     torch = torch_cuda
     g = load_golden(name)

@@ -23,7 +23,7 @@ def torch_cuda():
 
 @pytest.mark.parametrize("world", [2, 3])
 @pytest.mark.parametrize("precision", ["fp32", "mixed"])
-@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_comp", "mini_odd"])
+@pytest.mark.parametrize("name", ["mini_c1", "mini_c2", "mini_comp", "mini_odd", "mini_tilt"])
 def test_emulated_ranks_equal_reconstruct(torch_cuda, name, precision, world):
     torch = torch_cuda
     from jenhine_b200.zslab import slab_ranges, view_ranges
