@@ -81,7 +81,7 @@ class ScanGeometry:
         return self.ptms_f64().astype(np.float32)
 
     def rays(self, k: int):
-        """Unit ray directions [V][U][3] and the source of view k (FP64)."""
+        """The source of view k and its unit ray directions [V][U][3] (FP64)."""
         src, n_hat, eu, ev, cu, cv = self.frames()[k]
         a = (np.arange(self.det_u) - 0.5 - cu) * self.pixel_u
         b = (np.arange(self.det_v) - 0.5 - cv) * self.pixel_v

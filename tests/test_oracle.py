@@ -104,6 +104,26 @@ def test_preweight_grouping(oracle):
     assert [oracle.preweight_source_view(v, 40) for v in (0, 8, 9, 17, 35, 36, 39)] == [4, 4, 13, 13, 31, 39, 39]
 
 
+@pytest.mark.parametrize("tilt", [0.0, 15.0])
+def test_synthetic_ptms_match_the_rays(tilt):
+    """The synthetic scans' projection matrices and the rays the phantom is
+    projected along describe one geometry: a point on the ray of pixel
+    (iu, iv) maps to U / W = iu - 0.5, V / W = iv - 0.5 (BPCore then samples
+    at U / W + 0.5), with and without a tilted orbit (P[10] != 0)."""
+    from jenhine_b200.phantom import ScanGeometry
+    g = ScanGeometry(7, 480.0, 760.0, 33, 17, 2.5, 2.5, flex_shift_px=0.5, flex_tilt_deg=0.2,
+                     gantry_tilt_deg=tilt, seed=3)
+    P = g.ptms_f64().reshape(-1, 3, 4)
+    assert (np.count_nonzero(P[:, 2, 2]) > 0) == (tilt != 0.0)
+    rng = np.random.default_rng(4)
+    for k in range(g.n_views):
+        src, d = g.rays(k)
+        for iu, iv, t in zip(rng.integers(0, 33, 5), rng.integers(0, 17, 5), rng.uniform(300, 600, 5)):
+            x = src + t * d[iv, iu]
+            U, V, W = P[k] @ np.append(x, 1.0)
+            assert abs(U / W - (iu - 0.5)) < 1e-9 and abs(V / W - (iv - 0.5)) < 1e-9
+
+
 def test_uweights_centred_detector(oracle):
     from jenhine_b200.phantom import ScanGeometry
     g = ScanGeometry(4, 500.0, 800.0, 64, 32, 2.0, 2.0)
