@@ -20,7 +20,8 @@ import numpy as np
 
 @dataclasses.dataclass
 class ScanGeometry:
-    """Circular cone-beam orbit around the z axis."""
+    """Circular cone-beam orbit around the z axis, or around z tilted about x
+    by gantry_tilt_deg."""
     n_views: int
     sid: float            # source to isocentre (DSO), mm
     sdd: float            # source to detector (DSD), mm
