@@ -241,12 +241,16 @@ enum {
                                  JFDK_OPT_RAMP_PRODUCT = JFDK_RAMP_FP32_SIMT);
                                  0: the form's default                          */
     JFDK_OPT_RAMP_PRODUCT = 6,/* how the ramp product runs, a jfdk_ramp_product */
-    JFDK_OPT_DEVICE_MEMORY_LIMIT = 7 /* bytes of device memory the context may hold
+    JFDK_OPT_DEVICE_MEMORY_LIMIT = 7, /* bytes of device memory the context may hold
                                  in all (0, default: no limit).  An allocation
                                  that would exceed it fails like cudaMalloc:
                                  JFDK_ERR_OOM, "CUDA failed to malloc ...".  Lets
                                  a caller sharing the GPU bound the engine, and
                                  choose the z-parts of jfdk_bp_set_slab ahead  */
+    JFDK_OPT_BP_TILE = 8      /* backprojection CTA width in x: 4 (4 x 32
+                                 threads), 8 (8 x 16) or 32 (32 x 4); 0
+                                 (default): 4.  16-slice tiles are 4 wide.  The
+                                 volume does not depend on it                  */
 };
 /* Ramp products (JFDK_OPT_RAMP_PRODUCT).  The split products run on the
  * tcgen05 tensor cores as hi*hi + hi*lo + lo*hi with FP32 accumulation. */
@@ -296,11 +300,11 @@ jfdk_status jfdk_geometry_gradient(jfdk_ctx* ctx, const float* d_q, int v0, int 
 
 /* ---- autotuner and batches (no counterpart in the reference) -------------- */
 
-/* Pick the backprojection's voxel tile depth (JFDK_OPT_BP_ZPT: 4 or 8 slices
- * per thread, a 32 x 8 x ZPT tile per CTA) and the filter stage's views per
- * chunk (JFDK_OPT_VIEW_CHUNK: 16, 32 or 64) for this context's shape by
- * timing the candidates on the device (a 32-slice slab, the first 128 views
- * of zero frames).  Results are cached per shape in the process and, when
+/* Pick the backprojection's voxel tile (JFDK_OPT_BP_ZPT: 4 or 8 slices per
+ * thread; JFDK_OPT_BP_TILE: 4, 8 or 32 threads wide in x, 128 per CTA) and
+ * the filter stage's views per chunk (JFDK_OPT_VIEW_CHUNK: 16, 32 or 64) for
+ * this context's shape by timing the candidates on the device (a 32-slice
+ * slab, the first 128 views of zero frames).  Results are cached per shape in the process and, when
  * $JFDK_AUTOTUNE_CACHE names a file, appended to it and read back by later
  * processes.  Synchronises the context's stream. */
 enum { JFDK_AUTOTUNE_FORCE = 1 };  /* re-time even when the shape is cached */

@@ -23,7 +23,8 @@
 // row and column (pack_quads_kernel writes it).  The taper is stored as pairs
 // (w[c], RN(w[c+1] - w[c])), w[U] = 0.  The volume is [z][y][x], x fastest.
 //
-// Work split.  A CTA is kBPTileX x kBPTileY threads over (x, y); each thread owns ZPT
+// Work split.  A CTA is 128 threads over (x, y), TX x (128 / TX) (4 x 32 by
+// default, 8 x 16 or 32 x 4 by option or autotuner); each thread owns ZPT
 // consecutive slices of its (x, y) column and keeps (sum, weight) pairs in
 // registers across all views of the launch, so a launch covering every view
 // stores the volume once and never reads it.
@@ -68,8 +69,11 @@ constexpr int bp_min_blocks(int zpt) { return zpt == 8 ? 1024 / kBPThreads : 1; 
 // spills (12 bytes stored, 360 bytes of reloads) and made it 6.5 % faster
 // on a tilted c2 orbit; the FP32 kernels ran 0.8 % faster on c2.  The mixed
 // body with z-independent W measured 1 % slower with it and keeps the plain
-// read (GridTileHeld).
+// read (GridTileHeld).  TX is the tile's width in x (threads along x); the
+// CTA is TX x (128 / TX) threads, each warp 32 consecutive threads of it.
+template <int TX>
 struct GridTile {
+    static constexpr int kX = TX, kY = kBPThreads / TX;
     __device__ static int ctaid(int d) {
         unsigned r;
         if (d == 0) asm volatile("mov.u32 %0, %%ctaid.x;" : "=r"(r));
@@ -82,7 +86,9 @@ struct GridTile {
     __device__ int bz() const { return ctaid(2); }
 };
 
+template <int TX>
 struct GridTileHeld {
+    static constexpr int kX = TX, kY = kBPThreads / TX;
     __device__ int bx() const { return blockIdx.x; }
     __device__ int by() const { return blockIdx.y; }
     __device__ int bz() const { return blockIdx.z; }
@@ -91,6 +97,7 @@ struct GridTileHeld {
 __shared__ unsigned g_batch_tile;   // the batch kernel's current work item
 
 struct BatchTile {
+    static constexpr int kX = kBPTileX, kY = kBPTileY;
     const BatchScan& b;
     __device__ unsigned local() const { return *static_cast<volatile unsigned*>(&g_batch_tile) - b.first_tile; }
     __device__ int bx() const { return (int)(local() % (unsigned)b.gx); }
@@ -102,8 +109,8 @@ struct BatchTile {
 // or stored as accumulators.  The coordinates are asked for again here.
 template <int ZPT, bool FINALIZE, class Tile>
 __device__ __forceinline__ void epilogue(const BPParams& p, const Tile& tile, const float2 (&acc)[ZPT]) {
-    const int x = tile.bx() * kBPTileX + threadIdx.x;
-    const int y = tile.by() * kBPTileY + threadIdx.y;
+    const int x = tile.bx() * Tile::kX + threadIdx.x;
+    const int y = tile.by() * Tile::kY + threadIdx.y;
     const int zb = p.z_begin + tile.bz() * ZPT;
 #pragma unroll
     for (int k = 0; k < ZPT; ++k) {
@@ -124,8 +131,8 @@ __device__ __forceinline__ void epilogue(const BPParams& p, const Tile& tile, co
 
 template <int ZPT, bool FINALIZE, bool EXACT, bool WZ, class Tile>
 __device__ __forceinline__ void bp_block(const BPParams& p, const Tile& tile) {
-    const int x = tile.bx() * kBPTileX + threadIdx.x;
-    const int y = tile.by() * kBPTileY + threadIdx.y;
+    const int x = tile.bx() * Tile::kX + threadIdx.x;
+    const int y = tile.by() * Tile::kY + threadIdx.y;
     const int zb = p.z_begin + tile.bz() * ZPT;
     if (x >= p.X || y >= p.Y) return;
 
@@ -218,8 +225,8 @@ __device__ __forceinline__ float rcp_approx(float x) {
 
 template <int ZPT, bool FINALIZE, bool WZ, class Tile>
 __device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& tile) {
-    const int x = tile.bx() * kBPTileX + threadIdx.x;
-    const int y = tile.by() * kBPTileY + threadIdx.y;
+    const int x = tile.bx() * Tile::kX + threadIdx.x;
+    const int y = tile.by() * Tile::kY + threadIdx.y;
     const int zb = p.z_begin + tile.bz() * ZPT;
     if (x >= p.X || y >= p.Y) return;
     const float ax = (x - 0.5f * (p.X - 1)) * p.pxy;
@@ -296,18 +303,18 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& ti
     epilogue<ZPT, FINALIZE>(p, tile, acc);
 }
 
-// One CTA = one 32 x 8 x ZPT voxel tile of one launch's grid.
-template <int ZPT, bool FINALIZE, bool EXACT, bool WZ>
+// One CTA = one TX x (128 / TX) x ZPT voxel tile of one launch's grid.
+template <int ZPT, bool FINALIZE, bool EXACT, bool WZ, int TX>
 __global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_kernel(BPParams p) {
-    bp_block<ZPT, FINALIZE, EXACT, WZ>(p, GridTile{});
+    bp_block<ZPT, FINALIZE, EXACT, WZ>(p, GridTile<TX>{});
 }
 
-template <int ZPT, bool FINALIZE, bool WZ>
+template <int ZPT, bool FINALIZE, bool WZ, int TX>
 __global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_mixed_kernel(BPParams p) {
     if constexpr (WZ)
-        bp_mixed_block<ZPT, FINALIZE, WZ>(p, GridTile{});
+        bp_mixed_block<ZPT, FINALIZE, WZ>(p, GridTile<TX>{});
     else
-        bp_mixed_block<ZPT, FINALIZE, WZ>(p, GridTileHeld{});
+        bp_mixed_block<ZPT, FINALIZE, WZ>(p, GridTileHeld<TX>{});
 }
 
 // Persistent backprojection over the tiles of up to kBatchSlots scans: each
@@ -494,55 +501,87 @@ __global__ void __launch_bounds__(128) zfilter_kernel(float* frames, int nv, int
     }
 }
 
-template <int ZPT, bool F, bool E, bool WZ>
-cudaError_t go(const BPParams& p, cudaStream_t s) {
+// The launch grid covers the volume's columns with TX x (128 / TX) tiles and
+// the launch's slices with ZPT-deep ones; threads outside the volume return
+// at once, slices past z_end are skipped.
+template <int TX>
+dim3 bp_grid(const BPParams& p, int zpt) {
+    constexpr int TY = kBPThreads / TX;
     const int nz = p.z_end - p.z_begin;
-    dim3 grid((p.X + kBPTileX - 1) / kBPTileX, (p.Y + kBPTileY - 1) / kBPTileY, (nz + ZPT - 1) / ZPT);
-    bp_kernel<ZPT, F, E, WZ><<<grid, dim3(kBPTileX, kBPTileY), 0, s>>>(p);
+    return dim3((p.X + TX - 1) / TX, (p.Y + TY - 1) / TY, (nz + zpt - 1) / zpt);
+}
+
+template <int ZPT, bool F, bool E, bool WZ, int TX>
+cudaError_t go(const BPParams& p, cudaStream_t s) {
+    bp_kernel<ZPT, F, E, WZ, TX><<<bp_grid<TX>(p, ZPT), dim3(TX, kBPThreads / TX), 0, s>>>(p);
     return cudaGetLastError();
+}
+
+// Tile widths 4, 8 and 32 for the tile depths the autotuner chooses between
+// (4 and 8 slices); 16-slice tiles are 4 wide.
+template <int ZPT, bool F, bool E, bool WZ>
+cudaError_t go_tx(const BPParams& p, int tx, cudaStream_t s) {
+    if constexpr (ZPT != 16) {
+        if (tx == 8) return go<ZPT, F, E, WZ, 8>(p, s);
+        if (tx == 32) return go<ZPT, F, E, WZ, 32>(p, s);
+    }
+    return go<ZPT, F, E, WZ, 4>(p, s);
 }
 
 template <int ZPT, bool F, bool E>
-cudaError_t go2(const BPParams& p, bool wz, cudaStream_t s) {
-    return wz ? go<ZPT, F, E, true>(p, s) : go<ZPT, F, E, false>(p, s);
+cudaError_t go2(const BPParams& p, bool wz, int tx, cudaStream_t s) {
+    return wz ? go_tx<ZPT, F, E, true>(p, tx, s) : go_tx<ZPT, F, E, false>(p, tx, s);
 }
 
-template <int ZPT, bool F, bool WZ>
+template <int ZPT, bool F, bool WZ, int TX>
 cudaError_t go_mixed(const BPParams& p, cudaStream_t s) {
-    const int nz = p.z_end - p.z_begin;
-    dim3 grid((p.X + kBPTileX - 1) / kBPTileX, (p.Y + kBPTileY - 1) / kBPTileY, (nz + ZPT - 1) / ZPT);
-    bp_mixed_kernel<ZPT, F, WZ><<<grid, dim3(kBPTileX, kBPTileY), 0, s>>>(p);
+    bp_mixed_kernel<ZPT, F, WZ, TX><<<bp_grid<TX>(p, ZPT), dim3(TX, kBPThreads / TX), 0, s>>>(p);
     return cudaGetLastError();
 }
 
+template <int ZPT, bool F, bool WZ>
+cudaError_t go_mixed_tx(const BPParams& p, int tx, cudaStream_t s) {
+    if constexpr (ZPT != 16) {
+        if (tx == 8) return go_mixed<ZPT, F, WZ, 8>(p, s);
+        if (tx == 32) return go_mixed<ZPT, F, WZ, 32>(p, s);
+    }
+    return go_mixed<ZPT, F, WZ, 4>(p, s);
+}
+
 template <bool F, bool WZ>
-cudaError_t go_mixed2(const BPParams& p, int zpt, cudaStream_t s) {
+cudaError_t go_mixed2(const BPParams& p, int zpt, int tx, cudaStream_t s) {
     switch (zpt) {
-        case 16: return go_mixed<16, F, WZ>(p, s);
-        case 8: return go_mixed<8, F, WZ>(p, s);
-        default: return go_mixed<4, F, WZ>(p, s);
+        case 16: return go_mixed_tx<16, F, WZ>(p, tx, s);
+        case 8: return go_mixed_tx<8, F, WZ>(p, tx, s);
+        default: return go_mixed_tx<4, F, WZ>(p, tx, s);
     }
 }
 
 template <bool F, bool E>
-cudaError_t go3(const BPParams& p, bool wz, int zpt, cudaStream_t s) {
+cudaError_t go3(const BPParams& p, bool wz, int zpt, int tx, cudaStream_t s) {
     switch (zpt) {
-        case 16: return go2<16, F, E>(p, wz, s);
-        case 8: return go2<8, F, E>(p, wz, s);
-        default: return go2<4, F, E>(p, wz, s);
+        case 16: return go2<16, F, E>(p, wz, tx, s);
+        case 8: return go2<8, F, E>(p, wz, tx, s);
+        default: return go2<4, F, E>(p, wz, tx, s);
     }
 }
 
 }  // namespace
 
-cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, cudaStream_t s) {
-    if (finalize) return exact ? go3<true, true>(p, w_depends_on_z, zpt, s) : go3<true, false>(p, w_depends_on_z, zpt, s);
-    return exact ? go3<false, true>(p, w_depends_on_z, zpt, s) : go3<false, false>(p, w_depends_on_z, zpt, s);
+cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, int tile_x,
+                      cudaStream_t s) {
+    if (finalize)
+        return exact ? go3<true, true>(p, w_depends_on_z, zpt, tile_x, s)
+                     : go3<true, false>(p, w_depends_on_z, zpt, tile_x, s);
+    return exact ? go3<false, true>(p, w_depends_on_z, zpt, tile_x, s)
+                 : go3<false, false>(p, w_depends_on_z, zpt, tile_x, s);
 }
 
-cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, cudaStream_t s) {
-    if (finalize) return w_depends_on_z ? go_mixed2<true, true>(p, zpt, s) : go_mixed2<true, false>(p, zpt, s);
-    return w_depends_on_z ? go_mixed2<false, true>(p, zpt, s) : go_mixed2<false, false>(p, zpt, s);
+cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, int tile_x,
+                            cudaStream_t s) {
+    if (finalize)
+        return w_depends_on_z ? go_mixed2<true, true>(p, zpt, tile_x, s) : go_mixed2<true, false>(p, zpt, tile_x, s);
+    return w_depends_on_z ? go_mixed2<false, true>(p, zpt, tile_x, s) : go_mixed2<false, false>(p, zpt, tile_x, s);
 }
 
 namespace {

@@ -248,6 +248,9 @@ BPParams bp_params(const jfdk_ctx* c) {
 // Slices per thread: the option, else 8 (measured fastest in both forms).
 int bp_zpt(const jfdk_ctx* c) { return c->opt_bp_zpt ? c->opt_bp_zpt : 8; }
 
+// CTA width in x: the option, else 4 (4 x 32 threads).
+int bp_tile(const jfdk_ctx* c) { return c->opt_bp_tile ? c->opt_bp_tile : kBPTileX; }
+
 // Filtered frames [nv][rows][out_w] of rotation views view0.. -> the BP store,
 // slots slot0..: tapered FP32 quads, or in the mixed form FP16 records with
 // the views' scales.
@@ -274,10 +277,10 @@ jfdk_status run_bp_on(jfdk_ctx* c, BPParams b, bool finalize, cudaStream_t s) {
     if (mixed(c)) {
         b.qh = reinterpret_cast<const uint4*>(c->d_q4);
         b.qscale = c->d_qscale;
-        JFDK_LAUNCH(c, launch_bp_mixed(b, finalize, c->w_depends_on_z, bp_zpt(c), s), "backprojection");
+        JFDK_LAUNCH(c, launch_bp_mixed(b, finalize, c->w_depends_on_z, bp_zpt(c), bp_tile(c), s), "backprojection");
         return JFDK_OK;
     }
-    JFDK_LAUNCH(c, launch_bp(b, finalize, c->opt_bp_exact != 0, c->w_depends_on_z, bp_zpt(c), s),
+    JFDK_LAUNCH(c, launch_bp(b, finalize, c->opt_bp_exact != 0, c->w_depends_on_z, bp_zpt(c), bp_tile(c), s),
                 "backprojection");
     return JFDK_OK;
 }
@@ -616,6 +619,11 @@ jfdk_status jfdk_set_option(jfdk_ctx* c, int key, long long value) {
             if (value != 0 && value != 4 && value != 8 && value != 16)
                 return fail(c, JFDK_ERR_INVALID, "slices per thread must be 0 (default), 4, 8 or 16");
             c->opt_bp_zpt = (int)value;
+            return JFDK_OK;
+        case JFDK_OPT_BP_TILE:
+            if (value != 0 && value != 4 && value != 8 && value != 32)
+                return fail(c, JFDK_ERR_INVALID, "backprojection tile width must be 0 (default), 4, 8 or 32");
+            c->opt_bp_tile = (int)value;
             return JFDK_OK;
         case JFDK_OPT_FILTER_SIMT: c->opt_ramp = value ? JFDK_RAMP_FP32_SIMT : JFDK_RAMP_DEFAULT; return JFDK_OK;
         case JFDK_OPT_RAMP_PRODUCT:
@@ -1085,7 +1093,10 @@ jfdk_status jfdk_geometry_gradient(jfdk_ctx* c, const float* d_q, int v0, int nv
 namespace {
 
 std::mutex g_tune_mutex;
-std::map<std::string, std::pair<int, int>> g_tune_cache;   // shape -> (slices per thread, views per chunk)
+struct TuneChoice {
+    int zpt, chunk, tile;   // slices per thread, views per chunk, tile width in x
+};
+std::map<std::string, TuneChoice> g_tune_cache;   // shape -> choice
 bool g_tune_file_read = false;
 
 std::string tune_key(const jfdk_ctx* c) {
@@ -1095,7 +1106,8 @@ std::string tune_key(const jfdk_ctx* c) {
     return k;
 }
 
-// Optional persistent cache: $JFDK_AUTOTUNE_CACHE, lines "key zpt chunk".
+// Optional persistent cache: $JFDK_AUTOTUNE_CACHE, lines "key zpt chunk tile"
+// (lines without the tile width, from earlier builds, read as width 4).
 void tune_file_load() {
     if (g_tune_file_read) return;
     g_tune_file_read = true;
@@ -1103,19 +1115,22 @@ void tune_file_load() {
     if (!path) return;
     std::FILE* f = std::fopen(path, "r");
     if (!f) return;
-    char key[256];
-    int z, ch;
-    while (std::fscanf(f, "%255s %d %d", key, &z, &ch) == 3)
-        if ((z == 4 || z == 8) && (ch == 16 || ch == 32 || ch == 64)) g_tune_cache[key] = {z, ch};
+    char line[512], key[256];
+    while (std::fgets(line, sizeof line, f)) {
+        int z = 0, ch = 0, tx = kBPTileX;
+        if (std::sscanf(line, "%255s %d %d %d", key, &z, &ch, &tx) < 3) continue;
+        if ((z == 4 || z == 8) && (ch == 16 || ch == 32 || ch == 64) && (tx == 4 || tx == 8 || tx == 32))
+            g_tune_cache[key] = {z, ch, tx};
+    }
     std::fclose(f);
 }
 
-void tune_file_append(const std::string& key, int z, int ch) {
+void tune_file_append(const std::string& key, const TuneChoice& t) {
     const char* path = std::getenv("JFDK_AUTOTUNE_CACHE");
     if (!path) return;
     std::FILE* f = std::fopen(path, "a");
     if (!f) return;
-    std::fprintf(f, "%s %d %d\n", key.c_str(), z, ch);
+    std::fprintf(f, "%s %d %d %d\n", key.c_str(), t.zpt, t.chunk, t.tile);
     std::fclose(f);
 }
 
@@ -1152,37 +1167,44 @@ extern "C" jfdk_status jfdk_autotune(jfdk_ctx* c, int flags) {
         tune_file_load();
         auto it = g_tune_cache.find(key);
         if (it != g_tune_cache.end() && !(flags & JFDK_AUTOTUNE_FORCE)) {
-            c->opt_bp_zpt = it->second.first;
-            c->opt_view_chunk = it->second.second;
+            c->opt_bp_zpt = it->second.zpt;
+            c->opt_view_chunk = it->second.chunk;
+            c->opt_bp_tile = it->second.tile;
             return JFDK_OK;
         }
     }
     jfdk_status st = ensure_Q4(c, c->nviews);
     if (st) return st;
-    // voxel tile depth: a finalizing backprojection of a central slab into a
-    // slab-sized buffer (the kernel indexes the output by absolute slice, so
-    // it is given the buffer's address minus the slab's offset)
+    // voxel tile (depth x width): a finalizing backprojection of a central
+    // slab into a slab-sized buffer (the kernel indexes the output by
+    // absolute slice, so it is given the buffer's address minus the slab's
+    // offset)
     const int nz = std::min(c->Z, 32);
     const int z0 = (c->Z - nz) / 2;
     const size_t plane = (size_t)c->X * c->Y;
     float* slab = nullptr;
     if ((st = dev_alloc(c, &slab, plane * nz, "the autotuner's slab"))) return st;
-    int best_z = 8;
+    int best_z = 8, best_x = kBPTileX;
     float best_t = 1e30f;
     for (int zpt : {4, 8}) {
-        c->opt_bp_zpt = zpt;
-        BPParams b = jfdk::reconstruct_bp_params(c, slab - (ptrdiff_t)(z0 * plane), nullptr);
-        b.z_begin = z0;
-        b.z_end = z0 + nz;
-        b.apply_ct = 0;
-        float t = 0.0f;
-        st = time_ms(c, [&] { return run_bp(c, b, true); }, &t);
+        for (int tx : {4, 8, 32}) {
+            c->opt_bp_zpt = zpt;
+            c->opt_bp_tile = tx;
+            BPParams b = jfdk::reconstruct_bp_params(c, slab - (ptrdiff_t)(z0 * plane), nullptr);
+            b.z_begin = z0;
+            b.z_end = z0 + nz;
+            b.apply_ct = 0;
+            float t = 0.0f;
+            st = time_ms(c, [&] { return run_bp(c, b, true); }, &t);
+            if (st) break;
+            if (t < best_t) { best_t = t; best_z = zpt; best_x = tx; }
+        }
         if (st) break;
-        if (t < best_t) { best_t = t; best_z = zpt; }
     }
     dev_free(c, slab);
     if (st) return st;
     c->opt_bp_zpt = best_z;
+    c->opt_bp_tile = best_x;
     // views per chunk: the filter stage over the first views of zero frames
     int best_c = c->opt_view_chunk;
     if (c->in_w == c->used_u) {   // (compositing reads conjugate frames of the whole rotation)
@@ -1205,7 +1227,7 @@ extern "C" jfdk_status jfdk_autotune(jfdk_ctx* c, int flags) {
     }
     c->opt_view_chunk = best_c;
     std::lock_guard<std::mutex> lk(g_tune_mutex);
-    g_tune_cache[key] = {best_z, best_c};
-    tune_file_append(key, best_z, best_c);
+    g_tune_cache[key] = {best_z, best_c, best_x};
+    tune_file_append(key, g_tune_cache[key]);
     return JFDK_OK;
 }

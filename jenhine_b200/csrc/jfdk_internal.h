@@ -33,8 +33,8 @@ std::string build_host_operators(const jfdk_scan_params& scan, const jfdk_recon_
                                  int in_w, int out_w, int rows, int mirror, float hsr,
                                  HostOperators& ops);
 
-// Backprojection CTA: kBPTileX x kBPTileY threads over (x, y), each thread a
-// run of slices in z (4 or 8 per thread).
+// Backprojection CTA: kBPTileX x kBPTileY threads over (x, y) by default and
+// in the batch kernel, each thread a run of slices in z (4 or 8 per thread).
 constexpr int kBPTileX = 4;
 constexpr int kBPTileY = 32;
 
@@ -76,8 +76,10 @@ struct BatchScan {
 };
 
 // Launchers (return cudaError_t of the launch).
-// zpt: slices per thread (4, 8 or 16).
-cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, cudaStream_t s);
+// zpt: slices per thread (4, 8 or 16); tile_x: CTA width in x, 4, 8 or 32
+// (CTAs of 128 threads; other values and 16-slice tiles take 4).
+cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, int tile_x,
+                      cudaStream_t s);
 // A batched backprojection launch covers up to kBatchSlots scans that share
 // the tile depth and whether W depends on z; their parameters travel in the
 // kernel's parameter space.
@@ -92,7 +94,8 @@ cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tile
 // CTAs of a full persistent wave: SMs x resident CTAs per SM.
 cudaError_t bp_batch_ctas(bool mixed_form, int zpt, bool wz, int* ctas);
 // Mixed-precision form: FP16 footprints with a per-view scale (qh, qscale).
-cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, cudaStream_t s);
+cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, int tile_x,
+                            cudaStream_t s);
 // absmax[f] = bit pattern of max |plain[f][...]| over each of nv frames.
 cudaError_t launch_frame_absmax(const float* plain, long long frame, int nv, unsigned* absmax, cudaStream_t s);
 // Filtered frames -> mixed-precision records in slots [slot0, slot0 + nv);
@@ -294,6 +297,7 @@ struct jfdk_ctx {
     int opt_view_chunk = 32;
     int opt_stage_timing = 0;
     int opt_bp_zpt = 0;          // 0: default (bp_zpt() in jfdk_api.cpp)
+    int opt_bp_tile = 0;         // tile width in x: 4, 8 or 32; 0: default (4)
     int opt_ramp = 0;            // JFDK_OPT_RAMP_PRODUCT (0: the form's default)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // jfdk_reconstruct_host: a copy stream and a second compute stream, and

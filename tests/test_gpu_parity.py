@@ -155,6 +155,46 @@ def test_reconstruct_int16_output(torch_cuda, case, oracle):
     np.testing.assert_array_equal(hu16.cpu().numpy(), oracle.to_int16(hu.cpu().numpy()))
 
 
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_voxel_tiles_give_the_same_volume(torch_cuda, case, precision):
+    """Every backprojection tile the autotuner chooses between (4, 8 or 32
+    threads wide in x; 4 or 8 slices per thread) computes each voxel the same
+    way: the volume equals the default tile's bit for bit, in chunks too."""
+    from jenhine_b200 import _lib
+    raw = to_dev(torch_cuda, case["raw"])
+    filt = to_dev(torch_cuda, case["filt"])
+    e = engine_for(case, precision=precision, bp_exact=(precision == "fp32"))
+
+    def run(zpt, tx):
+        e.set_option(_lib.OPT_BP_ZPT, zpt)
+        e.set_option(_lib.OPT_BP_TILE, tx)
+        hu = e.reconstruct(raw).clone()
+        e.bp_reset()
+        for v0 in range(0, filt.shape[0], 9):
+            e.bp_accumulate(filt[v0:v0 + 9].contiguous(), v0)
+        return hu, e.finalize(apply_ctnum=False).clone()
+
+    def same(a, b):
+        return torch_cuda.equal(torch_cuda.nan_to_num(a, 1e30), torch_cuda.nan_to_num(b, 1e30))
+
+    for zpt in (4, 8):
+        # the mixed form steps z from each thread's first slice: compare
+        # within one tile depth; the FP32 volume does not depend on it either
+        want = run(zpt, 4) if precision == "mixed" or zpt == 4 else want
+        for tx in (8, 32):
+            got = run(zpt, tx)
+            assert same(got[0], want[0]) and same(got[1], want[1]), (zpt, tx)
+    if precision == "fp32":
+        np.testing.assert_array_equal(want[1].cpu().numpy(), case["bp"])
+
+
+def test_voxel_tile_option_is_checked(torch_cuda, case):
+    from jenhine_b200 import _lib
+    e = engine_for(case)
+    with pytest.raises(_lib.JfdkError):
+        e.set_option(_lib.OPT_BP_TILE, 16)
+
+
 def test_zfilter_matches_reference_order(torch_cuda, case):
     e = engine_for(case)
     x = case["filt"][:5].copy()
