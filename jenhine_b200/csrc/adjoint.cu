@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(256) bp_adjoint_kernel(AdjParams p) {
     for (int n = 0; n < p.nv; ++n, P4 += 3, qb += p.q_frame) {
         const float4 r0 = __ldg(P4), r1 = __ldg(P4 + 1), r2 = __ldg(P4 + 2);
         const XYTerms xy = bp_xy_terms(ax, ay, r0, r1, r2);
-        const float rxy = WZ ? 0.0f : __frcp_rn(xy.W);
+        const float rxy = WZ ? 0.0f : rcp_rn_nr(xy.W);
 #pragma unroll
         for (int k = 0; k < ZPT; ++k) {
             const float2 uv = bp_uv(xy, bp_w_r<WZ>(xy, rxy, az[k], r2.z), az[k], r0.z, r1.z);
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(256) geometry_gradient_kernel(AdjParams p) {
         if (valid) {
             const float4 r0 = __ldg(P4), r1 = __ldg(P4 + 1), r2 = __ldg(P4 + 2);
             const XYTerms xy = bp_xy_terms(ax, ay, r0, r1, r2);
-            const float rxy = WZ ? 0.0f : __frcp_rn(xy.W);
+            const float rxy = WZ ? 0.0f : rcp_rn_nr(xy.W);
             const float4* __restrict__ q = p.q4 + (size_t)n * p.q_frame;
             const float2* __restrict__ tw = p.tw + (size_t)((p.v0 + n) % p.num_views) * p.U;
 #pragma unroll

@@ -159,7 +159,7 @@ __device__ __forceinline__ void bp_block(const BPParams& p, const Tile& tile) {
     for (int n = 0; n < p.nv; ++n, P4 += 3, q += p.q4_frame, tw += p.U) {
         const float4 r0 = __ldg(P4), r1 = __ldg(P4 + 1), r2 = __ldg(P4 + 2);
         const XYTerms xy = bp_xy_terms(ax, ay, r0, r1, r2);
-        const float rxy = WZ ? 0.0f : __frcp_rn(xy.W);
+        const float rxy = WZ ? 0.0f : rcp_rn_nr(xy.W);
 #pragma unroll
         for (int k = 0; k < ZPT; ++k) {
             float2 uv = bp_uv(xy, bp_w_r<WZ>(xy, rxy, az[k], r2.z), az[k], r0.z, r1.z);

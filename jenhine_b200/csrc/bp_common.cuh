@@ -93,12 +93,23 @@ __device__ __forceinline__ XYTerms bp_xy_terms(float ax, float ay, const float4&
     return t;
 }
 
+// RN(1/w) from the approximate reciprocal (rcp.approx, at most 1 ulp off)
+// and one Newton-Raphson step with a fused residual, y' = RN(y + y RN(1 - w y))
+// (Markstein, IBM J. Res. Dev. 34(1), 1990).  Equal to __frcp_rn for every
+// float w whose reciprocal is a normal float, both signs (all 4.2e9 of them
+// checked on a B200); W of a voxel lies far inside that range.
+__device__ __forceinline__ float rcp_rn_nr(float w) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(w));
+    return fmaf(fmaf(-w, y, 1.0f), y, y);
+}
+
 // W and r = RN(1/W) at slice coordinate az (W independent of z unless WZ).
 template <bool WZ>
 __device__ __forceinline__ float2 bp_w_r(const XYTerms& t, float rxy, float az, float P10) {
     if (WZ) {
         const float W = __fadd_rn(t.W, __fmul_rn(az, P10));
-        return f2(W, __frcp_rn(W));
+        return f2(W, rcp_rn_nr(W));
     }
     return f2(t.W, rxy);
 }
