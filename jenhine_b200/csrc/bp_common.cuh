@@ -96,8 +96,8 @@ __device__ __forceinline__ XYTerms bp_xy_terms(float ax, float ay, const float4&
 // RN(1/w) from the approximate reciprocal (rcp.approx, at most 1 ulp off)
 // and one Newton-Raphson step with a fused residual, y' = RN(y + y RN(1 - w y))
 // (Markstein, IBM J. Res. Dev. 34(1), 1990).  Equal to __frcp_rn for every
-// float w whose reciprocal is a normal float, both signs (all 4.2e9 of them
-// checked on a B200); W of a voxel lies far inside that range.
+// float w whose reciprocal is a normal float, both signs (all 4.2e9 of them,
+// tests/cuda/reciprocal_check.cu); W of a voxel lies far inside that range.
 __device__ __forceinline__ float rcp_rn_nr(float w) {
     float y;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(w));
