@@ -362,6 +362,17 @@ long long jfdk_kernel_launches(const jfdk_ctx* ctx);
  * JFDK_OPT_DEVICE_MEMORY_LIMIT bounds). */
 long long jfdk_device_bytes(const jfdk_ctx* ctx);
 
+/* The backprojector's fetch ceiling on the current device (no counterpart in
+ * the reference): samples per second that the load path delivers when warps
+ * do nothing but a backprojection sample's loads -- one record_bytes (16 or
+ * 8) record per lane, plus an 8-byte taper pair when with_taper, `distinct`
+ * consecutive records per warp request (1-32), from an L1-resident table,
+ * at warps_per_sm resident warps (a multiple of 4, 4-64).  The ceiling that
+ * a backprojection's samples per second are measured against.  Allocates
+ * and frees 100 KB of device memory; synchronises. */
+jfdk_status jfdk_measure_gather_rate(int record_bytes, int with_taper, int distinct, int warps_per_sm,
+                                     double* samples_per_s);
+
 /* jfdk_sync also reports JFDK_ERR_CUDA when a kernel's bounded wait gave up
  * (the device status word is then cleared). */
 

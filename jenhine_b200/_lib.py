@@ -109,6 +109,7 @@ _SIGS = {
     "jfdk_batch_run": ([_P, _P, _P], C.c_int),
     "jfdk_batch_launches": ([_P], C.c_longlong),
     "jfdk_batch_schedule": ([_P], C.c_int),
+    "jfdk_measure_gather_rate": ([C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double)], C.c_int),
 }
 
 

@@ -57,3 +57,12 @@ def test_engine_fails_loudly_without_the_library(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "missing.so"))
     with pytest.raises(ImportError):
         _lib.load()
+
+
+def test_gather_rate_rejects_bad_arguments_before_touching_the_device():
+    from jenhine_b200 import _lib
+    lib = _lib.load()
+    r = ctypes.c_double(-1.0)
+    for args in ((12, 1, 6, 32), (16, 1, 0, 32), (16, 1, 33, 32), (8, 0, 4, 30), (8, 0, 4, 68)):
+        assert lib.jfdk_measure_gather_rate(*args, ctypes.byref(r)) == _lib.JFDK_ERR_INVALID
+    assert lib.jfdk_measure_gather_rate(16, 1, 6, 32, None) == _lib.JFDK_ERR_INVALID
