@@ -743,35 +743,51 @@ typedef struct {
 } bpp_job;
 
 static void* bpp_worker(void* arg) {
+    /* Points in blocks of BPP_BLOCK, views inside a block: a view's rows stay
+     * in cache while the block's points sample them (a view per point misses
+     * the cache on every sample).  The sums per point run over the views in
+     * order. */
+    enum { BPP_BLOCK = 1024 };
     bpp_job* j = (bpp_job*)arg;
     const int U = j->U, V = j->V;
-    for (int i = j->p0; i < j->p1; ++i) {
-        const double x = ((double)j->pts[3 * i] - (j->X - 1) / 2.0) * j->pitchXY;
-        const double y = ((double)j->pts[3 * i + 1] - (j->Y - 1) / 2.0) * j->pitchXY;
-        const double z = ((double)j->pts[3 * i + 2] - (j->Z - 1) / 2.0) * j->pitchZ;
-        double s = 0.0, c = 0.0;
+    double xs[BPP_BLOCK], ys[BPP_BLOCK], zs[BPP_BLOCK], ss[BPP_BLOCK], cs[BPP_BLOCK];
+    for (int b = j->p0; b < j->p1; b += BPP_BLOCK) {
+        const int n = j->p1 - b < BPP_BLOCK ? j->p1 - b : BPP_BLOCK;
+        for (int k = 0; k < n; ++k) {
+            const int i = b + k;
+            xs[k] = ((double)j->pts[3 * i] - (j->X - 1) / 2.0) * j->pitchXY;
+            ys[k] = ((double)j->pts[3 * i + 1] - (j->Y - 1) / 2.0) * j->pitchXY;
+            zs[k] = ((double)j->pts[3 * i + 2] - (j->Z - 1) / 2.0) * j->pitchZ;
+            ss[k] = 0.0;
+            cs[k] = 0.0;
+        }
         for (int iv = 0; iv < j->nv; ++iv) {
             const int view = j->v0 + iv;
             const double* P = j->ptms + (size_t)view * 12;
-            const double Uc = x * P[0] + y * P[1] + z * P[2] + P[3];
-            const double Vc = x * P[4] + y * P[5] + z * P[6] + P[7];
-            const double Wc = x * P[8] + y * P[9] + z * P[10] + P[11];
-            const double u = Uc / Wc + 0.5, v = Vc / Wc + 0.5;
-            if (!(u >= 0.0 && u <= U - 1 && v >= 0.0 && v <= V - 1)) continue;
-            const int ix = (int)floor(u), iy = (int)floor(v);
-            const int ix1 = ix + 1 < U ? ix + 1 : U - 1;
-            const int iy1 = iy + 1 < V ? iy + 1 : V - 1;
-            const double fx = u - ix, fy = v - iy;
             const double* p = j->proj + (size_t)iv * U * V;
             const float* w = j->uw + (size_t)view * U;
-            const double p00 = p[(size_t)iy * U + ix] * w[ix], p01 = p[(size_t)iy * U + ix1] * w[ix1];
-            const double p10 = p[(size_t)iy1 * U + ix] * w[ix], p11 = p[(size_t)iy1 * U + ix1] * w[ix1];
-            const double t0 = p00 + fx * (p01 - p00), t1 = p10 + fx * (p11 - p10);
-            s += t0 + fy * (t1 - t0);
-            c += (double)w[ix] + fx * ((double)w[ix1] - w[ix]);
+            for (int k = 0; k < n; ++k) {
+                const double x = xs[k], y = ys[k], z = zs[k];
+                const double Uc = x * P[0] + y * P[1] + z * P[2] + P[3];
+                const double Vc = x * P[4] + y * P[5] + z * P[6] + P[7];
+                const double Wc = x * P[8] + y * P[9] + z * P[10] + P[11];
+                const double u = Uc / Wc + 0.5, v = Vc / Wc + 0.5;
+                if (!(u >= 0.0 && u <= U - 1 && v >= 0.0 && v <= V - 1)) continue;
+                const int ix = (int)floor(u), iy = (int)floor(v);
+                const int ix1 = ix + 1 < U ? ix + 1 : U - 1;
+                const int iy1 = iy + 1 < V ? iy + 1 : V - 1;
+                const double fx = u - ix, fy = v - iy;
+                const double p00 = p[(size_t)iy * U + ix] * w[ix], p01 = p[(size_t)iy * U + ix1] * w[ix1];
+                const double p10 = p[(size_t)iy1 * U + ix] * w[ix], p11 = p[(size_t)iy1 * U + ix1] * w[ix1];
+                const double t0 = p00 + fx * (p01 - p00), t1 = p10 + fx * (p11 - p10);
+                ss[k] += t0 + fy * (t1 - t0);
+                cs[k] += (double)w[ix] + fx * ((double)w[ix1] - w[ix]);
+            }
         }
-        j->sum[i] += s;
-        j->cnt[i] += c;
+        for (int k = 0; k < n; ++k) {
+            j->sum[b + k] += ss[k];
+            j->cnt[b + k] += cs[k];
+        }
     }
     return NULL;
 }
@@ -801,6 +817,66 @@ void jo_bp_points_f64(double* sum, double* cnt, const double* proj, const float*
     for (size_t i = 0; i < 12 * (size_t)nviews; ++i) pd[i] = ptms[i];
     jo_bp_points_f64d(sum, cnt, proj, pd, uw, v0, nv, U, V, pts, npts, X, Y, Z, pitchXY, pitchZ, nthreads);
     free(pd);
+}
+
+/* Where voxels project, in double (test bookkeeping for the FP64 checks):
+ * interior[i] = 1 when every view samples point i at least `margin` pixels
+ * inside the detector; vrange = the smallest and largest v of the samples
+ * that fall inside the detector (0 <= u <= U-1, 0 <= v <= V-1), over all
+ * points and views (vrange[0] > vrange[1] when there are none). */
+typedef struct {
+    const int* pts; int p0, p1; const double* ptms; int nv, X, Y, Z; double pxy, pz; int U, V; double margin;
+    unsigned char* interior; double vmin, vmax;
+} survey_job;
+
+static void* survey_worker(void* arg) {
+    survey_job* j = (survey_job*)arg;
+    j->vmin = 1e300;
+    j->vmax = -1e300;
+    for (int i = j->p0; i < j->p1; ++i) {
+        const double x = ((double)j->pts[3 * i] - (j->X - 1) / 2.0) * j->pxy;
+        const double y = ((double)j->pts[3 * i + 1] - (j->Y - 1) / 2.0) * j->pxy;
+        const double z = ((double)j->pts[3 * i + 2] - (j->Z - 1) / 2.0) * j->pz;
+        int inside = 1;
+        for (int k = 0; k < j->nv; ++k) {
+            const double* P = j->ptms + (size_t)k * 12;
+            const double Wc = x * P[8] + y * P[9] + z * P[10] + P[11];
+            const double u = (x * P[0] + y * P[1] + z * P[2] + P[3]) / Wc + 0.5;
+            const double v = (x * P[4] + y * P[5] + z * P[6] + P[7]) / Wc + 0.5;
+            if (!(u >= j->margin && u <= j->U - 1 - j->margin && v >= j->margin && v <= j->V - 1 - j->margin))
+                inside = 0;
+            if (u >= 0.0 && u <= j->U - 1 && v >= 0.0 && v <= j->V - 1) {
+                if (v < j->vmin) j->vmin = v;
+                if (v > j->vmax) j->vmax = v;
+            }
+        }
+        j->interior[i] = (unsigned char)inside;
+    }
+    return NULL;
+}
+
+void jo_points_survey(unsigned char* interior, double* vrange, const int* pts, int npts, const double* ptms,
+                      int nv, int X, int Y, int Z, double pitchXY, double pitchZ, int U, int V, double margin,
+                      int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > npts) nthreads = npts > 0 ? npts : 1;
+    pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * nthreads);
+    survey_job* jobs = (survey_job*)malloc(sizeof(survey_job) * nthreads);
+    for (int t = 0; t < nthreads; ++t) {
+        survey_job jb = {pts, (int)((long)npts * t / nthreads), (int)((long)npts * (t + 1) / nthreads), ptms, nv,
+                         X, Y, Z, pitchXY, pitchZ, U, V, margin, interior, 0.0, 0.0};
+        jobs[t] = jb;
+        pthread_create(&th[t], NULL, survey_worker, &jobs[t]);
+    }
+    vrange[0] = 1e300;
+    vrange[1] = -1e300;
+    for (int t = 0; t < nthreads; ++t) {
+        pthread_join(th[t], NULL);
+        if (jobs[t].vmin < vrange[0]) vrange[0] = jobs[t].vmin;
+        if (jobs[t].vmax > vrange[1]) vrange[1] = jobs[t].vmax;
+    }
+    free(th);
+    free(jobs);
 }
 
 /* BPCore::DoneSlice (BPCore.cpp:198-205): out = sum / cnt. */

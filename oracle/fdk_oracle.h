@@ -112,6 +112,12 @@ void jo_bp_points_f64(double* sum, double* cnt, const double* proj, const float*
 void jo_bp_points_f64d(double* sum, double* cnt, const double* proj, const double* ptms,
                        const float* uw, int v0, int nv, int U, int V, const int* pts, int npts,
                        int X, int Y, int Z, float pitchXY, float pitchZ, int nthreads);
+/* interior[i]: every view samples point i at least `margin` pixels inside
+ * the detector; vrange[2]: least and largest v of the in-detector samples.
+ * Double precision; ptms [nv][12] in double. */
+void jo_points_survey(unsigned char* interior, double* vrange, const int* pts, int npts, const double* ptms,
+                      int nv, int X, int Y, int Z, double pitchXY, double pitchZ, int U, int V, double margin,
+                      int nthreads);
 /* out = sum / cnt (BPCore::DoneSlice). */
 void jo_bp_finalize(float* out, const float* sum, const float* cnt, size_t n);
 

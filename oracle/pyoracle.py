@@ -54,6 +54,7 @@ class Oracle:
             "jo_composite": [_P, _P, _P, _P, _P, F, I, I, I],
             "jo_bp_points_f64": [_P, _P, _P, _P, _P, I, I, I, I, _P, I, I, I, I, F, F, I],
             "jo_bp_points_f64d": [_P, _P, _P, _P, _P, I, I, I, I, _P, I, I, I, I, F, F, I],
+            "jo_points_survey": [_P, _P, _P, I, _P, I, I, I, I, C.c_double, C.c_double, I, I, C.c_double, I],
             "jo_filter_kernel_f64": [_P, _P, I], "jo_bp_uweights": [_P, _P, I, I],
             "jo_bp_accumulate": [_P, _P, _P, _P, _P, I, I, I, I, I, I, I, F, F, I, I, I],
             "jo_bp_accumulate_f64": [_P, _P, _P, _P, _P, I, I, I, I, I, I, I, F, F, I, I, I],
@@ -286,20 +287,26 @@ class Oracle:
                                    nthreads or os.cpu_count() or 1)
         return s, c
 
-    @staticmethod
-    def _check_band(ptms, pts, X, Y, Z, pitch_xy, pitch_z, U, V, r0, r1):
-        P = ptms.astype(np.float64)
-        xyz1 = np.stack([(pts[:, 0] - (X - 1) / 2.0) * pitch_xy, (pts[:, 1] - (Y - 1) / 2.0) * pitch_xy,
-                         (pts[:, 2] - (Z - 1) / 2.0) * pitch_z, np.ones(len(pts))], 1)
-        for k in range(P.shape[0]):
-            uvw = xyz1 @ P[k].reshape(3, 4).T
-            u = uvw[:, 0] / uvw[:, 2] + 0.5
-            v = uvw[:, 1] / uvw[:, 2] + 0.5
-            used = (u >= 0) & (u <= U - 1) & (v >= 0) & (v <= V - 1)
-            if used.any():
-                lo, hi = np.floor(v[used]).min(), np.floor(v[used]).max() + 1
-                if lo < r0 or hi >= r1:
-                    raise ValueError(f"view {k}: samples rows {lo:.0f}..{hi:.0f} outside [{r0}, {r1})")
+    def points_survey(self, ptms, pts, X, Y, Z, pitch_xy, pitch_z, U, V, margin=1.0, nthreads=None):
+        """(interior, vrange) of voxels pts[n][3] in double: interior[i] when
+        every view samples point i at least `margin` pixels inside the U x V
+        detector; vrange = (least, largest) v over the samples inside the
+        detector, or None when no sample is."""
+        P = _c(np.asarray(ptms, np.float64).reshape(-1, 12), np.float64)
+        pts = _c(pts, np.int32).reshape(-1, 3)
+        inside = np.zeros(len(pts), np.uint8)
+        vr = np.zeros(2, np.float64)
+        self.lib.jo_points_survey(_ptr(inside), _ptr(vr), _ptr(pts), len(pts), _ptr(P), P.shape[0], X, Y, Z,
+                                  float(pitch_xy), float(pitch_z), U, V, float(margin),
+                                  nthreads or os.cpu_count() or 1)
+        return inside.astype(bool), (None if vr[0] > vr[1] else (float(vr[0]), float(vr[1])))
+
+    def _check_band(self, ptms, pts, X, Y, Z, pitch_xy, pitch_z, U, V, r0, r1):
+        _, vr = self.points_survey(ptms, pts, X, Y, Z, pitch_xy, pitch_z, U, V)
+        if vr is not None:
+            lo, hi = np.floor(vr[0]), np.floor(vr[1]) + 1
+            if lo < r0 or hi >= r1:
+                raise ValueError(f"samples rows {lo:.0f}..{hi:.0f} outside [{r0}, {r1})")
 
     @staticmethod
     def ctnum_f64(mu, norm0, norm1, mu_water=0.02):

@@ -38,13 +38,22 @@ def project_points(g: dict, pts: np.ndarray):
     return uvw[:, 0] / uvw[:, 2] + 0.5, uvw[:, 1] / uvw[:, 2] + 0.5
 
 
+def survey(g: dict, pts: np.ndarray, margin: float = 1.0):
+    """(interior, vrange) of the points (oracle.points_survey, in double):
+    interior[i] when every view samples point i at least `margin` pixels
+    inside the detector; vrange the least and largest detector row (as
+    floats) of the samples inside the detector, or None."""
+    from oracle.pyoracle import Oracle
+    X, Y, Z = (int(v) for v in g["vol"])
+    pxy, pz = (float(v) for v in g["pitch"])
+    V, U = g["raw"].shape[1:]
+    return Oracle().points_survey(g["ptms"], pts, X, Y, Z, pxy, pz, U, V, margin)
+
+
 def interior(g: dict, pts: np.ndarray, margin: float = 1.0) -> np.ndarray:
     """Points that every view samples at least `margin` pixels inside the
     detector: their sample set does not depend on how u, v are rounded."""
-    V, U = g["raw"].shape[1:]
-    u, v = project_points(g, pts)
-    ok = (u >= margin) & (u <= U - 1 - margin) & (v >= margin) & (v <= V - 1 - margin)
-    return ok.all(axis=0)
+    return survey(g, pts, margin)[0]
 
 
 def all_points(X: int, Y: int, Z: int, z0: int = 0, nz: int | None = None, stride: int = 1) -> np.ndarray:
@@ -60,10 +69,9 @@ def fdk_f64(oracle, g: dict, pts: np.ndarray) -> np.ndarray:
     X, Y, Z = (int(v) for v in g["vol"])
     pxy, pz = (float(v) for v in g["pitch"])
     # detector rows the points sample (+1 for the lower neighbour)
-    _, v = project_points(g, pts)
-    vin = v[(v >= 0) & (v <= Hh - 1)]
-    r0 = max(int(np.floor(vin.min())) - 1, 0) if vin.size else 0
-    r1 = min(int(np.floor(vin.max())) + 3, Hh) if vin.size else Hh
+    band = survey(g, pts)[1]
+    r0 = max(int(np.floor(band[0])) - 1, 0) if band else 0
+    r1 = min(int(np.floor(band[1])) + 3, Hh) if band else Hh
     pre = np.stack([oracle.preprocess(raw[i], float(g["bright_field"]), tuple(g["bhc"])) for i in range(nv)])
     L = oracle.fft_length(W)
     H = oracle.filter_spectrum(L, float(g["hsr"]), float(g["cut"][0]), float(g["cut"][1]), g["adj_pts"],
