@@ -4,20 +4,20 @@ The form: filtered projections stored as FP16 with a power-of-two scale per
 view, the ramp product in split precision on the tensor cores, approximate
 reciprocal coordinates, FP32 accumulation.  Bars, over the interior voxels --
 those that every view samples at least one pixel inside the detector:
-  * rel-L2 of the attenuation (HU + 1000) <= 1e-4 at the benchmark size
-    (600 views); <= 2e-4 for the 36- and 40-view fixtures, where each voxel
-    averages the FP16 rounding of 15x fewer samples;
+  * rel-L2 of the attenuation (HU + 1000) <= 1e-4, at the benchmark size
+    (600 views) and on the 36- to 60-view fixtures alike;
   * max |dHU| <= 1.
 At the edge of the field of view a voxel whose sample point lies within
 rounding distance of the detector border gains or loses that view in any
 finite precision, the plain FP32 form included (at the benchmark size the
-plain form differs from FP64 by up to ~35 HU there); those voxels are
-reported (rel_l2_all, max_hu_all) but not bounded.  The plain form is
-measured beside the mixed one; at the benchmark size its distance to FP64
-(~3e-5 rel-L2, ~0.1 HU near the metal inserts, where sums of large filtered
-values of both signs cancel) is float rounding of the reference algorithm
-itself, so it is held to the same FP64 bars there (its bar against the
-reference's float cores is 1e-5, tested in test_gpu_parity.py)."""
+plain form differs from FP64 by up to ~35 HU there); over all voxels the
+rel-L2 is held to the same 1e-4 and the largest |dHU| and the number of
+voxels over 1 HU are reported.  The plain form is measured beside the mixed
+one; at the benchmark size its distance to FP64 (~3e-5 rel-L2, ~0.1 HU near
+the metal inserts, where sums of large filtered values of both signs cancel)
+is float rounding of the reference algorithm itself, so it is held to the
+same FP64 bars there (its bar against the reference's float cores is 1e-5,
+tested in test_gpu_parity.py and test_parity_configs.py)."""
 import numpy as np
 import pytest
 
@@ -48,8 +48,7 @@ def test_mixed_vs_fp64_oracle_mini(torch_cuda, oracle, name):
         hu = engine_for(g, precision=form).reconstruct(raw).cpu().numpy().ravel()
         err = errors(hu, ref, inside)
         report(name, form, err)
-        # the fixtures have 36-40 views: each voxel averages fewer FP16 roundings
-        assert err["rel_l2_interior"] <= (2e-4 if form == "mixed" else 1e-5), err
+        assert err["rel_l2_interior"] <= (1e-4 if form == "mixed" else 1e-5), err
         assert err["max_hu_interior"] <= 1.0, err
 
 
@@ -73,25 +72,28 @@ def test_mixed_stages_equal_whole_volume(torch_cuda):
 
 def test_mixed_c2_slab_vs_fp64_oracle(torch_cuda, oracle):
     """Full benchmark size (600 views of 768 x 768 -> 640 x 640 x 480): a
-    64-slice slab through the centre, every 5th voxel in x and y, against the
-    FP64 oracle."""
+    64-slice slab through the centre, every voxel (26.2 M), against the FP64
+    oracle."""
     from jenhine_b200.fdk import FDKEngine
     from jenhine_b200.workloads import c2
     w = c2()
     raw = w.raw_torch()
     r = w.recon
-    z0, nz, stride = r.num_pixels_z // 2 - 32, 64, 5
-    pts = all_points(r.num_pixels_x, r.num_pixels_y, r.num_pixels_z, z0=z0, nz=nz, stride=stride)
+    z0, nz = r.num_pixels_z // 2 - 32, 64
+    pts = all_points(r.num_pixels_x, r.num_pixels_y, r.num_pixels_z, z0=z0, nz=nz)
     g = case_from_workload(w, raw.cpu().numpy())
     ref = fdk_f64(oracle, g, pts)
     inside = interior(g, pts)
     for form in ("fp32", "mixed"):
         e = FDKEngine(w.scan, w.recon, w.geom.ptms(), precision=form)
         vol = e.reconstruct(raw)
-        hu = vol[z0:z0 + nz, ::stride, ::stride].cpu().numpy().ravel()
+        hu = vol[z0:z0 + nz].cpu().numpy().ravel()
         e.close()
         del vol
         err = errors(hu, ref, inside)
-        report("c2_slab64_stride5", form, err)
+        err["voxels_over_1hu"] = int(np.count_nonzero(np.abs(hu - ref) > 1.0))
+        report("c2_slab64", form, err)
+        print(form, err)
         assert err["rel_l2_interior"] <= 1e-4, err
         assert err["max_hu_interior"] <= 1.0, err
+        assert err["rel_l2_all"] <= 1e-4, err
