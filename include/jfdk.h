@@ -121,20 +121,25 @@ jfdk_status jfdk_preprocess_frames(jfdk_ctx* ctx, const uint16_t* d_raw, int nv,
 jfdk_status jfdk_filter_frames(jfdk_ctx* ctx, const float* d_in, int v0, int nv, float* d_out);
 
 /* jfdk_filter_frames for callers that must not allocate device memory while
- * they run: code being captured into a CUDA graph (cudaMalloc is not allowed
- * during capture), hosts whose framework owns all device memory through its
- * own pool, and acquisition threads that cannot afford a cudaMalloc.  No
- * counterpart in the reference: it is an addition of this library.  Same
- * inputs, outputs and results as jfdk_filter_frames, but its working rows
- * live in one 4 MiB array compiled into libjfdk.so (held by every GPU that
- * loads the library until the process exits) instead of memory allocated on
- * first use; nothing is allocated or freed.  Limit: nv * rows * pitch + nv *
- * rows floats must fit in 1,048,576 floats, where pitch is filter_in_w rounded
- * up to a multiple of 64 (for a 768 x 768 frame: one view per call); larger
+ * they run: hosts whose framework owns all device memory through its own
+ * pool or budget, and acquisition threads that cannot afford a cudaMalloc
+ * (it can synchronise the device and take milliseconds).  No counterpart in
+ * the reference: it is an addition of this library.  Same inputs and outputs
+ * as jfdk_filter_frames; its working rows live in one 4 MiB array compiled
+ * into libjfdk.so (held by every GPU that loads the library until the process
+ * exits) instead of memory allocated on first use; nothing is allocated or
+ * freed.  The ramp product always runs on FP32 CUDA cores, whatever the
+ * context's precision or JFDK_OPT_RAMP_PRODUCT: the result equals
+ * jfdk_filter_frames' under JFDK_RAMP_FP32_SIMT bit for bit and the other
+ * products' within their rounding (rel-L2 <= 1e-5 against TF32x3 and
+ * FP16x3, <= 5e-5 against BF16x3).  Limit: nv * rows * pitch + nv * rows
+ * floats must fit in 1,048,576 floats, where pitch is filter_in_w rounded up
+ * to a multiple of 64 (for a 768 x 768 frame: one view per call); larger
  * requests return JFDK_ERR_INVALID.  The first call on each device looks up
- * the array's device address (with that device current) and caches it: make
- * that first call before any stream capture.  All calls share the array:
- * calls whose kernels can overlap on the GPU race and must be serialised. */
+ * the array's device address (with that device current) and caches it for
+ * the life of the process; the cache is not valid across cudaDeviceReset.
+ * All calls share the array: calls whose kernels can overlap on the GPU race
+ * and must be serialised. */
 jfdk_status jfdk_filter_frames_noalloc(jfdk_ctx* ctx, const float* d_in, int v0, int nv, float* d_out);
 
 /* CompositeAgent::ProcessTask + CompositeCore::Process

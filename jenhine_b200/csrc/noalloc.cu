@@ -1,14 +1,14 @@
 // noalloc.cu -- the ramp-filter stage without any device allocation.
 //
 // Who needs this: callers that must not allocate device memory while they
-// run -- code that is being captured into a CUDA graph (cudaMalloc is not
-// allowed inside a capture), hosts whose framework owns every allocation
-// through its own pool, and real-time or interrupt-driven acquisition threads
-// where a cudaMalloc (which can synchronise the device and take milliseconds)
-// is not acceptable.  jfdk_filter_frames allocates its working rows on first
-// use; jfdk_filter_frames_noalloc runs the same two kernels (pre-weight + edge
-// means, then the ramp product) with that working storage taken from one
-// fixed array compiled into the library.
+// run -- hosts whose framework owns every allocation through its own pool or
+// budget, and real-time or interrupt-driven acquisition threads where a
+// cudaMalloc (which can synchronise the device and take milliseconds) is not
+// acceptable.  jfdk_filter_frames allocates its working rows on first use;
+// jfdk_filter_frames_noalloc runs the pre-weight + edge-mean kernel and the
+// FP32 CUDA-core ramp product (the JFDK_RAMP_FP32_SIMT path of
+// jfdk_filter_frames, whatever the context's form) with that working storage
+// taken from one fixed array compiled into the library.
 //
 // The array is a file-scope __device__ variable, so every GPU that loads
 // libjfdk.so holds its 4 MiB until the process exits, and every call shares
@@ -16,7 +16,9 @@
 // race on it and must be serialised by the caller.  Each call overwrites all
 // of the part it reads (the pre-weight kernel writes every row element,
 // including the zero padding up to the row pitch, and every edge mean), so
-// nothing needs clearing between calls.
+// nothing needs clearing between calls.  Its device address is looked up
+// once per device and kept for the life of the process; a cudaDeviceReset
+// makes it stale.
 #include <cuda_runtime.h>
 
 #include <cstdio>

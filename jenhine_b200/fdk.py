@@ -196,22 +196,38 @@ class FDKEngine:
         self._check(self.lib.jfdk_preprocess_frames(self.ctx, _ptr(raw), nv, _ptr(out)))
         return out
 
-    def filter(self, frames, v0: int = 0, out=None):
+    def _filter_buffers(self, frames, out):
+        """Checks frames (nv, rows, filter_in_w) and out (nv, rows,
+        filter_out_w): contiguous float32 CUDA tensors; out is made when not
+        given.  The C ABI takes raw pointers and would read or write past a
+        tensor of another shape."""
         import torch
+
+        def check(t, w, what):
+            if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+                raise ValueError(f"{what} must be a contiguous float32 CUDA tensor")
+            if t.dim() != 3 or tuple(t.shape[1:]) != (self.rows, w):
+                raise ValueError(f"{what} must be (views, {self.rows}, {w}), got {tuple(t.shape)}")
+        check(frames, self.filter_in_w, "frames")
         nv = frames.shape[0]
-        out = out if out is not None else torch.empty((nv, self.rows, self.filter_out_w), dtype=torch.float32,
-                                                      device=frames.device)
+        if out is None:
+            out = torch.empty((nv, self.rows, self.filter_out_w), dtype=torch.float32, device=frames.device)
+        check(out, self.filter_out_w, "out")
+        if out.shape[0] != nv:
+            raise ValueError(f"out holds {out.shape[0]} views, frames {nv}")
+        return nv, out
+
+    def filter(self, frames, v0: int = 0, out=None):
+        nv, out = self._filter_buffers(frames, out)
         self._check(self.lib.jfdk_filter_frames(self.ctx, _ptr(frames), v0, nv, _ptr(out)))
         return out
 
     def filter_noalloc(self, frames, v0: int = 0, out=None):
         """``filter`` through jfdk_filter_frames_noalloc: working rows in the
         library's fixed 4 MiB device array, no allocation by the library (out
-        must be given by callers that cannot allocate)."""
-        import torch
-        nv = frames.shape[0]
-        out = out if out is not None else torch.empty((nv, self.rows, self.filter_out_w), dtype=torch.float32,
-                                                      device=frames.device)
+        must be given by callers that cannot allocate); the ramp product on
+        FP32 CUDA cores whatever the context's form."""
+        nv, out = self._filter_buffers(frames, out)
         self._check(self.lib.jfdk_filter_frames_noalloc(self.ctx, _ptr(frames), v0, nv, _ptr(out)))
         return out
 

@@ -1,10 +1,14 @@
 """jfdk_filter_frames_noalloc: the ramp-filter stage for callers that cannot
-allocate device memory while they run (graph capture, framework-owned memory
-pools, real-time acquisition threads).  Its working rows sit in a fixed 4 MiB
-array inside libjfdk.so.  Checked through the C ABI against
-jfdk_filter_frames on two calls in a row (the array keeps the first call's
-contents when the second starts), at the filter's parity tolerance
-(rel-L2 <= 1e-5, as in test_gpu_parity), and for its size limit.
+allocate device memory while they run (framework-owned memory pools or
+budgets, real-time acquisition threads).  Its working rows sit in a fixed
+4 MiB array inside libjfdk.so and its ramp product runs on FP32 CUDA cores in
+either form.  Checked through the C ABI against jfdk_filter_frames on two
+calls in a row (the array keeps the first call's contents when the second
+starts): at the filter's parity tolerance against the FP32 form's default
+product (rel-L2 <= 1e-5, as in test_gpu_parity), at the BF16x3 product's
+tolerance (5e-5) against the mixed form's default, bit for bit against
+jfdk_filter_frames with the same FP32 CUDA-core product; and for its size
+limit.
 
 This file is collected last on purpose."""
 import numpy as np
@@ -15,7 +19,7 @@ from conftest import load_golden, rel_l2
 pytestmark = pytest.mark.gpu
 
 
-def _engine(g):
+def _engine(g, precision="fp32"):
     from jenhine_b200.fdk import FDKEngine, ReconConfig, ScanConfig
     raw = g["raw"]
     X, Y, Z = (int(v) for v in g["vol"])
@@ -25,7 +29,7 @@ def _engine(g):
     recon = ReconConfig(X, Y, Z, float(g["pitch"][0]), float(g["pitch"][1]),
                         filter_cutoff_start=float(g["cut"][0]), filter_cutoff_end=float(g["cut"][1]),
                         adjust_points=tuple(g["adj_pts"]), adjust_level_db=tuple(g["adj_db"]))
-    return FDKEngine(scan, recon, g["ptms"])
+    return FDKEngine(scan, recon, g["ptms"], precision=precision)
 
 
 def test_noalloc_filter_matches_filter_on_two_calls_in_a_row():
@@ -45,6 +49,25 @@ def test_noalloc_filter_matches_filter_on_two_calls_in_a_row():
         assert np.isfinite(got).all()
         assert rel_l2(got, want) <= 1e-5
         assert rel_l2(got, g["filt"][v0:v1]) <= 1e-5
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_noalloc_filter_runs_the_fp32_cuda_core_product_in_either_form(precision):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from jenhine_b200 import _lib
+    g = load_golden("mini_c2")
+    e = _engine(g, precision)
+    simt = _engine(g, precision)
+    simt.set_option(_lib.OPT_RAMP_PRODUCT, _lib.RAMP_FP32_SIMT)
+    prep = torch.from_numpy(np.ascontiguousarray(g["prep"])).cuda()
+    for v0, v1 in ((0, 9), (9, 30)):
+        frames = prep[v0:v1].contiguous()
+        got = e.filter_noalloc(frames, v0=v0).cpu().numpy()
+        np.testing.assert_array_equal(got, simt.filter(frames, v0=v0).cpu().numpy())
+        default = e.filter(frames, v0=v0).cpu().numpy()   # TF32x3 (fp32) or BF16x3 (mixed)
+        assert rel_l2(got, default) <= (5e-5 if precision == "mixed" else 1e-5)
 
 
 def test_noalloc_filter_rejects_requests_beyond_the_array():
