@@ -17,6 +17,17 @@ whose *name* is that literal string) and puts that directory on the quoted
 include path.  Nothing from the reference is copied; the forwarders only hold
 an ``#include`` of the real file.
 
+A third library, ``baseline/_ref/libbpcuda_ref.so``, holds the reference's
+GPU backprojector (``BPCUDAAgent/BPCUDACore.cu`` and ``BPCUDACore.cpp`` with
+the ``CUDA/`` wrappers it uses), compiled unchanged for sm_100a, plus
+``ref_gpu/bpcuda_driver.cpp``, which drives it the way BPCUDAAgent does.  It
+is the GPU baseline bench.py times beside the engine; git-ignored, it travels
+with the working tree like the others.
+
+The reference tree is taken from ``--reference DIR``, else from
+``$JFDK_REFERENCE_DIR``, else from the path it is mounted at in the build
+container.
+
 Usage:  python oracle/build.py [--reference DIR]
 """
 from __future__ import annotations
@@ -28,7 +39,12 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_DEFAULT = "/root/reference"
+REF_DEFAULT = os.environ.get("JFDK_REFERENCE_DIR", "/root/reference")
+REPO = os.path.dirname(HERE)
+OUT_GPU = os.path.join(REPO, "baseline", "_ref")
+GPU_SO = os.path.join(OUT_GPU, "libbpcuda_ref.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+CUDA_HOME = os.path.dirname(os.path.dirname(NVCC))
 OUT_REF = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(HERE, "libjfdk_oracle.so")
 REF_SO = os.path.join(OUT_REF, "libjref.so")
@@ -134,6 +150,62 @@ def build_ref(ref: str = REF_DEFAULT, force: bool = False) -> str | None:
     return REF_SO
 
 
+# The reference's GPU backprojector and the CUDA wrappers it uses.
+# CUDA/Tex2DFloat.cpp specialises Tex2D<float>'s members without `template<>`
+# (accepted by MSVC, rejected by g++); ref_gpu/tex2d_shim.cpp restates it.
+GPU_CU = ["BPCUDAAgent/BPCUDACore.cu"]
+GPU_CPP = ["BPCUDAAgent/BPCUDACore.cpp", "CUDA/DeviceMemory.cpp", "CUDA/ErrorChecking.cpp"]
+
+
+def build_ref_gpu(ref: str = REF_DEFAULT, force: bool = False) -> str | None:
+    """Compile the reference's BPCUDACore (unchanged, sm_100a) + the scalar
+    shims + the driver into baseline/_ref/libbpcuda_ref.so.  Returns the .so
+    path, or None when the reference tree is absent (an earlier build is
+    kept)."""
+    if not os.path.isdir(ref):
+        return GPU_SO if os.path.exists(GPU_SO) else None
+    shim = os.path.join(HERE, "ref_shims", "ipp_mkl_shims.cpp")
+    drv = os.path.join(HERE, "ref_gpu", "bpcuda_driver.cpp")
+    tex = os.path.join(HERE, "ref_gpu", "tex2d_shim.cpp")
+    deps = [os.path.join(ref, s) for s in GPU_CU + GPU_CPP] + [shim, drv, tex, os.path.join(HERE, "fdk_oracle.c")]
+    if (not force and os.path.exists(GPU_SO)
+            and all(os.path.getmtime(GPU_SO) >= os.path.getmtime(d) for d in deps)):
+        return GPU_SO
+    if not os.path.exists(os.path.join(OUT_REF, "inc")):
+        build_ref(ref)   # writes the forwarding headers the shims include
+    obj_dir = os.path.join(OUT_GPU, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    inc = ["-I", ref, "-I", os.path.join(CUDA_HOME, "include")]
+    force_inc = []
+    for h in FORCE_INCLUDES:
+        force_inc += ["-include", h]
+    cxx = ["g++", "-std=c++17", "-O2", "-fPIC", "-w"] + inc + force_inc
+    objs = []
+    for s in GPU_CU:
+        o = os.path.join(obj_dir, s.replace("/", "_") + ".o")
+        _run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-w", "-Xcompiler", "-fPIC"]
+             + inc + force_inc + ["-c", os.path.join(ref, s), "-o", o])
+        objs.append(o)
+    for s in GPU_CPP:
+        o = os.path.join(obj_dir, s.replace("/", "_") + ".o")
+        # DeviceMemory.cpp instantiates DeviceMemory<float> only through a
+        # sample function; without inlining the members are emitted out of line
+        extra = ["-fno-inline"] if s.endswith("DeviceMemory.cpp") else []
+        _run(cxx + extra + ["-c", os.path.join(ref, s), "-o", o])
+        objs.append(o)
+    for src, name in ((shim, "shim.o"), (drv, "driver.o"), (tex, "tex2d.o")):
+        o = os.path.join(obj_dir, name)
+        _run(cxx + ["-iquote", os.path.join(OUT_REF, "inc"), "-I", HERE, "-c", src, "-o", o])
+        objs.append(o)
+    o = os.path.join(obj_dir, "fdk_oracle.o")
+    _run(["gcc", "-std=c11", "-D_GNU_SOURCE", "-O2", "-fPIC", "-ffp-contract=off", "-w", "-c",
+          os.path.join(HERE, "fdk_oracle.c"), "-o", o])
+    objs.append(o)
+    _run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", GPU_SO] + objs +
+         ["-lpthread", "-lm"])
+    return GPU_SO
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=REF_DEFAULT)
@@ -141,6 +213,7 @@ def main() -> None:
     a = ap.parse_args()
     print(build_oracle(a.force))
     print(build_ref(a.reference, a.force))
+    print(build_ref_gpu(a.reference, a.force))
 
 
 if __name__ == "__main__":
