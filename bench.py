@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--zpt", type=int, default=0, help="slices per backprojection thread (0: form default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-gpu-baseline", action="store_true",
+                    help="skip timing the reference's own GPU backprojector (baseline/_ref)")
     ap.add_argument("--split", default="scans", choices=["scans", "zslab"],
                     help="scans: one independent scan per GPU (weak scaling); zslab: one volume, each GPU "
                          "filters 1/N of the views and backprojects 1/N of the slices (strong scaling)")
@@ -91,7 +93,10 @@ def workload_config(w):
                                                                           r.num_pixels_z],
             "voxel_mm": [r.pitch_xy, r.pitch_z], "sid_sdd_mm": [g.sid, g.sdd],
             "updates_per_volume": w.updates,
-            "l2": "inputs larger than L2 (raw frames, filtered store and volume each > 126 MB)"}
+            "l2": "inputs larger than L2 (raw frames, filtered store and volume each > 126 MB)"
+                  if w.updates > FULL_CPU_UPDATES else "L2 flushed before each timed step (256 MB write)",
+            "setup": "per-geometry setup (ramp operator, pre-weight table, u-taper) at context creation, outside "
+                     "the timed step"}
 
 
 class ClockSampler:
@@ -175,9 +180,28 @@ def profile_traffic(name: str):
     return None
 
 
-def cpu_sample(w, raw_np, filt_np, ptms, bounded=True):
-    """Reference CPU Cores on a bounded sample, extrapolated to one volume.
-    Returns (GUPS, cores, kind, sample description, seconds spent)."""
+FULL_CPU_UPDATES = 2_000_000_000   # workloads up to this many updates run whole on the CPU
+
+
+def cpu_full(w) -> bool:
+    """The CPU baseline runs the whole workload (not a sample) when it is
+    small enough to finish in seconds on the host (c1: 7.6e8 updates)."""
+    return w.updates <= FULL_CPU_UPDATES
+
+
+CPU_NOTES = {"ipp_mkl": "the reference's Cores compiled from source with scalar restatements of its Intel IPP / MKL "
+                        "calls (oracle/ref_shims; IPP and MKL are not in the image)",
+             "setup": "per-geometry setup (FilterCore spectrum, pre-weight generator, BPCore axes) outside the timed "
+                      "run, as the engine's context creation is outside its timed step"}
+
+
+def cpu_sample(w, raw_np, filt_np, ptms):
+    """The reference CPU Cores on the workload: all of it when cpu_full(w)
+    (raw_np holds every view), else a bounded sample -- preprocess + filter of
+    12 views, BPCore over 60 views of a 16-slice central slab (filt_np: those
+    60 views filtered) -- extrapolated linearly to one volume.
+    Returns (GUPS, cores, kind, sample description, seconds spent, seconds
+    per volume, extrapolated)."""
     import numpy as np
     try:
         from oracle.pyoracle import RefCores
@@ -187,40 +211,47 @@ def cpu_sample(w, raw_np, filt_np, ptms, bounded=True):
         impl, kind = Oracle(), "port"
     cores = os.cpu_count() or 1
     r, g = w.recon, w.geom
-    nv_f = min(12, g.n_views)
-    nv_b = min(60, g.n_views)
-    nz = min(16, r.num_pixels_z)
+    full = cpu_full(w)
+    nv_f = g.n_views if full else min(12, g.n_views)
+    nv_b = g.n_views if full else min(60, g.n_views)
+    nz = r.num_pixels_z if full else min(16, r.num_pixels_z)
     t0 = time.perf_counter()
     if kind == "reference":
         prep = impl.preprocess(raw_np[:nv_f], w.bright_field, w.beam_hardening, nthreads=cores)
         t1 = time.perf_counter()
-        impl.filter(prep, ptms, g.half_sample_rate, g.sid, nthreads=cores)
+        filt = impl.filter(prep, ptms, g.half_sample_rate, g.sid, nthreads=cores)
         t2 = time.perf_counter()
-        # BPCore over a z-slab: the reference backprojects the whole volume,
-        # whose cost is linear in slices; the slab is the first nz slices.
-        zmid = r.num_pixels_z // 2 - nz // 2
-        slab = _ref_bp_slab(impl, filt_np[:nv_b], ptms[:nv_b], r, nz, zmid, cores)
+        if full:
+            vol = impl.bp(filt, ptms, r.num_pixels_x, r.num_pixels_y, r.num_pixels_z, r.pitch_xy, r.pitch_z,
+                          nthreads=cores)
+        else:
+            # BPCore over a central z-slab: the reference backprojects the
+            # whole volume, whose cost is linear in slices
+            vol = _ref_bp_slab(impl, filt_np[:nv_b], ptms[:nv_b], r, nz, r.num_pixels_z // 2 - nz // 2, cores)
         t3 = time.perf_counter()
-        impl.ctnum(slab, r.ct_norm0, r.ct_norm1)
+        impl.ctnum(vol, r.ct_norm0, r.ct_norm1)
         t4 = time.perf_counter()
     else:
         prep = impl.preprocess(raw_np[:nv_f], w.bright_field, w.beam_hardening)
         t1 = time.perf_counter()
         H = impl.filter_spectrum(impl.fft_length(g.det_u), g.half_sample_rate)
-        for v in range(nv_f):
-            impl.filter_rows(prep[v], H, impl.fft_length(g.det_u))
+        filt = np.stack([impl.filter_rows(prep[v], H, impl.fft_length(g.det_u)) for v in range(nv_f)])
         t2 = time.perf_counter()
-        slab = impl.bp(filt_np[:nv_b], ptms[:nv_b], r.num_pixels_x, r.num_pixels_y, r.num_pixels_z,
-                       r.pitch_xy, r.pitch_z, z0=r.num_pixels_z // 2 - nz // 2, nz=nz, nthreads=cores)
+        vol = impl.bp(filt if full else filt_np[:nv_b], ptms[:nv_b], r.num_pixels_x, r.num_pixels_y,
+                      r.num_pixels_z, r.pitch_xy, r.pitch_z, z0=r.num_pixels_z // 2 - nz // 2, nz=nz,
+                      nthreads=cores)
         t3 = time.perf_counter()
-        impl.ctnum(slab, r.ct_norm0, r.ct_norm1)
+        impl.ctnum(vol, r.ct_norm0, r.ct_norm1)
         t4 = time.perf_counter()
     per_volume = ((t1 - t0) + (t2 - t1)) * g.n_views / nv_f + (t3 - t2) * (g.n_views / nv_b) * (
         r.num_pixels_z / nz) + (t4 - t3) * r.num_pixels_z / nz
-    sample = (f"preprocess+filter of {nv_f} views (x{g.n_views / nv_f:g}) and BP of {nv_b} views into "
-              f"{nz} of {r.num_pixels_z} slices (x{g.n_views / nv_b * r.num_pixels_z / nz:g}), "
-              f"extrapolated to one volume: {per_volume:.1f} s/volume")
-    return w.updates / per_volume / 1e9, cores, kind, sample, t4 - t0, per_volume
+    if full:
+        sample = f"the whole workload, not extrapolated: {per_volume:.2f} s/volume"
+    else:
+        sample = (f"preprocess+filter of {nv_f} views (x{g.n_views / nv_f:g}) and BP of {nv_b} views into "
+                  f"{nz} of {r.num_pixels_z} slices (x{g.n_views / nv_b * r.num_pixels_z / nz:g}), "
+                  f"extrapolated linearly to one volume: {per_volume:.1f} s/volume")
+    return w.updates / per_volume / 1e9, cores, kind, sample, t4 - t0, per_volume, not full
 
 
 def _ref_bp_slab(ref, filt, ptms, r, nz, z0, cores):
@@ -231,6 +262,93 @@ def _ref_bp_slab(ref, filt, ptms, r, nz, z0, cores):
     zc = (z0 + (nz - 1) / 2.0) - (r.num_pixels_z - 1) / 2.0
     p = np.stack([ref.ptm_modify(ptms[i], "move_z", float(np.float32(zc * r.pitch_z))) for i in range(len(ptms))])
     return ref.bp(filt, p, r.num_pixels_x, r.num_pixels_y, nz, r.pitch_xy, r.pitch_z, nthreads=cores)
+
+
+def error_sample(w):
+    """The voxels each form's error against the FP64 oracle is stated on:
+    (first slice, slices, stride in x and y) -- the 8 central slices, every
+    4th voxel in x and y (the whole volume for volumes of at most 2^21
+    voxels)."""
+    r = w.recon
+    if r.num_pixels_x * r.num_pixels_y * r.num_pixels_z <= 1 << 21:
+        return 0, r.num_pixels_z, 1
+    nz = min(8, r.num_pixels_z)
+    return r.num_pixels_z // 2 - nz // 2, nz, 4
+
+
+def fp64_errors(w, raw_np, samples):
+    """Error of each form's volume against the FP64 oracle on the error
+    sample (tests/fp64_fdk.py: the reference's float preprocessing and
+    pre-weight, then filter, backprojection and CT numbers in double):
+    rel-L2 of HU + 1000 and max |dHU| over the interior voxels (sampled at
+    least a pixel inside the detector by every view) and over all voxels."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from fp64_fdk import all_points, case_from_workload, errors, fdk_f64, survey
+    from oracle.pyoracle import Oracle
+    r = w.recon
+    z0, nz, stride = error_sample(w)
+    pts = all_points(r.num_pixels_x, r.num_pixels_y, r.num_pixels_z, z0=z0, nz=nz, stride=stride)
+    g = case_from_workload(w, raw_np)
+    ref = fdk_f64(Oracle(), g, pts)
+    inside = survey(g, pts)[0]
+    out = {}
+    for form, hu in samples.items():
+        e = errors(np.asarray(hu, np.float64).ravel(), ref, inside)
+        out[form] = {"rel_l2": e["rel_l2_interior"], "max_hu": e["max_hu_interior"], "rel_l2_all": e["rel_l2_all"],
+                     "max_hu_all": e["max_hu_all"], "voxels": e["voxels"], "interior_voxels": e["interior_voxels"]}
+    out["sample"] = (f"slices {z0}..{z0 + nz - 1}, every {stride}th voxel in x and y" if stride > 1 else
+                     f"slices {z0}..{z0 + nz - 1}, every voxel")
+    out["oracle"] = ("FP64 FDK (tests/fp64_fdk.py): float preprocessing and pre-weight as the reference, then "
+                     "filter, taper, coordinates, lerps, sums and CT numbers in double; rel_l2 / max_hu over the "
+                     "interior voxels, *_all over every voxel")
+    return out
+
+
+def gpu_baseline(w, raw, ptms, local):
+    """The reference's own GPU backprojector (BPCUDAAgent/BPCUDACore.cu,
+    compiled unchanged for sm_100a into baseline/_ref by oracle/build.py)
+    through the host loop BPCUDAAgent drives it with: per view three Scale
+    kernels and a stream sync (PreCalculate_Synced), the BackProject kernel
+    (a texture fetch and a global read-modify-write of the volume per voxel)
+    and a sync; then per slice the host-side FP16 weight expansion, its upload
+    and the Div2 kernel.  Fed the engine's own filtered projections, one part
+    (the volume fits).  Host-timed: the reference synchronises after every
+    kernel.  None when the library is not built."""
+    import ctypes as C
+    import numpy as np
+    from jenhine_b200.fdk import FDKEngine
+    path = os.path.join(ROOT, "baseline", "_ref", "libbpcuda_ref.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    lib.jrefgpu_bp.restype = C.c_int
+    lib.jrefgpu_last_error.restype = C.c_char_p
+    g, r = w.geom, w.recon
+    eng = FDKEngine(w.scan, w.recon, ptms)
+    filt = np.empty((g.n_views, eng.rows, eng.filter_out_w), np.float32)
+    for v0 in range(0, g.n_views, 100):
+        filt[v0:v0 + 100] = eng.filter(eng.preprocess(raw[v0:v0 + 100]), v0).cpu().numpy()
+    eng.close()
+    t = (C.c_double * 3)()
+    P = np.ascontiguousarray(ptms, np.float32)
+    clocks = ClockSampler(local)
+    clocks.start()
+    st = lib.jrefgpu_bp(None, filt.ctypes.data_as(C.c_void_p), P.ctypes.data_as(C.c_void_p), g.n_views,
+                        eng.filter_out_w, eng.rows, r.num_pixels_x, r.num_pixels_y, r.num_pixels_z,
+                        C.c_float(r.pitch_xy), C.c_float(r.pitch_z), 1, 2, t)
+    clk = clocks.stop()
+    if st != 0:
+        return {"unavailable": "reference GPU backprojector failed: " + lib.jrefgpu_last_error().decode()}
+    return {"value": w.updates / (t[0] / 1000.0) / 1e9, "unit": "GUPS", "backprojection_ms": t[0],
+            "normalise_output_ms": t[1], "setup_ms": t[2],
+            "kernel": "reference BPCUDACore (BPCUDAAgent/BPCUDACore.cu) compiled unchanged for sm_100a, driven by "
+                      "BPCUDAAgent's loop (oracle/ref_gpu/bpcuda_driver.cpp)",
+            "timed": "backprojection_ms: every view (PreCalculate_Synced, DeployBackProj, SyncBackProj); value = "
+                     "updates / backprojection_ms, comparable with stages_ms.backprojection_hu; normalise_output_ms: "
+                     "every slice (DeployUpdateOutput, SyncUpdateOutput); setup_ms (not in value): texture uploads "
+                     "and the weight pass the reference caches in a file",
+            "clocks": clk}
 
 
 def time_zslab(a, w, raw, ptms, precision, dist, rank, world, local):
@@ -275,23 +393,24 @@ def run_reference(a, w, rank, world):
     """--impl reference: the reference CPU implementation, rank 0 only."""
     if rank != 0:
         return
-    import numpy as np
     from jenhine_b200.phantom import line_integrals, raw_frames
     g = w.geom
     ptms = g.ptms()
-    # inputs for the sample: raw frames of the first views and filtered views
-    nv = min(60, g.n_views)
+    full = cpu_full(w)
+    # inputs: every view (whole run), or the first views (bounded sample)
+    nv = g.n_views if full else min(60, g.n_views)
     lint = line_integrals(g, w.phantom(), views=range(nv))
     raw = raw_frames(lint, g.seed + 2, i0=w.i0, bright_field=w.bright_field, gain_spread=w.gain_spread,
                      offset_max=w.offset_max)
-    from oracle.pyoracle import Oracle
-    o = Oracle()
-    prep = o.preprocess(raw, w.bright_field, w.beam_hardening)
-    H = o.filter_spectrum(o.fft_length(g.det_u), g.half_sample_rate)
-    filt = np.stack([o.filter_rows(prep[v], H, o.fft_length(g.det_u)) for v in range(nv)])
+    filt = None
+    if not full:   # the BP sample's filtered views, from the reference Cores
+        from oracle.pyoracle import RefCores
+        ref = RefCores()
+        prep = ref.preprocess(raw, w.bright_field, w.beam_hardening, nthreads=os.cpu_count() or 1)
+        filt = ref.filter(prep, ptms, g.half_sample_rate, g.sid, nthreads=os.cpu_count() or 1)
     vals, secs = [], []
     for i in range(a.warmup + a.steps):
-        gups, cores, kind, sample, spent, per_volume = cpu_sample(w, raw, filt, ptms)
+        gups, cores, kind, sample, spent, per_volume, extrap = cpu_sample(w, raw, filt, ptms)
         if i >= a.warmup:
             vals.append(gups)
             secs.append(per_volume)
@@ -300,7 +419,8 @@ def run_reference(a, w, rank, world):
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": statistics.median(secs) * 1000.0,
             "s_per_volume": statistics.median(secs), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": DATA, "config": workload_config(w),
-            "cpu_baseline": {"value": value, "unit": "GUPS", "cores": cores, "kind": kind, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "GUPS", "cores": cores, "kind": kind, "sample": sample,
+                             "extrapolated": extrap, **CPU_NOTES},
             "e2e": {"value": value, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -327,24 +447,38 @@ def time_form(a, w, raw, ptms, precision, dist, world, local):
     launches0 = eng.kernel_launches
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     stage_ms = []
+    # a workload whose inputs partly fit in L2 gets L2 flushed before each
+    # step (a 256 MB write, outside the step's events)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if w.updates <= FULL_CPU_UPDATES else None
+    step_ms = 0.0
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     start.record()
     for _ in range(a.steps):
+        if flush is not None:
+            flush.fill_(1)
+            s1, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s1.record()
         eng.reconstruct(raw, vol)
-        stage_ms.append(eng.stage_times())   # events on the engine's stream
+        if flush is not None:
+            e1.record()
+        stage_ms.append(eng.stage_times())   # events on the engine's stream (synchronises)
+        if flush is not None:
+            step_ms += s1.elapsed_time(e1)
     end.record()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     launches = eng.kernel_launches - launches0
     clk = clocks.stop()
-    ms = max_over_ranks(dist, start.elapsed_time(end) / a.steps)
+    ms = max_over_ranks(dist, (step_ms if flush is not None else start.elapsed_time(end)) / a.steps)
+    z0, nz, stride = error_sample(w)
+    sample = vol[z0:z0 + nz, ::stride, ::stride].cpu().numpy()
     out = {"value": w.updates * world / (ms / 1000.0) / 1e9, "ms_per_step": ms, "s_per_volume": ms / 1000.0,
            "stages_ms": {"preprocess_weight_filter": statistics.mean(s[0] for s in stage_ms),
                          "backprojection_hu": statistics.mean(s[2] for s in stage_ms)},
-           "gpu_launches": launches, "clocks": clk}
+           "gpu_launches": launches, "clocks": clk, "_sample": sample}
 
     # end to end through the host-buffer call, pinned memory
     if not a.no_e2e:
@@ -629,6 +763,7 @@ def main():
     raw = w.raw_torch()
     ptms = w.geom.ptms()
     res = {f: time_form(a, w, raw, ptms, f, dist, world, local) for f in forms}
+    samples = {f: res[f].pop("_sample") for f in forms}
 
     if rank == 0:
         head = res[forms[0]]
@@ -659,17 +794,31 @@ def main():
                                      proj_bytes=2)
             m["speedup_vs_fp32"] = head["ms_per_step"] / m["ms_per_step"]
             line["forms"] = {"fp32": {k: v for k, v in head.items()}, "mixed": m}
+        if not a.no_gpu_baseline and world == 1 and not w.composite:
+            gb = gpu_baseline(w, raw, ptms, local)
+            if gb is not None:
+                line["gpu_baseline"] = gb
         if not a.no_cpu_baseline and world == 1 and not w.composite:
+            # the CPU leg (rank 0, one GPU): the reference Cores timed on the
+            # host, and each form's error against the FP64 oracle
             from jenhine_b200.fdk import FDKEngine
             g = w.geom
-            nvb = min(60, g.n_views)
-            eng = FDKEngine(w.scan, w.recon, ptms)
-            raw_np = raw[:12].cpu().numpy()
-            filt = eng.filter(eng.preprocess(raw[:nvb]), 0).cpu().numpy()
-            eng.close()
-            gups, cores, kind, sample, spent, _ = cpu_sample(w, raw_np, filt, ptms)
+            full = cpu_full(w)
+            nvb = g.n_views if full else min(60, g.n_views)
+            raw_np = raw.cpu().numpy() if full else raw[:12].cpu().numpy()
+            filt = None
+            if not full:
+                eng = FDKEngine(w.scan, w.recon, ptms)
+                filt = eng.filter(eng.preprocess(raw[:nvb]), 0).cpu().numpy()
+                eng.close()
+            gups, cores, kind, sample, spent, _, extrap = cpu_sample(w, raw_np, filt, ptms)
             line["cpu_baseline"] = {"value": gups, "unit": "GUPS", "cores": cores, "kind": kind,
-                                    "sample": sample, "seconds": spent}
+                                    "sample": sample, "seconds": spent, "extrapolated": extrap, **CPU_NOTES}
+            errs = fp64_errors(w, raw.cpu().numpy(), samples)
+            line["error_vs_fp64"] = {"sample": errs["sample"], "oracle": errs["oracle"], **errs[forms[0]]}
+            if len(forms) == 2:
+                line["forms"]["mixed"]["error_vs_fp64"] = errs["mixed"]
+                line["forms"]["fp32"]["error_vs_fp64"] = errs["fp32"]
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
