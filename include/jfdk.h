@@ -215,6 +215,17 @@ jfdk_status jfdk_reconstruct_host(jfdk_ctx* ctx, const uint16_t* h_raw, float* h
  * slices from every view (jfdk_backproject_store).  Results equal
  * jfdk_reconstruct's bit for bit when the slabs start at multiples of the
  * tile depth (JFDK_OPT_BP_ZPT; 8 by default). */
+/* The filter stage of jfdk_reconstruct for views [v0, v0+nv) of the
+ * rotation -- preprocessing (and compositing), pre-weight, ramp filter,
+ * z-filter -- into caller-owned filtered frames: d_raw the rotation's frames
+ * (num_views x NumDetsV x NumDetsU uint16; only these views, and their
+ * conjugates when compositing, are read), d_frames nv x rows x filter_out_w
+ * float.  A z-slab rank filters its share of the views with it; the frames
+ * of all views (4 bytes a pixel) are then exchanged and each rank
+ * backprojects them into its slab with jfdk_bp_set_slab / jfdk_bp_reset /
+ * jfdk_bp_accumulate (views in order) / jfdk_finalize, which equals
+ * jfdk_reconstruct on those slices bit for bit. */
+jfdk_status jfdk_filter_raw(jfdk_ctx* ctx, const uint16_t* d_raw, int v0, int nv, float* d_frames);
 /* Filter views [v0, v0+nv) into the store.  d_raw: the rotation's frames
  * (num_views x NumDetsV x NumDetsU uint16); only the frames of these views
  * (and, when compositing, of their conjugates) are read. */
@@ -318,10 +329,10 @@ jfdk_status jfdk_autotune(jfdk_ctx* ctx, int flags);
 /* A batch of scans (one context each, all of the same form) reconstructed
  * together, on one of two schedules:
  *  - persistent: every scan's filter stage, then ONE persistent
- *    backprojection launch over the tiles of up to 8 scans (scans in order;
+ *    backprojection launch over the tiles of up to 16 scans (scans in order;
  *    a CTA takes the next tile when it finishes one, so scans of uneven size
- *    leave no tail; consecutive scans of another tile depth or W(z) start a
- *    new launch);
+ *    leave no tail; each scan keeps its own tile depth; consecutive scans
+ *    whose W does not depend on z the same way start a new launch);
  *  - pipelined: each scan's own backprojection launch, the filter stage of
  *    the next scan running beside it on a second stream.
  * JFDK_BATCH_AUTOTUNE tunes each context (jfdk_autotune) and, on the first

@@ -1,8 +1,8 @@
 // batch.cpp -- several scans through one pipeline, on one of two schedules:
 // persistent (every scan's filter stage, then persistent backprojection
 // launches over the tiles of all scans -- bp_batch_kernel, one launch per run
-// of up to 8 consecutive scans that share the tile depth and W's
-// z-dependence) or pipelined (each scan's own backprojection, the next
+// of up to 16 consecutive scans that share W's z-dependence, each scan with
+// its own tile depth) or pipelined (each scan's own backprojection, the next
 // scan's filter stage beside it on a second stream); optionally recorded
 // once as a CUDA graph and replayed.
 #include <cuda_runtime.h>
@@ -25,7 +25,7 @@ struct jfdk_batch {
     bool own_stream = false;
     struct Group {                      // one persistent launch
         BatchSlots slots;
-        int n, zpt, wz, ctas;
+        int n, wz, ctas;
         unsigned total;
     };
     std::vector<Group> groups;
@@ -67,8 +67,8 @@ void drop_graph(jfdk_batch* b) {
 
 // Scan descriptors for the given outputs: each scan's finalizing BP params,
 // its grid of kBPTileX x kBPTileY x ZPT tiles and its first tile in its group's
-// work list; consecutive scans with the same tile depth and W(z) share a
-// group of up to kBatchSlots.
+// work list; consecutive scans with the same W(z) share a group of up to
+// kBatchSlots.
 jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
     b->groups.clear();
     for (size_t i = 0; i < b->ctx.size(); ++i) {
@@ -81,13 +81,11 @@ jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
         s.gx = (c->X + kBPTileX - 1) / kBPTileX;
         s.gy = (c->Y + kBPTileY - 1) / kBPTileY;
         s.gz = (c->Z + s.zpt - 1) / s.zpt;
-        if (b->groups.empty() || b->groups.back().n == kBatchSlots || b->groups.back().zpt != s.zpt ||
-            b->groups.back().wz != s.wz) {
+        if (b->groups.empty() || b->groups.back().n == kBatchSlots || b->groups.back().wz != s.wz) {
             jfdk_batch::Group g;
             std::memset(&g, 0, sizeof g);
-            g.zpt = s.zpt;
             g.wz = s.wz;
-            BATCH_CUDA(b, bp_batch_ctas(b->mixed != 0, g.zpt, g.wz != 0, &g.ctas), "occupancy query");
+            BATCH_CUDA(b, bp_batch_ctas(b->mixed != 0, g.wz != 0, &g.ctas), "occupancy query");
             b->groups.push_back(g);
         }
         jfdk_batch::Group& g = b->groups.back();
@@ -111,7 +109,7 @@ jfdk_status enqueue_persistent(jfdk_batch* b, const uint16_t* const* d_raw) {
     }
     for (size_t k = 0; k < b->groups.size(); ++k) {
         const jfdk_batch::Group& g = b->groups[k];
-        BATCH_CUDA(b, launch_bp_batch(g.slots, g.n, g.total, b->mixed != 0, g.zpt, g.wz != 0, b->d_counter + k, g.ctas,
+        BATCH_CUDA(b, launch_bp_batch(g.slots, g.n, g.total, b->mixed != 0, g.wz != 0, b->d_counter + k, g.ctas,
                                       b->stream),
                    "batched backprojection");
         ++b->launches;

@@ -49,14 +49,17 @@ namespace {
 
 constexpr int kBPThreads = kBPTileX * kBPTileY;
 
-// Resident CTAs per SM the compiler must allow for: 8 slices per thread fit
-// in 64 registers at 32 warps per SM, which measured faster than the
-// 80-register allocation the compiler picks unconstrained.  Small CTAs
-// (4 warps, 8 per SM) measured 4 % faster than 8-warp ones: a finishing CTA
-// leaves fewer warps idle while the SM waits for the next.  Each warp covers
-// 4 x 8 voxels in (x, y) rather than a row of 32: its sample points spread
-// less on the detector (1.5-1.7 % faster than 32 x 1 in both forms).
+// Resident CTAs per SM the compiler must allow for, with 8 slices per
+// thread: the mixed form fits 64 registers at 32 warps per SM (8 CTAs), which
+// measured faster than 80 registers at 24 warps (102 vs 120 ms on c2); the
+// FP32 form measured the other way round (160.6 ms at 80 registers and 24
+// warps against 164.0 ms at 64 and 32).  Small CTAs (4 warps) measured 4 %
+// faster than 8-warp ones: a finishing CTA leaves fewer warps idle while the
+// SM waits for the next.  Each warp covers 4 x 8 voxels in (x, y) rather than
+// a row of 32: its sample points spread less on the detector (1.5-1.7 %
+// faster than 32 x 1 in both forms).
 constexpr int bp_min_blocks(int zpt) { return zpt == 8 ? 1024 / kBPThreads : 1; }
+constexpr int bp_fp32_min_blocks(int zpt) { return zpt == 8 ? 6 : 1; }
 
 // Where a CTA's tile lies: the launch grid's block index for the per-scan
 // kernels, the current work item of the batch kernel.  The tile bodies ask
@@ -305,7 +308,7 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& ti
 
 // One CTA = one TX x (128 / TX) x ZPT voxel tile of one launch's grid.
 template <int ZPT, bool FINALIZE, bool EXACT, bool WZ, int TX>
-__global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_kernel(BPParams p) {
+__global__ void __launch_bounds__(kBPThreads, bp_fp32_min_blocks(ZPT)) bp_kernel(BPParams p) {
     bp_block<ZPT, FINALIZE, EXACT, WZ>(p, GridTile<TX>{});
 }
 
@@ -324,22 +327,41 @@ __global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_mixed_kerne
 // parameters sit at a fixed offset of the kernel's parameter space (slot S,
 // a compile-time index), so the tile body reads them as constant operands
 // exactly as the single-scan kernels do; a shared-memory or indexed copy of
-// them measured 16-27 % slower at the 64-register bound.  The next tile's
-// index is fetched while the current one runs.
-template <int S, bool MIXED, int ZPT, bool WZ>
+// them measured 16-27 % slower at the 64-register bound.  Each slot holds its
+// scan's own tile depth (4 or 8 slices, a uniform branch per tile), so scans
+// tuned to either depth share the launch.  The next tile's index is fetched
+// while the current one runs.
+template <int S, bool MIXED, bool WZ>
 __device__ __forceinline__ void batch_slot_tile(const BatchSlots& t) {
     const BatchTile tile{t.s[S]};
-    if (MIXED)
-        bp_mixed_block<ZPT, true, WZ>(t.s[S].p, tile);
-    else
-        bp_block<ZPT, true, false, WZ>(t.s[S].p, tile);
+    if (t.s[S].zpt == 8) {
+        if (MIXED)
+            bp_mixed_block<8, true, WZ>(t.s[S].p, tile);
+        else
+            bp_block<8, true, false, WZ>(t.s[S].p, tile);
+    } else {
+        if (MIXED)
+            bp_mixed_block<4, true, WZ>(t.s[S].p, tile);
+        else
+            bp_block<4, true, false, WZ>(t.s[S].p, tile);
+    }
 }
 
-template <bool MIXED, int ZPT, bool WZ>
-__global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT))
+// The tile of slot si (si < kBatchSlots): a compile-time slot per case.
+template <int S, bool MIXED, bool WZ>
+__device__ __forceinline__ void batch_dispatch(const BatchSlots& t, int si) {
+    if constexpr (S < kBatchSlots) {
+        if (si == S)
+            batch_slot_tile<S, MIXED, WZ>(t);
+        else
+            batch_dispatch<S + 1, MIXED, WZ>(t, si);
+    }
+}
+
+template <bool MIXED, bool WZ>
+__global__ void __launch_bounds__(kBPThreads, bp_min_blocks(8))
     bp_batch_kernel(const __grid_constant__ BatchSlots t, int nscans, unsigned* __restrict__ counter,
                     unsigned total) {
-    static_assert(kBatchSlots == 8, "one case per slot below");
     __shared__ unsigned s_next;
     const int tid = threadIdx.y * kBPTileX + threadIdx.x;
     if (tid == 0) g_batch_tile = atomicAdd(counter, 1u);
@@ -350,16 +372,7 @@ __global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT))
         if (tid == 0) s_next = atomicAdd(counter, 1u);   // the next tile, while this one runs
         int si = 0;
         while (si + 1 < nscans && it >= t.s[si + 1].first_tile) ++si;
-        switch (si) {
-            case 0: batch_slot_tile<0, MIXED, ZPT, WZ>(t); break;
-            case 1: batch_slot_tile<1, MIXED, ZPT, WZ>(t); break;
-            case 2: batch_slot_tile<2, MIXED, ZPT, WZ>(t); break;
-            case 3: batch_slot_tile<3, MIXED, ZPT, WZ>(t); break;
-            case 4: batch_slot_tile<4, MIXED, ZPT, WZ>(t); break;
-            case 5: batch_slot_tile<5, MIXED, ZPT, WZ>(t); break;
-            case 6: batch_slot_tile<6, MIXED, ZPT, WZ>(t); break;
-            default: batch_slot_tile<7, MIXED, ZPT, WZ>(t); break;
-        }
+        batch_dispatch<0, MIXED, WZ>(t, si);
         __syncthreads();   // every thread is done with the current tile
         if (tid == 0) g_batch_tile = s_next;
         __syncthreads();
@@ -586,50 +599,40 @@ cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_
 
 namespace {
 
-template <bool M, int Z, bool W>
+template <bool M, bool W>
 cudaError_t batch_go(const BatchSlots& t, int nscans, unsigned total, unsigned* counter, int ctas, cudaStream_t s) {
-    bp_batch_kernel<M, Z, W><<<ctas, dim3(kBPTileX, kBPTileY), 0, s>>>(t, nscans, counter, total);
+    bp_batch_kernel<M, W><<<ctas, dim3(kBPTileX, kBPTileY), 0, s>>>(t, nscans, counter, total);
     return cudaGetLastError();
 }
 
-template <bool M, int Z, bool W>
+template <bool M, bool W>
 cudaError_t batch_occ(int* per) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, bp_batch_kernel<M, Z, W>, kBPThreads, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, bp_batch_kernel<M, W>, kBPThreads, 0);
 }
 
 }  // namespace
 
-cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tiles, bool mixed_form, int zpt, bool wz,
+cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tiles, bool mixed_form, bool wz,
                             unsigned* counter, int ctas, cudaStream_t s) {
-    if (nscans < 1 || nscans > kBatchSlots || (zpt != 4 && zpt != 8)) return cudaErrorInvalidValue;
+    if (nscans < 1 || nscans > kBatchSlots) return cudaErrorInvalidValue;
+    for (int i = 0; i < nscans; ++i)
+        if (t.s[i].zpt != 4 && t.s[i].zpt != 8) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
-    const bool z8 = zpt == 8;
-    if (mixed_form) {
-        if (z8) return wz ? batch_go<true, 8, true>(t, nscans, total_tiles, counter, ctas, s)
-                          : batch_go<true, 8, false>(t, nscans, total_tiles, counter, ctas, s);
-        return wz ? batch_go<true, 4, true>(t, nscans, total_tiles, counter, ctas, s)
-                  : batch_go<true, 4, false>(t, nscans, total_tiles, counter, ctas, s);
-    }
-    if (z8) return wz ? batch_go<false, 8, true>(t, nscans, total_tiles, counter, ctas, s)
-                      : batch_go<false, 8, false>(t, nscans, total_tiles, counter, ctas, s);
-    return wz ? batch_go<false, 4, true>(t, nscans, total_tiles, counter, ctas, s)
-              : batch_go<false, 4, false>(t, nscans, total_tiles, counter, ctas, s);
+    if (mixed_form)
+        return wz ? batch_go<true, true>(t, nscans, total_tiles, counter, ctas, s)
+                  : batch_go<true, false>(t, nscans, total_tiles, counter, ctas, s);
+    return wz ? batch_go<false, true>(t, nscans, total_tiles, counter, ctas, s)
+              : batch_go<false, false>(t, nscans, total_tiles, counter, ctas, s);
 }
 
-cudaError_t bp_batch_ctas(bool mixed_form, int zpt, bool wz, int* ctas) {
+cudaError_t bp_batch_ctas(bool mixed_form, bool wz, int* ctas) {
     int dev = 0, sms = 0, per = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) {
-        const bool z8 = zpt == 8;
-        if (mixed_form)
-            e = z8 ? (wz ? batch_occ<true, 8, true>(&per) : batch_occ<true, 8, false>(&per))
-                   : (wz ? batch_occ<true, 4, true>(&per) : batch_occ<true, 4, false>(&per));
-        else
-            e = z8 ? (wz ? batch_occ<false, 8, true>(&per) : batch_occ<false, 8, false>(&per))
-                   : (wz ? batch_occ<false, 4, true>(&per) : batch_occ<false, 4, false>(&per));
-    }
+    if (e == cudaSuccess)
+        e = mixed_form ? (wz ? batch_occ<true, true>(&per) : batch_occ<true, false>(&per))
+                       : (wz ? batch_occ<false, true>(&per) : batch_occ<false, false>(&per));
     *ctas = sms * (per > 0 ? per : 1);
     return e;
 }

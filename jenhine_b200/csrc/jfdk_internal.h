@@ -81,18 +81,19 @@ struct BatchScan {
 cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, int tile_x,
                       cudaStream_t s);
 // A batched backprojection launch covers up to kBatchSlots scans that share
-// the tile depth and whether W depends on z; their parameters travel in the
-// kernel's parameter space.
-constexpr int kBatchSlots = 8;
+// whether W depends on z (each with its own tile depth, 4 or 8 slices); their
+// parameters travel in the kernel's parameter space (16 slots: ~4.4 KB of the
+// 32 KB a launch may carry).
+constexpr int kBatchSlots = 16;
 struct BatchSlots {
     BatchScan s[kBatchSlots];
 };
 // All tiles of nscans scans in one persistent launch of `ctas` CTAs (the
 // SMs' resident CTAs); *counter is the work-list cursor (cleared here).
-cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tiles, bool mixed_form, int zpt, bool wz,
+cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tiles, bool mixed_form, bool wz,
                             unsigned* counter, int ctas, cudaStream_t s);
 // CTAs of a full persistent wave: SMs x resident CTAs per SM.
-cudaError_t bp_batch_ctas(bool mixed_form, int zpt, bool wz, int* ctas);
+cudaError_t bp_batch_ctas(bool mixed_form, bool wz, int* ctas);
 // Mixed-precision form: FP16 footprints with a per-view scale (qh, qscale).
 cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, int tile_x,
                             cudaStream_t s);

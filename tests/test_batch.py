@@ -79,3 +79,26 @@ def test_batch_rejects_mixed_forms(torch_cuda):
     b = make_scans("mixed", SHAPES[:1])
     with pytest.raises(_lib.JfdkError):
         FDKBatch([a[0][1], b[0][1]], autotune=False)
+
+
+def test_sixteen_uneven_scans_in_one_persistent_launch(torch_cuda):
+    """16 scans of uneven size (views, detectors and volumes drawn from the
+    four shapes, tile depths 4 and 8 mixed): one persistent backprojection
+    launch, every volume equal to the scan's own reconstruction."""
+    torch = torch_cuda
+    from jenhine_b200 import _lib
+    from jenhine_b200.fdk import FDKBatch
+    shapes = [SHAPES[i % 4] for i in range(16)]
+    for precision in ("fp32", "mixed"):
+        scans = make_scans(precision, shapes)
+        for i, (_, e, _) in enumerate(scans):
+            e.set_option(_lib.OPT_BP_ZPT, 4 if i % 3 == 0 else 8)
+        refs = [e.reconstruct(raw).clone() for _, e, raw in scans]
+        batch = FDKBatch([e for _, e, _ in scans], autotune=False, graph=False, schedule="persistent")
+        outs = [torch.full_like(r, -7.0) for r in refs]
+        n0 = batch.launches
+        batch.run([raw for _, _, raw in scans], outs)
+        torch.cuda.synchronize()
+        assert batch.launches - n0 == 1
+        assert all(same(torch, o, r) for o, r in zip(outs, refs))
+        batch.close()
