@@ -353,9 +353,11 @@ def gpu_baseline(w, raw, ptms, local):
 
 def time_zslab(a, w, raw, ptms, precision, dist, rank, world, local):
     """One volume over the job's GPUs (jenhine_b200.zslab): per step each rank
-    filters its share of the views, the projection stores are completed by
-    broadcasts over NVLink, and each rank backprojects its slab.  Device-timed,
-    max over ranks; value = one volume's updates per second."""
+    filters its share of the views, the FP32 filtered frames of every view
+    reach every rank by broadcasts over NVLink (overlapped with the
+    backprojection of the views already there), and each rank backprojects
+    its slab.  Device-timed, max over ranks; value = one volume's updates per
+    second."""
     import torch
     from jenhine_b200.fdk import FDKEngine
     from jenhine_b200.zslab import reconstruct_zslab, slab_ranges
@@ -363,8 +365,9 @@ def time_zslab(a, w, raw, ptms, precision, dist, rank, world, local):
     r = w.recon
     z0, nz = slab_ranges(r.num_pixels_z, world)[rank]
     out = torch.empty((max(nz, 1), r.num_pixels_y, r.num_pixels_x), dtype=torch.float32, device="cuda")
+    frames = torch.empty((w.geom.n_views, eng.rows, eng.filter_out_w), dtype=torch.float32, device="cuda")
     for _ in range(a.warmup):
-        reconstruct_zslab(eng, raw, rank, world, out=out[:nz] if nz else None)
+        reconstruct_zslab(eng, raw, rank, world, out=out[:nz] if nz else None, frames=frames)
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
@@ -376,7 +379,7 @@ def time_zslab(a, w, raw, ptms, precision, dist, rank, world, local):
     torch.cuda.synchronize()
     start.record()
     for _ in range(a.steps):
-        reconstruct_zslab(eng, raw, rank, world, out=out[:nz] if nz else None)
+        reconstruct_zslab(eng, raw, rank, world, out=out[:nz] if nz else None, frames=frames)
     end.record()
     torch.cuda.synchronize()
     if dist:
@@ -386,7 +389,8 @@ def time_zslab(a, w, raw, ptms, precision, dist, rank, world, local):
     launches = eng.kernel_launches - l0
     eng.close()
     return {"value": w.updates / (ms / 1000.0) / 1e9, "ms_per_step": ms, "s_per_volume": ms / 1000.0,
-            "gpu_launches": launches, "clocks": clk}
+            "gpu_launches": launches, "clocks": clk,
+            "exchange_bytes_per_step": int(frames.numel() * 4) if world > 1 else 0}
 
 
 def run_reference(a, w, rank, world):
@@ -506,24 +510,62 @@ def time_form(a, w, raw, ptms, precision, dist, world, local):
     return out
 
 
-def roofline(w, bp_ms, kernel, prof, proj_bytes=4):
-    """HBM roofline of the backprojection kernel: algorithmic bytes (the
-    filtered projections read once at proj_bytes per sample, the volume
-    written once) over its CUDA-event time."""
-    peak, peak_kind = measured_peaks()
+def gather_ceiling(record_bytes: int, with_taper: bool, distinct: int, warps_per_sm: int = 32):
+    """Samples per second the load path delivers for the backprojector's
+    fetch pattern (jfdk_measure_gather_rate, measured here on this GPU)."""
+    import ctypes as C
+    from jenhine_b200 import _lib
+    r = C.c_double()
+    st = _lib.load().jfdk_measure_gather_rate(record_bytes, int(with_taper), distinct, warps_per_sm, C.byref(r))
+    return r.value if st == 0 else None
+
+
+def roofline(w, bp_ms, form, clocks):
+    """The backprojector (the dominant kernel) against the bounds that bind
+    it, from its CUDA-event time:
+      issue  -- SMs x 4 schedulers x the SM clock sampled during the run,
+                over the warp instructions it issues per 32 updates (ncu, the
+                same build, profiles/<kernel>_c2_chunks.md);
+      gather -- the samples per second the load path delivers for its fetch
+                pattern (record bytes, taper pair, records per warp request
+                from the same profile), measured live by a microbenchmark;
+      hbm    -- algorithmic bytes (filtered projections read once at 4 bytes
+                (FP32) or 2 bytes (FP16) a pixel, the volume written once)
+                against the measured copy bandwidth, with the DRAM traffic
+                of a full-size launch (ncu, profiles/<kernel>_c2.md).
+    frac is the issue fraction: the kernel's binding bound."""
+    import torch
+    kernel = "bp_kernel" if form == "fp32" else "bp_mixed_kernel"
+    prof = f"{kernel}_{w.name}"
     r, g = w.recon, w.geom
-    alg = g.n_views * g.det_v * g.det_u * proj_bytes + r.num_pixels_x * r.num_pixels_y * r.num_pixels_z * 4
-    achieved = alg / (bp_ms / 1000.0) / 1e9
-    return {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs ({'of measured' if peak_kind == 'measured' else 'of fallback'})",
-            "algorithmic_bytes_per_launch": alg, "traffic": profile_traffic(prof),
-            "note": "the backprojector is bound by instruction issue and L1 traffic (its footprint reads "
-                    "hit L1/L2), not by HBM: frac shows the distance to the memory floor",
-            "sm_bound": {"issue_active": profile_figure(prof.replace("_c2", "_c2_slab"), "issue_active"),
-                         "l1_data_pipe_wavefronts": profile_figure(prof.replace("_c2", "_c2_slab"),
-                                                                   "l1_data_pipe_wavefronts"),
-                         "unit": "fraction of peak (ncu, c2 slab)",
-                         "source": f"profiles/{prof.replace('_c2', '_c2_slab')}.md"}}
+    gups = w.updates / (bp_ms / 1000.0) / 1e9
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    w32 = profile_figure(f"{kernel}_c2_chunks", "warp_instructions_per_32_updates")
+    rec_bytes = 16 if form == "fp32" else 8
+    per_req = profile_figure(f"{kernel}_c2_chunks", "records_per_request") or 6.0
+    gather = gather_ceiling(rec_bytes, True, max(1, min(32, int(round(per_req)))))
+    peak, peak_kind = measured_peaks()
+    alg = g.n_views * g.det_v * g.det_u * (4 if form == "fp32" else 2) + r.num_pixels_x * r.num_pixels_y * \
+        r.num_pixels_z * 4
+    hbm = alg / (bp_ms / 1000.0) / 1e9
+    out = {"kernel": f"{kernel} (backprojection + normalisation + CT numbers)", "bound": "issue",
+           "achieved": gups, "unit": "GUPS (voxel-view updates/s)"}
+    if w32:
+        ceiling = sms * 4 * mhz * 1e6 * 32.0 / w32 / 1e9
+        out.update({"peak": ceiling, "frac": gups / ceiling,
+                    "peak_source": f"issue ceiling: {sms} SMs x 4 schedulers x {mhz:.0f} MHz (sampled) / {w32:.2f} "
+                                   f"warp instructions per 32 updates (ncu, profiles/{kernel}_c2_chunks.md)"})
+    else:
+        out.update({"peak": None, "frac": None, "peak_source": "no instruction count committed for this kernel"})
+    out["gather"] = {"peak": gather / 1e9 if gather else None, "achieved": gups,
+                     "frac": gups / (gather / 1e9) if gather else None, "unit": "G samples/s",
+                     "pattern": f"{rec_bytes}-byte record + 8-byte taper pair per sample, {per_req:g} records per "
+                                f"warp request, 32 warps per SM, L1-resident (jfdk_measure_gather_rate, this run)"}
+    out["hbm"] = {"achieved": hbm, "peak": peak, "frac": hbm / peak, "unit": "GB/s",
+                  "peak_source": f"{peak_kind} hbm_gbs ({'of measured' if peak_kind == 'measured' else 'of fallback'})",
+                  "algorithmic_bytes_per_launch": alg, "traffic": profile_traffic(prof)}
+    return out
 
 
 def run_batch(a, rank, world, local):
@@ -778,10 +820,7 @@ def main():
                            bp_rounding="bpcore-exact" if a.exact else "fast",
                            parallelism=f"{world} independent scans, one per GPU"),
             "stages_ms": head["stages_ms"],
-            "roofline": roofline(w, head["stages_ms"]["backprojection_hu"],
-                                 "bp_kernel (backprojection + normalisation + CT numbers)",
-                                 f"bp_kernel_{w.name}" if forms[0] == "fp32" else f"bp_mixed_kernel_{w.name}",
-                                 proj_bytes=4 if forms[0] == "fp32" else 2),
+            "roofline": roofline(w, head["stages_ms"]["backprojection_hu"], forms[0], head["clocks"]),
             "gpu_launches": sum(r["gpu_launches"] for r in res.values()),
             "clocks": head["clocks"],
         }
@@ -789,9 +828,7 @@ def main():
             line["e2e"] = head["e2e"]
         if len(forms) == 2:
             m = dict(res["mixed"])
-            m["roofline"] = roofline(w, m["stages_ms"]["backprojection_hu"],
-                                     "bp_mixed_kernel (FP16 records, FP32 accumulation)", f"bp_mixed_kernel_{w.name}",
-                                     proj_bytes=2)
+            m["roofline"] = roofline(w, m["stages_ms"]["backprojection_hu"], "mixed", m["clocks"])
             m["speedup_vs_fp32"] = head["ms_per_step"] / m["ms_per_step"]
             line["forms"] = {"fp32": {k: v for k, v in head.items()}, "mixed": m}
         if not a.no_gpu_baseline and world == 1 and not w.composite:

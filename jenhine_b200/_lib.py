@@ -101,6 +101,7 @@ _SIGS = {
     "jfdk_geometry_gradient": ([_P, _P, C.c_int, C.c_int, _P, _P, _P, _P], C.c_int),
     "jfdk_autotune": ([_P, C.c_int], C.c_int),
     "jfdk_filter_to_store": ([_P, _P, C.c_int, C.c_int], C.c_int),
+    "jfdk_filter_raw": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),
     "jfdk_store_range": ([_P, C.c_int, C.c_int, _P, _P, _P], C.c_int),
     "jfdk_backproject_store": ([_P, C.c_int, C.c_int, _P, _P], C.c_int),
     "jfdk_batch_create": ([C.POINTER(_P), _P, C.c_int, C.c_int, _P], C.c_int),

@@ -801,6 +801,35 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, in
     return JFDK_OK;
 }
 
+jfdk_status jfdk_filter_raw(jfdk_ctx* c, const uint16_t* d_raw, int v0, int nv, float* d_frames) {
+    if (!c || !d_raw || !d_frames || v0 < 0 || nv < 0 || v0 > c->nviews - nv)
+        return fail(c, JFDK_ERR_INVALID, "filter_raw: bad argument");
+    if (nv == 0) return JFDK_OK;
+    if (c->in_w != c->used_u && !compositing(c))
+        return fail(c, JFDK_ERR_UNSUPPORTED,
+                    "filter_raw: filter input width must be the frame width or twice it (compositing)");
+    const int chunk = std::min(c->opt_view_chunk, c->nviews);
+    jfdk_status st = ensure_A(c, (size_t)chunk * c->rows);
+    if (st) return st;
+    const size_t frame = (size_t)c->scan.num_dets_u * c->scan.num_dets_v;
+    for (int a = v0; a < v0 + nv; a += chunk) {
+        const int n = std::min(chunk, v0 + nv - a);
+        PrepParams pp = prep_params(c, d_raw + (size_t)a * frame);
+        if (compositing(c)) {
+            pp.width = c->in_w;
+            pp.raw_rotation = d_raw;
+            pp.raw_frame = (long long)frame;
+        }
+        JFDK_LAUNCH(c, launch_prep_weight(pp, n, a, weight_params_raw(c), a_operand(c), c->d_e, c->stream),
+                    compositing(c) ? "preprocess + compositing + pre-weight" : "preprocess + pre-weight");
+        float* out = d_frames + (size_t)(a - v0) * frame_px(c);
+        JFDK_LAUNCH(c, launch_ramp(c, ramp_params(c, n, out)), "ramp filter");
+        if (c->recon.z_filter)
+            JFDK_LAUNCH(c, launch_zfilter(out, n, c->rows, c->out_w, frame_px(c), c->out_w, c->stream), "z-filter");
+    }
+    return JFDK_OK;
+}
+
 jfdk_status jfdk_filter_to_store(jfdk_ctx* c, const uint16_t* d_raw, int v0, int nv) {
     if (!c || !d_raw || v0 < 0 || nv < 0 || v0 > c->nviews - nv)
         return fail(c, JFDK_ERR_INVALID, "filter_to_store: bad argument");

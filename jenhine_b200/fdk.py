@@ -287,6 +287,18 @@ class FDKEngine:
 
     # -- derivatives of the FP32 form (torch CUDA tensors) ------------------------
     # -- one volume over several GPUs (z-slabs; jenhine_b200.zslab) -------------
+    def filter_raw(self, raw, v0: int, nv: int, out=None):
+        """Filtered frames (nv, rows, filter_out_w) of views [v0, v0 + nv)
+        from raw, the rotation's frames on the device (jfdk_filter_raw)."""
+        import torch
+        if out is None:
+            out = torch.empty((nv, self.rows, self.filter_out_w), dtype=torch.float32, device=raw.device)
+        if not (out.is_cuda and out.dtype == torch.float32 and out.is_contiguous()
+                and tuple(out.shape) == (nv, self.rows, self.filter_out_w)):
+            raise ValueError(f"out must be a contiguous float32 CUDA tensor ({nv}, {self.rows}, {self.filter_out_w})")
+        self._check(self.lib.jfdk_filter_raw(self.ctx, _ptr(raw), int(v0), int(nv), _ptr(out)))
+        return out
+
     def filter_to_store(self, raw, v0: int, nv: int):
         """Filter views [v0, v0 + nv) of raw (the rotation's frames, device) into
         the projection store."""

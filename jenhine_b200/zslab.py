@@ -1,17 +1,20 @@
 """One volume over several GPUs: z-slabs.
 
 Each rank (one process per GPU, torch.distributed over NCCL) filters its
-share of the views into its engine's projection store, the stores are
-completed by one broadcast per rank of that rank's records (over NVLink; the
-records of all views, 16 bytes a pixel, cross each link once), and each rank
-backprojects its own slab of slices from every view.  Per GPU: V/N views of
-preprocessing and ramp filtering, 1/N of the voxel-view updates, no
-reduction.  The slabs start at multiples of the backprojection's tile depth,
-so the slab volumes equal one GPU's jfdk_reconstruct bit for bit.
-
-The engine's steps (FDKEngine.filter_to_store, store_range,
-backproject_store) are the C ABI's jfdk_filter_to_store, jfdk_store_range
-and jfdk_backproject_store; this module adds the partition and the exchange.
+share of the views into FP32 filtered frames (jfdk_filter_raw), the frames of
+every view reach every rank by one broadcast per rank (over NVLink; 4 bytes a
+pixel, each view's frames crossing each link once), and each rank
+backprojects every view into its own slab of slices (jfdk_bp_set_slab,
+jfdk_bp_reset, jfdk_bp_accumulate, jfdk_finalize).  The broadcasts are all
+issued up front and run on the collective stream while the backprojection
+of the views already present runs on the compute stream; the views are
+accumulated in order, rank by rank as their frames arrive, so each rank's
+slab equals one GPU's jfdk_reconstruct on those slices bit for bit (the
+partial sums are stored and reloaded exactly).  The slabs start at
+multiples of the backprojection's tile depth for the same reason.  Per GPU:
+V/N views of preprocessing and ramp filtering, 1/N of the voxel-view
+updates, no reduction; each rank packs the backprojection's store from the
+exchanged frames itself.
 """
 from __future__ import annotations
 
@@ -67,24 +70,37 @@ def exchange(parts, rank: int, group=None) -> None:
             dist.broadcast(t, src=src, group=group)
 
 
-def reconstruct_zslab(engine, raw, rank: int, world: int, group=None, out=None, tile_depth: int = 8):
-    """This rank's slab of the HU volume: (z0, tensor of nz x Y x X).  raw:
-    the rotation's frames on this rank's GPU (only this rank's views -- and
-    their conjugates when compositing -- are read)."""
-    views = view_ranges(engine.scan.num_views, world)
+def reconstruct_zslab(engine, raw, rank: int, world: int, group=None, out=None, tile_depth: int = 8, frames=None):
+    """This rank's slab of the HU volume: (z0, tensor of nz x Y x X, or None
+    when the rank has no slices).  raw: the rotation's frames on this rank's
+    GPU (only this rank's views -- and their conjugates when compositing --
+    are read); frames: an optional (views, rows, filter_out_w) float32 device
+    buffer for the filtered frames of every view."""
+    import torch
+    V = engine.scan.num_views
+    views = view_ranges(V, world)
     slabs = slab_ranges(engine.recon.num_pixels_z, world, tile_depth)
+    if frames is None:
+        frames = torch.empty((V, engine.rows, engine.filter_out_w), dtype=torch.float32, device=raw.device)
     v0, nv = views[rank]
-    engine.filter_to_store(raw, v0, nv)
+    if nv:
+        engine.filter_raw(raw, v0, nv, out=frames[v0:v0 + nv])
+    works = [None] * world
     if world > 1:
-        recs, scales = [], []
-        for (a, n) in views:
-            rec, sc = engine.store_range(a, n)
-            recs.append(device_bytes(*rec, raw.device))
-            scales.append(device_bytes(*sc, raw.device) if sc else None)
-        exchange(recs, rank, group)
-        if scales[0] is not None:
-            exchange(scales, rank, group)
+        import torch.distributed as dist
+        # every rank issues the same broadcasts in the same order, all at once
+        for s, (a, n) in enumerate(views):
+            if n:
+                works[s] = dist.broadcast(frames[a:a + n], src=s, group=group, async_op=True)
     z0, nz = slabs[rank]
-    if nz == 0:
+    if nz:
+        engine.bp_set_slab(z0, nz)
+        engine.bp_reset()
+    for s, (a, n) in enumerate(views):
+        if works[s] is not None:
+            works[s].wait()          # the compute stream waits for rank s's frames
+        if nz and n:
+            engine.bp_accumulate(frames[a:a + n], a)
+    if not nz:
         return z0, None
-    return z0, engine.backproject_store(z0, nz, out=out, device=raw.device)
+    return z0, engine.finalize(apply_ctnum=True, z0=z0, nz=nz, out=out, device=raw.device)

@@ -1,7 +1,8 @@
 """Host logic of the multi-GPU paths, on CPU with world_size-2 gloo process
-groups: the z-slab partition (jenhine_b200.zslab), its exchange of the
-projection stores (one broadcast per rank), and the bench's max-over-ranks
-timing reduction."""
+groups: the z-slab partition (jenhine_b200.zslab), its exchange (one
+broadcast per rank), the z-slab reconstruction's order of steps over a
+stand-in engine (filtered frames exchanged, every view accumulated in order
+into each rank's slab), and the bench's max-over-ranks timing reduction."""
 import os
 import socket
 import sys
@@ -72,3 +73,79 @@ def test_zslab_exchange_and_rank_max_gloo():
     for rank, ok_store, got in sorted(results):
         assert ok_store, (rank, got)
         assert got == 10.0 + world - 1, (rank, got)
+
+
+class _FakeEngine:
+    """The engine steps reconstruct_zslab calls, on CPU: filtered frames are
+    the view index in every pixel; bp_accumulate checks that the frames it
+    is given are those of its views and records the order."""
+
+    class _C:
+        pass
+
+    def __init__(self, views, slices):
+        self.scan, self.recon = self._C(), self._C()
+        self.scan.num_views = views
+        self.recon.num_pixels_z, self.recon.num_pixels_y, self.recon.num_pixels_x = slices, 2, 2
+        self.rows, self.filter_out_w = 2, 3
+        self.log = []
+
+    def filter_raw(self, raw, v0, nv, out):
+        out.copy_(torch.arange(v0, v0 + nv, dtype=torch.float32).view(nv, 1, 1).expand_as(out))
+        self.log.append(("filter", v0, nv))
+
+    def bp_set_slab(self, z0, nz):
+        self.log.append(("slab", z0, nz))
+
+    def bp_reset(self):
+        self.log.append(("reset",))
+
+    def bp_accumulate(self, frames, v0):
+        n = frames.shape[0]
+        ok = torch.equal(frames[:, 0, 0], torch.arange(v0, v0 + n, dtype=torch.float32))
+        self.log.append(("acc", v0, n, ok))
+
+    def finalize(self, apply_ctnum, z0, nz, out=None, device="cpu"):
+        self.log.append(("finalize", z0, nz))
+        return torch.zeros((nz, 2, 2))
+
+
+def _zslab_worker(rank, world, port, q):
+    try:
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+        sys.path.insert(0, ROOT)
+        import bench
+        from jenhine_b200 import zslab
+        dist = bench.init_dist(world, 0, backend="gloo")
+        e = _FakeEngine(10, 20)
+        z0, vol = zslab.reconstruct_zslab(e, torch.zeros(1), rank, world, tile_depth=8)
+        dist.barrier()
+        dist.destroy_process_group()
+        q.put((rank, e.log, z0, None if vol is None else tuple(vol.shape)))
+    except Exception as ex:  # reported to the test, never left hanging
+        q.put((rank, repr(ex), None, None))
+
+
+def test_zslab_reconstruction_steps_gloo():
+    from jenhine_b200.zslab import slab_ranges, view_ranges
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_zslab_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    results = [q.get(timeout=240) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+    views, slabs = view_ranges(10, world), slab_ranges(20, world, 8)
+    for rank, log, z0, shape in sorted(results):
+        assert isinstance(log, list), log
+        a, n = views[rank]
+        sz0, snz = slabs[rank]
+        assert log[0] == ("filter", a, n)
+        assert log[1:3] == [("slab", sz0, snz), ("reset",)]
+        accs = [x for x in log if x[0] == "acc"]
+        # every view, in order, each chunk carrying its own views' frames
+        assert [(x[1], x[2]) for x in accs] == views and all(x[3] for x in accs), accs
+        assert log[-1] == ("finalize", sz0, snz) and z0 == sz0 and shape == (snz, 2, 2)

@@ -1,9 +1,12 @@
-"""One volume in z-slabs (jfdk_filter_to_store, jfdk_store_range,
-jfdk_backproject_store; jenhine_b200.zslab) on one GPU: the ranks are
-emulated in turn on one engine -- each filters its views into the shared
-store, then each backprojects its slab -- and the slabs together equal
-jfdk_reconstruct bit for bit, in both forms and with compositing.  The
-exchange between processes is covered on CPU (test_multirank.py)."""
+"""One volume in z-slabs (jfdk_filter_raw, then jfdk_bp_set_slab /
+jfdk_bp_reset / jfdk_bp_accumulate / jfdk_finalize per slab;
+jenhine_b200.zslab) on one GPU: the ranks are emulated in turn on one
+engine -- each filters its views into the shared frames, then each
+backprojects every view, in order, into its slab -- and the slabs together
+equal jfdk_reconstruct bit for bit, in both forms and with compositing.  The
+store-level entry points (jfdk_filter_to_store, jfdk_store_range,
+jfdk_backproject_store) are checked the same way.  The exchange between
+processes is covered on CPU (test_multirank.py)."""
 import numpy as np
 import pytest
 
@@ -32,10 +35,27 @@ def test_emulated_ranks_equal_reconstruct(torch_cuda, name, precision, world):
     raw = to_dev(torch, g["raw"])
     whole = e.reconstruct(raw).clone()
     Z = whole.shape[0]
-    for v0, nv in view_ranges(raw.shape[0], world):
-        e.filter_to_store(raw, v0, nv)
-    parts = [e.backproject_store(z0, nz) for z0, nz in slab_ranges(Z, world) if nz]
+    views = view_ranges(raw.shape[0], world)
+    frames = torch.empty((raw.shape[0], e.rows, e.filter_out_w), dtype=torch.float32, device="cuda")
+    for v0, nv in views:              # each rank filters its views
+        e.filter_raw(raw, v0, nv, out=frames[v0:v0 + nv])
+    parts = []
+    for z0, nz in slab_ranges(Z, world):
+        if not nz:
+            continue
+        e.bp_set_slab(z0, nz)         # each rank backprojects every view into its slab
+        e.bp_reset()
+        for v0, nv in views:
+            e.bp_accumulate(frames[v0:v0 + nv], v0)
+        parts.append(e.finalize(apply_ctnum=True, z0=z0, nz=nz))
     got = torch.cat(parts)
+    torch.cuda.synchronize()
+    assert torch.equal(torch.nan_to_num(got, 1e30), torch.nan_to_num(whole, 1e30))
+    # the store-level entry points, the same way
+    e.bp_set_slab(0, Z)
+    for v0, nv in views:
+        e.filter_to_store(raw, v0, nv)
+    got = torch.cat([e.backproject_store(z0, nz) for z0, nz in slab_ranges(Z, world) if nz])
     torch.cuda.synchronize()
     assert torch.equal(torch.nan_to_num(got, 1e30), torch.nan_to_num(whole, 1e30))
 
@@ -47,7 +67,7 @@ def test_store_range_describes_the_store(torch_cuda):
         e = engine_for(g, precision=precision)
         (p0, n0), sc0 = e.store_range(0, 4)
         (p1, n1), sc1 = e.store_range(4, 6)
-        frame = e.rows * e.filter_out_w * 16
+        frame = e.rows * e.filter_out_w * 16      # float4 quads / 16-byte records
         assert n0 == 4 * frame and n1 == 6 * frame and p1 == p0 + 4 * frame
         if precision == "mixed":
             assert sc0[1] == 16 and sc1[0] == sc0[0] + 16
