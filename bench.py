@@ -542,9 +542,11 @@ def roofline(w, bp_ms, form, clocks):
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     mhz = (clocks or {}).get("sm_mhz") or 1965.0
     w32 = profile_figure(f"{kernel}_c2_chunks", "warp_instructions_per_32_updates")
-    rec_bytes = 16 if form == "fp32" else 8
+    # FP32: a 16-byte quad and an 8-byte taper pair per sample; mixed: one
+    # 16-byte record that carries the taper
+    taper = form == "fp32"
     per_req = profile_figure(f"{kernel}_c2_chunks", "records_per_request") or 6.0
-    gather = gather_ceiling(rec_bytes, True, max(1, min(32, int(round(per_req)))))
+    gather = gather_ceiling(16, taper, max(1, min(32, int(round(per_req)))))
     peak, peak_kind = measured_peaks()
     alg = g.n_views * g.det_v * g.det_u * (4 if form == "fp32" else 2) + r.num_pixels_x * r.num_pixels_y * \
         r.num_pixels_z * 4
@@ -560,8 +562,9 @@ def roofline(w, bp_ms, form, clocks):
         out.update({"peak": None, "frac": None, "peak_source": "no instruction count committed for this kernel"})
     out["gather"] = {"peak": gather / 1e9 if gather else None, "achieved": gups,
                      "frac": gups / (gather / 1e9) if gather else None, "unit": "G samples/s",
-                     "pattern": f"{rec_bytes}-byte record + 8-byte taper pair per sample, {per_req:g} records per "
-                                f"warp request, 32 warps per SM, L1-resident (jfdk_measure_gather_rate, this run)"}
+                     "pattern": ("16-byte quad + 8-byte taper pair" if taper else "one 16-byte record") +
+                                f" per sample, {per_req:g} records per warp request, 32 warps per SM, L1-resident "
+                                f"(jfdk_measure_gather_rate, this run)"}
     out["hbm"] = {"achieved": hbm, "peak": peak, "frac": hbm / peak, "unit": "GB/s",
                   "peak_source": f"{peak_kind} hbm_gbs ({'of measured' if peak_kind == 'measured' else 'of fallback'})",
                   "algorithmic_bytes_per_launch": alg, "traffic": profile_traffic(prof)}
