@@ -328,7 +328,8 @@ jfdk_status jfdk_autotune(jfdk_ctx* ctx, int flags);
 
 /* A batch of scans (one context each, all of the same form) reconstructed
  * together, on one of two schedules:
- *  - persistent: every scan's filter stage, then ONE persistent
+ *  - persistent: every scan's filter stage (the scans dealt over four
+ *    streams, so small scans' stages run side by side), then ONE persistent
  *    backprojection launch over the tiles of up to 16 scans (scans in order;
  *    a CTA takes the next tile when it finishes one, so scans of uneven size
  *    leave no tail; each scan keeps its own tile depth; consecutive scans

@@ -32,6 +32,10 @@ struct jfdk_batch {
     unsigned* d_counter = nullptr;      // one work cursor per group
     int schedule = 0;                   // JFDK_BATCH_PERSISTENT / _PIPELINED, 0 not chosen
     cudaStream_t aux = nullptr;         // the pipelined schedule's filter stream
+    // the persistent schedule's filter stages run on the batch stream and
+    // these, scans dealt round-robin, joined before the persistent launch
+    std::vector<cudaStream_t> filt;
+    std::vector<cudaEvent_t> filt_ev;   // [fork, join] per stream of filt
     std::vector<cudaEvent_t> ev;        // [scans] filtered, fork, join, two timing events
     std::vector<float*> hu;             // the outputs of the run being enqueued
     cudaGraph_t graph = nullptr;
@@ -96,16 +100,29 @@ jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
     return JFDK_OK;
 }
 
-// Persistent: every scan's filter stage on the batch stream, then the
-// persistent BP launches.
+// Persistent: every scan's filter stage -- dealt round-robin over the batch
+// stream and kFilterStreams - 1 more, so the stages of small scans, which
+// leave most of the GPU idle, run side by side -- then the persistent BP
+// launches once all have joined.
+constexpr int kFilterStreams = 4;
+
 jfdk_status enqueue_persistent(jfdk_batch* b, const uint16_t* const* d_raw) {
+    const size_t ns = b->filt.size() + 1;
+    for (size_t j = 0; j + 1 < ns; ++j) {
+        BATCH_CUDA(b, cudaEventRecord(b->filt_ev[2 * j], b->stream), "event");
+        BATCH_CUDA(b, cudaStreamWaitEvent(b->filt[j], b->filt_ev[2 * j], 0), "event");
+    }
     for (size_t i = 0; i < b->ctx.size(); ++i) {
         jfdk_ctx* c = b->ctx[i];
         cudaStream_t saved = c->stream;
-        c->stream = b->stream;
+        c->stream = i % ns == 0 ? b->stream : b->filt[i % ns - 1];
         jfdk_status st = reconstruct_filter_stage(c, d_raw[i], c->nviews);
         c->stream = saved;
         if (st) return berr(b, st, std::string("scan ") + std::to_string(i) + ": " + c->err);
+    }
+    for (size_t j = 0; j + 1 < ns; ++j) {
+        BATCH_CUDA(b, cudaEventRecord(b->filt_ev[2 * j + 1], b->filt[j]), "event");
+        BATCH_CUDA(b, cudaStreamWaitEvent(b->stream, b->filt_ev[2 * j + 1], 0), "event");
     }
     for (size_t k = 0; k < b->groups.size(); ++k) {
         const jfdk_batch::Group& g = b->groups[k];
@@ -201,6 +218,17 @@ jfdk_status jfdk_batch_create(jfdk_batch** out, jfdk_ctx* const* ctxs, int n, in
     b->schedule = (flags & JFDK_BATCH_PIPELINED) ? JFDK_BATCH_PIPELINED
                   : (flags & JFDK_BATCH_PERSISTENT) ? JFDK_BATCH_PERSISTENT : 0;
     BATCH_CUDA(b, cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking), "creating the filter stream");
+    const int extra = std::min(kFilterStreams, n) - 1;
+    for (int j = 0; j < extra; ++j) {
+        cudaStream_t st = nullptr;
+        BATCH_CUDA(b, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "creating a filter stream");
+        b->filt.push_back(st);
+        for (int k = 0; k < 2; ++k) {
+            cudaEvent_t e = nullptr;
+            BATCH_CUDA(b, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "creating an event");
+            b->filt_ev.push_back(e);
+        }
+    }
     b->ev.assign((size_t)n + 4, nullptr);
     for (auto& e : b->ev) BATCH_CUDA(b, cudaEventCreate(&e), "creating an event");
     if (flags & JFDK_BATCH_AUTOTUNE)
@@ -219,10 +247,13 @@ void jfdk_batch_destroy(jfdk_batch* b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graph(b);
     if (b->aux) cudaStreamSynchronize(b->aux);
+    for (cudaStream_t st : b->filt) cudaStreamSynchronize(st);
     if (b->d_counter) cudaFree(b->d_counter);
     for (cudaEvent_t e : b->ev)
         if (e) cudaEventDestroy(e);
     if (b->aux) cudaStreamDestroy(b->aux);
+    for (cudaStream_t st : b->filt) cudaStreamDestroy(st);
+    for (cudaEvent_t e : b->filt_ev) cudaEventDestroy(e);
     if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
     delete b;
 }

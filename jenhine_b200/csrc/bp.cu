@@ -359,7 +359,7 @@ __device__ __forceinline__ void batch_dispatch(const BatchSlots& t, int si) {
 }
 
 template <bool MIXED, bool WZ>
-__global__ void __launch_bounds__(kBPThreads, bp_min_blocks(8))
+__global__ void __launch_bounds__(kBPThreads, MIXED ? bp_min_blocks(8) : bp_fp32_min_blocks(8))
     bp_batch_kernel(const __grid_constant__ BatchSlots t, int nscans, unsigned* __restrict__ counter,
                     unsigned total) {
     __shared__ unsigned s_next;
