@@ -131,8 +131,8 @@ jfdk_status jfdk_filter_frames(jfdk_ctx* ctx, const float* d_in, int v0, int nv,
  * freed.  The ramp product always runs on FP32 CUDA cores, whatever the
  * context's precision or JFDK_OPT_RAMP_PRODUCT: the result equals
  * jfdk_filter_frames' under JFDK_RAMP_FP32_SIMT bit for bit and the other
- * products' within their rounding (rel-L2 <= 1e-5 against TF32x3 and
- * FP16x3, <= 5e-5 against BF16x3).  Limit: nv * rows * pitch + nv * rows
+ * products' within their rounding (rel-L2 <= 1e-5 against I8x14, TF32x3
+ * and FP16x3, <= 5e-5 against BF16x3).  Limit: nv * rows * pitch + nv * rows
  * floats must fit in 1,048,576 floats, where pitch is filter_in_w rounded up
  * to a multiple of 64 (for a 768 x 768 frame: one view per call); larger
  * requests return JFDK_ERR_INVALID.  The first call on each device looks up
@@ -269,14 +269,22 @@ enum {
                                  volume does not depend on it                  */
 };
 /* Ramp products (JFDK_OPT_RAMP_PRODUCT).  The split products run on the
- * tcgen05 tensor cores as hi*hi + hi*lo + lo*hi with FP32 accumulation. */
+ * tcgen05 tensor cores as hi*hi + hi*lo + lo*hi with FP32 accumulation; the
+ * int8 product runs on them with exact int32 accumulation. */
 typedef enum {
-    JFDK_RAMP_DEFAULT = 0,    /* TF32x3 in the FP32 form, BF16x3 in the mixed form */
+    JFDK_RAMP_DEFAULT = 0,    /* I8x14 in the FP32 form, BF16x3 in the mixed form  */
     JFDK_RAMP_TF32X3 = 1,     /* ~2^-22 relative                                    */
     JFDK_RAMP_BF16X3 = 2,     /* ~2^-17 relative, twice the tensor rate of TF32    */
     JFDK_RAMP_FP16X3 = 3,     /* rows and operator scaled by powers of two into the
                                  FP16 range; ~2^-22 relative at the BF16 rate     */
-    JFDK_RAMP_FP32_SIMT = 4   /* FP32 CUDA cores                                    */
+    JFDK_RAMP_FP32_SIMT = 4,  /* FP32 CUDA cores                                    */
+    JFDK_RAMP_I8X14 = 5       /* rows and the operator (from its FP64 kernel) as
+                                 32-bit fixed point below power-of-two scales, each
+                                 cut into four signed bytes; the ten leading byte
+                                 products summed exactly in int32, combined exactly
+                                 in int64, rounded once: the product of the float
+                                 rows to ~2^-30 of the leading term, independent of
+                                 the tiling (the FP32 form's default)            */
 } jfdk_ramp_product;
 jfdk_status jfdk_set_option(jfdk_ctx* ctx, int key, long long value);
 /* Stage times (ms) of the last jfdk_reconstruct with JFDK_OPT_STAGE_TIMING:

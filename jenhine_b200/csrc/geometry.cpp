@@ -149,30 +149,6 @@ std::vector<float> filter_spectrum(int L, float hsr, float cutStart, float cutEn
     return H;
 }
 
-// 4x4 inverse in FP64 (Gauss-Jordan with partial pivoting).
-bool invert4_f64(const double* m, double* inv) {
-    double a[4][8];
-    for (int i = 0; i < 4; ++i)
-        for (int j = 0; j < 8; ++j) a[i][j] = j < 4 ? m[i * 4 + j] : (j - 4 == i ? 1.0 : 0.0);
-    for (int c = 0; c < 4; ++c) {
-        int p = c;
-        for (int r = c + 1; r < 4; ++r)
-            if (std::fabs(a[r][c]) > std::fabs(a[p][c])) p = r;
-        if (a[p][c] == 0.0) return false;
-        if (p != c)
-            for (int j = 0; j < 8; ++j) std::swap(a[p][j], a[c][j]);
-        const double d = a[c][c];
-        for (int j = 0; j < 8; ++j) a[c][j] /= d;
-        for (int r = 0; r < 4; ++r)
-            if (r != c) {
-                const double f = a[r][c];
-                for (int j = 0; j < 8; ++j) a[r][j] -= f * a[c][j];
-            }
-    }
-    for (int i = 0; i < 4; ++i)
-        for (int j = 0; j < 4; ++j) inv[i * 4 + j] = a[i][j + 4];
-    return true;
-}
 }  // namespace
 
 int fft_length(int width) {  // FilterAgent/FilterCore.cpp:254-260
@@ -207,7 +183,11 @@ std::string build_host_operators(const jfdk_scan_params& scan, const jfdk_recon_
         }
     }
     // -- inverse transform matrix per 9-view pre-weight group: PTM2TM in
-    //    float (TransformMatrix/MatrixConvertor.cpp:8-27), inverse in FP64 --
+    //    float (TransformMatrix/MatrixConvertor.cpp:8-27), then TM^-1 solved
+    //    in float against the identity as PreFilterWeightGenerator.cpp:20-31
+    //    does (LinearEquationSolver, LAPACK's sgesv order), one column at a
+    //    time: the weights' distance is a difference of two back-projected
+    //    points, so the inverse must round as the reference's does --
     const int G = (N + 8) / 9;
     ops.tinv.assign((size_t)G * 16, 0.0f);
     const float dso = scan.dso;
@@ -221,10 +201,16 @@ std::string build_host_operators(const jfdk_scan_params& scan, const jfdk_recon_
         std::memcpy(tm, P, 8 * sizeof(float));
         tm[8] = s20 * P[8]; tm[9] = s20 * P[9]; tm[10] = 0.0f; tm[11] = s23 * P[11];
         std::memcpy(tm + 12, P + 8, 4 * sizeof(float));
-        double md[16], inv[16];
-        for (int i = 0; i < 16; ++i) md[i] = tm[i];
-        if (!invert4_f64(md, inv)) return "singular transform matrix for view " + std::to_string(src);
-        for (int i = 0; i < 16; ++i) ops.tinv[(size_t)g * 16 + i] = (float)inv[i];
+        for (int j = 0; j < 4; ++j) {
+            float A[16], e[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            std::memcpy(A, tm, sizeof A);
+            e[j] = 1.0f;
+            solve4_f32(A, e);
+            for (int i = 0; i < 4; ++i) {
+                if (!std::isfinite(e[i])) return "singular transform matrix for view " + std::to_string(src);
+                ops.tinv[(size_t)g * 16 + i * 4 + j] = e[i];
+            }
+        }
     }
     // -- inverse transform matrix of every view, solved in float in LAPACK's
     //    order like CompositeCore::Inverse (CompositeAgent/CompositeCore.cpp:186-191),
@@ -256,6 +242,8 @@ std::string build_host_operators(const jfdk_scan_params& scan, const jfdk_recon_
     std::vector<double> h(L);
     for (int i = 0; i < L; ++i) h[i] = z[i].real() / L;
     const int off = mirror ? out_w : 0;                  // FilterCore.cpp:28
+    ops.h = h;
+    ops.off = off;
     ops.T.assign((size_t)out_w * in_w, 0.0f);
     for (int j = 0; j < out_w; ++j)
         for (int i = 0; i < in_w; ++i) {

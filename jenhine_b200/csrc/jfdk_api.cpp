@@ -102,7 +102,7 @@ bool mixed(const jfdk_ctx* c) { return c->precision == JFDK_PRECISION_MIXED; }
 
 int ramp_kind(const jfdk_ctx* c) {
     if (c->opt_ramp != JFDK_RAMP_DEFAULT) return c->opt_ramp;
-    return mixed(c) ? JFDK_RAMP_BF16X3 : JFDK_RAMP_TF32X3;
+    return mixed(c) ? JFDK_RAMP_BF16X3 : JFDK_RAMP_I8X14;
 }
 
 // The A operand in the layout the chosen ramp product reads: the high part
@@ -112,8 +112,9 @@ AOperand a_operand(const jfdk_ctx* c) {
     const int k = ramp_kind(c);
     a.kind = k == JFDK_RAMP_TF32X3 ? AOUT_TF32X2
              : k == JFDK_RAMP_BF16X3 ? AOUT_BF16X2
-             : k == JFDK_RAMP_FP16X3 ? AOUT_FP16X2 : AOUT_F32;
-    const size_t elem = (a.kind == AOUT_BF16X2 || a.kind == AOUT_FP16X2) ? 2 : 4;
+             : k == JFDK_RAMP_FP16X3 ? AOUT_FP16X2
+             : k == JFDK_RAMP_I8X14 ? AOUT_I8X4 : AOUT_F32;
+    const size_t elem = a.kind == AOUT_I8X4 ? 1 : (a.kind == AOUT_BF16X2 || a.kind == AOUT_FP16X2) ? 2 : 4;
     a.hi = c->d_A;
     a.lo = static_cast<char*>(c->d_A) + c->a_rows * a_pitch(c) * elem;
     a.row_scale = c->d_arow;
@@ -298,6 +299,12 @@ cudaError_t launch_ramp(jfdk_ctx* c, RampParams r) {
         case JFDK_RAMP_BF16X3:
             return launch_ramp_gemm_tc(r, RAMP_BF16X3, a.hi, a.lo, c->d_Tb, c->d_Tb + (size_t)c->out_w * a_pitch(c),
                                        c->d_status, c->stream);
+        case JFDK_RAMP_I8X14:
+            r.row_scale = c->d_arow;
+            r.b_scale = c->i8_scale;
+            return launch_ramp_i8(r, static_cast<const int8_t*>(a.hi),
+                                  (long long)(static_cast<const int8_t*>(a.lo) - static_cast<const int8_t*>(a.hi)),
+                                  c->d_Ti8, (long long)c->out_w * a_pitch(c), c->d_i8mask, c->d_status, c->stream);
         default:
             r.row_scale = c->d_arow;
             r.b_scale = c->tf_inv_scale;
@@ -429,6 +436,7 @@ void jfdk_destroy(jfdk_ctx* c) {
     dev_free(c, c->d_ptm); dev_free(c, c->d_tw); dev_free(c, c->d_tinv); dev_free(c, c->d_dmin); dev_free(c, c->d_pw);
     dev_free(c, c->d_tinv_view); dev_free(c, c->d_cmask);
     dev_free(c, c->d_T); dev_free(c, c->d_Th); dev_free(c, c->d_Tl); dev_free(c, c->d_Tb); dev_free(c, c->d_Tf);
+    dev_free(c, c->d_Ti8); dev_free(c, c->d_i8mask);
     dev_free(c, c->d_status); dev_free(c, c->d_c); dev_free(c, c->d_A); dev_free(c, c->d_e); dev_free(c, c->d_arow);
     dev_free(c, c->d_plain);
     dev_free(c, c->d_q4); dev_free(c, c->d_qscale); dev_free(c, c->d_absmax);
@@ -573,6 +581,45 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
         JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "upload");
     }
     JFDK_CUDA(c, cudaMemcpyAsync(c->d_c, c->ops.c.data(), sizeof(float) * c->out_w, cudaMemcpyHostToDevice, c->stream), "upload");
+    {   // int8 digits of the operator from its FP64 kernel (32-bit fixed
+        // point below 2^F in four balanced bytes, as the weight kernel cuts
+        // the rows), and which digit planes each (output tile, K block) of
+        // the int8 product needs
+        const int P = a_pitch(c), N = c->out_w, K = c->in_w, L = (int)c->ops.h.size();
+        double tmax = 0.0;
+        for (double v : c->ops.h) tmax = std::max(tmax, std::fabs(v));
+        int F = 0;
+        if (tmax > 0.0) {
+            F = std::ilogb(tmax) - 6;
+            if (tmax > std::ldexp(127.0, F)) ++F;
+        }
+        c->i8_scale = (float)std::ldexp(1.0, F);
+        const size_t plane = (size_t)N * P;
+        std::vector<int8_t> td((size_t)kI8OpDigits * plane, 0);
+        for (int j = 0; j < N; ++j)
+            for (int i = 0; i < K; ++i) {
+                int d = (c->ops.off + j - i) % L;
+                if (d < 0) d += L;
+                long long q = std::llrint(std::ldexp(c->ops.h[d], 24 - F));   // |q| <= 127 * 2^24
+                for (int t = kI8OpDigits - 1; t > 0; --t) {
+                    const long long lo = ((q + 128) & 255) - 128;
+                    td[t * plane + (size_t)j * P + i] = (int8_t)lo;
+                    q = (q - lo) / 256;
+                }
+                td[(size_t)j * P + i] = (int8_t)q;
+            }
+        const int tn = (N + kI8TileN - 1) / kI8TileN, nk = (P + kI8BlockK - 1) / kI8BlockK;
+        std::vector<uint8_t> mask((size_t)tn * nk, 0);
+        for (int t = 0; t < kI8OpDigits; ++t)
+            for (int j = 0; j < N; ++j)
+                for (int i = 0; i < P; ++i)
+                    if (td[t * plane + (size_t)j * P + i]) mask[(size_t)(j / kI8TileN) * nk + i / kI8BlockK] |= (uint8_t)(1u << t);
+        if ((st = dev_alloc(c, &c->d_Ti8, td.size(), "the operator's digits"))) return bail(st);
+        if ((st = dev_alloc(c, &c->d_i8mask, mask.size(), "the digit masks"))) return bail(st);
+        JFDK_CUDA(c, cudaMemcpyAsync(c->d_Ti8, td.data(), td.size(), cudaMemcpyHostToDevice, c->stream), "upload");
+        JFDK_CUDA(c, cudaMemcpyAsync(c->d_i8mask, mask.data(), mask.size(), cudaMemcpyHostToDevice, c->stream), "upload");
+        JFDK_CUDA(c, cudaStreamSynchronize(c->stream), "upload");
+    }
     {   // T^T [in_w][round64(out_w)] for the filter adjoint
         std::vector<float> tt((size_t)c->in_w * tt_pitch, 0.0f);
         for (int j = 0; j < c->out_w; ++j)
@@ -627,7 +674,7 @@ jfdk_status jfdk_set_option(jfdk_ctx* c, int key, long long value) {
             return JFDK_OK;
         case JFDK_OPT_FILTER_SIMT: c->opt_ramp = value ? JFDK_RAMP_FP32_SIMT : JFDK_RAMP_DEFAULT; return JFDK_OK;
         case JFDK_OPT_RAMP_PRODUCT:
-            if (value < JFDK_RAMP_DEFAULT || value > JFDK_RAMP_FP32_SIMT)
+            if (value < JFDK_RAMP_DEFAULT || value > JFDK_RAMP_I8X14)
                 return fail(c, JFDK_ERR_INVALID, "unknown ramp product");
             c->opt_ramp = (int)value;
             return JFDK_OK;

@@ -21,6 +21,8 @@ struct HostOperators {
     std::vector<float> tinv;    // [groups][16]     inverse TM per 9-view group
     std::vector<float> tinv_view;  // [views][16]   inverse TM per view, float solve (compositing)
     std::vector<float> T;       // [out_w][in_w]    ramp operator (Toeplitz)
+    std::vector<double> h;      // [L]              its kernel in double: T[j][i] = h[(off + j - i) mod L]
+    int off = 0;                // output offset of the kernel (FilterCore.cpp:28)
     std::vector<float> c;       // [out_w]          edge-ramp response
     std::vector<float> H;       // [L/2+1]          filter spectrum
 };
@@ -149,14 +151,19 @@ struct WeightParams {
 cudaError_t launch_preprocess(const PrepParams& p, int nv, float* out, cudaStream_t s);
 
 // The ramp product's A operand as the weight kernels write it.
-enum AOutKind { AOUT_F32 = 0, AOUT_TF32X2 = 1, AOUT_BF16X2 = 2, AOUT_FP16X2 = 3 };
+enum AOutKind { AOUT_F32 = 0, AOUT_TF32X2 = 1, AOUT_BF16X2 = 2, AOUT_FP16X2 = 3, AOUT_I8X4 = 4 };
 struct AOperand {
     int kind;             // AOutKind
-    void* hi;             // [M][pitch]: fp32 (F32, TF32X2) or 16-bit values
-    void* lo;             // low parts (split kinds)
-    float* row_scale;     // FP16X2: [M] 1 / the row's power-of-two scale
+    void* hi;             // [M][pitch]: fp32 (F32, TF32X2), 16-bit values, or int8 digit plane 0 (I8X4)
+    void* lo;             // low parts (split kinds); I8X4: digit plane 1 (planes lo - hi bytes apart)
+    float* row_scale;     // FP16X2: [M] 1 / the row's power-of-two scale; I8X4: [M] 2^E of the row
     int pitch;            // elements per row (K padded)
 };
+// Digits of the int8 product: rows and operator as 32-bit fixed point below
+// power-of-two scales (|x| <= 127 * 2^E, Q = round(x * 2^(24 - E))), each
+// split into four balanced signed bytes, most significant first.
+constexpr int kI8RowDigits = 4;
+constexpr int kI8OpDigits = 4;
 // Composite nv preprocessed direct / conjugate frame pairs of views
 // v0.. into out [nv][H][2W] (CompositeAgent path).
 cudaError_t launch_composite_frames(const float* dirc, const float* conj, int v0, int nv, const CompositeParams& c,
@@ -191,13 +198,22 @@ struct RampParams {
 };
 cudaError_t launch_ramp_gemm(const RampParams& p, cudaStream_t s);
 // Tensor-core split products (ramp_gemm_tc.cu).
-enum RampKind { RAMP_TF32X3 = 0, RAMP_BF16X3 = 1, RAMP_FP16X3 = 2 };
+enum RampKind { RAMP_TF32X3 = 0, RAMP_BF16X3 = 1, RAMP_FP16X3 = 2, RAMP_I8X14 = 3 };
 // Ah, Al [M][a_pitch] and Bh, Bl [N][a_pitch] in the kind's element type;
 // a_pitch a multiple of 32 (TF32X3) or 64.  A timed-out pipeline wait sets
 // *status (device word) and the CTA skips the rest of its work.
 cudaError_t launch_ramp_gemm_tc(const RampParams& p, int kind, const void* Ah, const void* Al, const void* Bh,
                                 const void* Bl, int* status, cudaStream_t s);
 float tf32_round_host(float x);
+// The exact int8 product (ramp_gemm_tc.cu): A digit planes [kI8RowDigits]
+// [M][a_pitch] (a_plane bytes apart, p.row_scale the rows' 2^E), operator
+// digit planes [kI8OpDigits][N][a_pitch] (b_plane bytes apart, p.b_scale
+// its 2^F), and per output tile x K block the mask of operator digit planes
+// that are not all zero ([ceil(N / kI8TileN)][ceil(a_pitch / kI8BlockK)]).
+constexpr int kI8TileN = 64;
+constexpr int kI8BlockK = 128;
+cudaError_t launch_ramp_i8(const RampParams& p, const int8_t* A, long long a_plane, const int8_t* B,
+                           long long b_plane, const uint8_t* masks, int* status, cudaStream_t s);
 
 // Derivatives (adjoint.cu).
 struct AdjParams {
@@ -268,6 +284,9 @@ struct jfdk_ctx {
     uint16_t* d_Tf = nullptr;    // FP16 split of the scaled operator (high, low)
     float tf_inv_scale = 1.0f;   // 1 / the FP16 operator's scale
     float* d_Tt = nullptr;       // transposed operator [in_w][round64(out_w)] (filter adjoint)
+    int8_t* d_Ti8 = nullptr;     // int8 digits of the operator [kI8OpDigits][out_w][a_pitch]
+    uint8_t* d_i8mask = nullptr; // [ceil(out_w / kI8TileN)][a_pitch / kI8BlockK] non-zero digit planes
+    float i8_scale = 1.0f;       // 2^F of the operator's digits
     float* d_czero = nullptr;    // [in_w] zeros
     float* d_c = nullptr;
     int* d_status = nullptr;     // nonzero: a kernel's bounded wait gave up

@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(256) weight_kernel(PrepParams P, const float* 
     auto value = [&](int i, float p) -> float {
         return __fmul_rn(p, pwrow ? __ldg(pwrow + i) : __fdiv_rn(dmin, pw_dist(r, u_axis(i, width, W.det_right))));
     };
-    const int elem = OUT == AOUT_F32 || OUT == AOUT_TF32X2 ? 4 : 2;
+    const int elem = OUT == AOUT_F32 || OUT == AOUT_TF32X2 ? 4 : OUT == AOUT_I8X4 ? 1 : 2;
     const bool vec = FROM_RAW && !comp && ((reinterpret_cast<uintptr_t>(P.raw) & 7) == 0) &&
                      ((reinterpret_cast<uintptr_t>(A.hi) & 15) == 0) &&
                      (OUT == AOUT_F32 || (reinterpret_cast<uintptr_t>(A.lo) & 15) == 0) &&
@@ -339,7 +339,72 @@ __global__ void __launch_bounds__(256) weight_kernel(PrepParams P, const float* 
         scale = (mx > 0.0f && mx <= 3.0e38f) ? ldexpf(1.0f, 14 - ilogbf(mx)) : 1.0f;
         if (threadIdx.x == 0) A.row_scale[m] = __fdiv_rn(1.0f, scale);
     }
-    if (vec) {
+    if constexpr (OUT == AOUT_I8X4) {
+        // The row's values (staged in shared memory), its power-of-two scale
+        // 2^E (the least E with max |a| <= 127 * 2^E), then per element the
+        // 32-bit fixed point Q = round(a * 2^(24 - E)) (|Q| < 2^31; exact for
+        // every a down to 2^-31 of the row's largest) as four balanced signed
+        // bytes, Q = d0 2^24 + d1 2^16 + d2 2^8 + d3, each in [-128, 127].
+        extern __shared__ float s_row[];
+        float mx = 0.0f;
+        if (vec) {
+            for (int i4 = threadIdx.x * 4; i4 < width; i4 += blockDim.x * 4) {
+                const uint2 raw4 = *reinterpret_cast<const uint2*>(src + i4);
+                const float p[4] = {(float)(raw4.x & 0xffffu), (float)(raw4.x >> 16), (float)(raw4.y & 0xffffu),
+                                    (float)(raw4.y >> 16)};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float v = value(i4 + k, prep_pixel(p[k], P));
+                    s_row[i4 + k] = v;
+                    mx = fmaxf(mx, fabsf(v));
+                }
+            }
+        } else {
+            for (int i = threadIdx.x; i < width; i += blockDim.x) {
+                const float v = value(i, pix(i));
+                s_row[i] = v;
+                mx = fmaxf(mx, fabsf(v));
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+        __syncthreads();
+        mx = red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mx = fmaxf(mx, red[w]);
+        int E = 0;
+        if (mx > 0.0f && mx <= 3.0e38f) {
+            E = ilogbf(mx) - 6;
+            if (mx > ldexpf(127.0f, E)) ++E;
+        }
+        const float up = ldexpf(1.0f, 24 - E);
+        if (threadIdx.x == 0) A.row_scale[m] = ldexpf(1.0f, E);
+        int8_t* plane = static_cast<int8_t*>(A.hi);
+        const size_t pstride = (size_t)(static_cast<int8_t*>(A.lo) - static_cast<int8_t*>(A.hi));
+        for (int i4 = threadIdx.x * 4; i4 < A.pitch; i4 += blockDim.x * 4) {
+            int q[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                // |x| <= 127 * 2^24 < 2^31; non-finite rows (E = 0) are clamped
+                const float x = i4 + k < width ? s_row[i4 + k] * up : 0.0f;
+                q[k] = __float2int_rn(fmaxf(-2130706432.0f, fminf(2130706432.0f, x)));
+            }
+            signed char d[kI8RowDigits][4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+#pragma unroll
+                for (int s = kI8RowDigits - 1; s > 0; --s) {
+                    const int lo = ((q[k] + 128) & 255) - 128;
+                    d[s][k] = (signed char)lo;
+                    q[k] = (q[k] - lo) >> 8;
+                }
+                d[0][k] = (signed char)q[k];
+            }
+#pragma unroll
+            for (int s = 0; s < kI8RowDigits; ++s)
+                *reinterpret_cast<char4*>(plane + s * pstride + a0 + i4) = make_char4(d[s][0], d[s][1], d[s][2], d[s][3]);
+        }
+    } else if (vec) {
         for (int i4 = threadIdx.x * 4; i4 < width; i4 += blockDim.x * 4) {
             const uint2 raw4 = *reinterpret_cast<const uint2*>(src + i4);
             const float p[4] = {(float)(raw4.x & 0xffffu), (float)(raw4.x >> 16), (float)(raw4.y & 0xffffu),
@@ -352,8 +417,114 @@ __global__ void __launch_bounds__(256) weight_kernel(PrepParams P, const float* 
     } else {
         for (int i = threadIdx.x; i < width; i += blockDim.x) store1<OUT>(A.hi, A.lo, a0 + i, value(i, pix(i)) * scale);
     }
-    for (int i = width + threadIdx.x; i < A.pitch; i += blockDim.x) store1<OUT>(A.hi, A.lo, a0 + i, 0.0f);
+    if constexpr (OUT != AOUT_I8X4)
+        for (int i = width + threadIdx.x; i < A.pitch; i += blockDim.x) store1<OUT>(A.hi, A.lo, a0 + i, 0.0f);
     if (threadIdx.x == 0) {
+        // FilterCore.cpp:203-214 -- mean of the three outermost unweighted samples
+        const float edge = W.mirror ? __fdiv_rn(__fadd_rn(__fadd_rn(pix(width - 1), pix(width - 2)), pix(width - 3)), 3.0f)
+                                    : __fdiv_rn(__fadd_rn(__fadd_rn(pix(0), pix(1)), pix(2)), 3.0f);
+        e[m] = edge;
+    }
+}
+
+// The int8 digit form with one warp per row: the row's values stay in
+// registers (width <= 32 * 4 * kI8WarpGroups), the scale's maximum is a
+// warp reduction; the same values, scale and digits as weight_kernel's
+// AOUT_I8X4 path.  No compositing (weight_kernel handles it).
+constexpr int kI8WarpGroups = 16;
+template <bool FROM_RAW>
+__global__ void __launch_bounds__(256) weight_i8_kernel(PrepParams P, const float* __restrict__ in, int width,
+                                                        int rows, int v0, WeightParams W, AOperand A,
+                                                        float* __restrict__ e) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int row = blockIdx.x * 8 + warp, vl = blockIdx.y;
+    const int view = (v0 + vl) % W.num_views;
+    const int g = view / 9;
+    __shared__ float T[16];
+    if (threadIdx.x < 16) T[threadIdx.x] = W.tinv[g * 16 + threadIdx.x];
+    __syncthreads();
+    if (row >= rows) return;
+    const float dmin = W.dmin[g];
+    const PWRow r = pw_row(T, (float)row);
+    const size_t m = (size_t)vl * rows + row;
+    const size_t a0 = m * A.pitch;
+    const uint16_t* src = FROM_RAW ? P.raw + ((size_t)vl * P.in_h + row + P.crop_y) * P.in_w + P.crop_x : nullptr;
+    const float* fin = FROM_RAW ? nullptr : in + m * width;
+    const float* pwrow = W.pw ? W.pw + ((size_t)g * rows + row) * width : nullptr;
+    auto weight = [&](int i) -> float {
+        return pwrow ? __ldg(pwrow + i) : __fdiv_rn(dmin, pw_dist(r, u_axis(i, width, W.det_right)));
+    };
+    auto pix = [&](int i) -> float { return FROM_RAW ? prep_pixel((float)src[i], P) : fin[i]; };
+    const bool vec4 = (width & 3) == 0 &&
+                      (FROM_RAW ? ((reinterpret_cast<uintptr_t>(src) & 7) == 0)
+                                : ((reinterpret_cast<uintptr_t>(fin) & 15) == 0)) &&
+                      (!pwrow || (reinterpret_cast<uintptr_t>(pwrow) & 15) == 0);
+    float v[kI8WarpGroups][4];
+    float mx = 0.0f;
+#pragma unroll
+    for (int gi = 0; gi < kI8WarpGroups; ++gi) {
+        const int i4 = gi * 128 + lane * 4;
+        if (gi * 128 >= width) break;
+        if (vec4 && i4 < width) {
+            float p[4], w[4];
+            if constexpr (FROM_RAW) {
+                const uint2 raw4 = *reinterpret_cast<const uint2*>(src + i4);
+                p[0] = prep_pixel((float)(raw4.x & 0xffffu), P); p[1] = prep_pixel((float)(raw4.x >> 16), P);
+                p[2] = prep_pixel((float)(raw4.y & 0xffffu), P); p[3] = prep_pixel((float)(raw4.y >> 16), P);
+            } else {
+                const float4 f = *reinterpret_cast<const float4*>(fin + i4);
+                p[0] = f.x; p[1] = f.y; p[2] = f.z; p[3] = f.w;
+            }
+            if (pwrow) {
+                const float4 q = __ldg(reinterpret_cast<const float4*>(pwrow + i4));
+                w[0] = q.x; w[1] = q.y; w[2] = q.z; w[3] = q.w;
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) w[k] = weight(i4 + k);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[gi][k] = __fmul_rn(p[k], w[k]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[gi][k] = i4 + k < width ? __fmul_rn(pix(i4 + k), weight(i4 + k)) : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) mx = fmaxf(mx, fabsf(v[gi][k]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    int E = 0;
+    if (mx > 0.0f && mx <= 3.0e38f) {
+        E = ilogbf(mx) - 6;
+        if (mx > ldexpf(127.0f, E)) ++E;
+    }
+    const float up = ldexpf(1.0f, 24 - E);
+    if (lane == 0) A.row_scale[m] = ldexpf(1.0f, E);
+    int8_t* plane = static_cast<int8_t*>(A.hi);
+    const size_t pstride = (size_t)(static_cast<int8_t*>(A.lo) - static_cast<int8_t*>(A.hi));
+#pragma unroll
+    for (int gi = 0; gi < kI8WarpGroups; ++gi) {
+        const int i4 = gi * 128 + lane * 4;
+        if (gi * 128 >= A.pitch) break;
+        if (i4 >= A.pitch) continue;
+        signed char d[kI8RowDigits][4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float x = (gi * 128 < width ? v[gi][k] : 0.0f) * up;
+            int q = __float2int_rn(fmaxf(-2130706432.0f, fminf(2130706432.0f, x)));
+#pragma unroll
+            for (int s2 = kI8RowDigits - 1; s2 > 0; --s2) {
+                const int lo = ((q + 128) & 255) - 128;
+                d[s2][k] = (signed char)lo;
+                q = (q - lo) >> 8;
+            }
+            d[0][k] = (signed char)q;
+        }
+#pragma unroll
+        for (int s2 = 0; s2 < kI8RowDigits; ++s2)
+            *reinterpret_cast<char4*>(plane + s2 * pstride + a0 + i4) = make_char4(d[s2][0], d[s2][1], d[s2][2], d[s2][3]);
+    }
+    if (lane == 0) {
         // FilterCore.cpp:203-214 -- mean of the three outermost unweighted samples
         const float edge = W.mirror ? __fdiv_rn(__fadd_rn(__fadd_rn(pix(width - 1), pix(width - 2)), pix(width - 3)), 3.0f)
                                     : __fdiv_rn(__fadd_rn(__fadd_rn(pix(0), pix(1)), pix(2)), 3.0f);
@@ -370,6 +541,15 @@ cudaError_t launch_weight_t(const PrepParams& p, const float* in, int nv, int v0
         case AOUT_TF32X2: weight_kernel<FROM_RAW, AOUT_TF32X2><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e); break;
         case AOUT_BF16X2: weight_kernel<FROM_RAW, AOUT_BF16X2><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e); break;
         case AOUT_FP16X2: weight_kernel<FROM_RAW, AOUT_FP16X2><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e); break;
+        case AOUT_I8X4:
+            if (A.pitch % 4 != 0) return cudaErrorInvalidValue;
+            if (!(FROM_RAW && w.comp.W > 0) && A.pitch <= 128 * kI8WarpGroups) {
+                weight_i8_kernel<FROM_RAW><<<dim3((rows + 7) / 8, nv), 256, 0, s>>>(p, in, width, rows, v0, w, A, e);
+                break;
+            }
+            if (width > 12288) return cudaErrorInvalidValue;   // the row in 48 KB of shared memory
+            weight_kernel<FROM_RAW, AOUT_I8X4><<<grid, threads, sizeof(float) * width, s>>>(p, in, width, rows, v0, w, A, e);
+            break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -75,8 +75,8 @@ def test_filter_matches_ramp_operator_and_oracle(torch_cuda, case, oracle):
     assert rel_l2(out, ref) <= 1e-5
 
 
-@pytest.mark.parametrize("kind,bar", [(1, 1e-5), (2, 5e-5), (3, 1e-5), (4, 1e-5)],
-                         ids=["tf32x3", "bf16x3", "fp16x3", "fp32-simt"])
+@pytest.mark.parametrize("kind,bar", [(1, 1e-5), (2, 5e-5), (3, 1e-5), (4, 1e-5), (5, 1e-7)],
+                         ids=["tf32x3", "bf16x3", "fp16x3", "fp32-simt", "i8x14"])
 def test_filter_ramp_products(torch_cuda, case, oracle, kind, bar):
     """Every ramp product against the oracle's FFT filter, in both forms."""
     from jenhine_b200 import _lib
@@ -89,6 +89,25 @@ def test_filter_ramp_products(torch_cuda, case, oracle, kind, bar):
         e.set_option(_lib.OPT_RAMP_PRODUCT, kind)
         out = e.filter(to_dev(torch_cuda, case["prep"]), v0=0).cpu().numpy()
         assert rel_l2(out, ref) <= bar, (form, rel_l2(out, ref))
+
+
+def test_int8_product_is_as_close_to_fp64_as_the_fft(torch_cuda, case, oracle):
+    """The int8 product (the FP32 form's default) against the FP64 filter:
+    no farther than the reference's float FFT filter (both start from the
+    same float pre-weighted rows, whose rounding sets the floor), and
+    within 1e-7 of that FFT filter."""
+    from jenhine_b200 import _lib
+    W = case["prep"].shape[2]
+    H = oracle.filter_spectrum(oracle.fft_length(W), float(case["hsr"]), *case["cut"], case["adj_pts"],
+                               case["adj_db"])
+    fft = oracle.filter_projections(case["prep"], case["ptms"], H, float(case["dso"]))
+    f64 = oracle.filter_projections_f64(case["prep"], case["ptms"], H, float(case["dso"]))
+    e = engine_for(case)
+    out = e.filter(to_dev(torch_cuda, case["prep"]), v0=0).cpu().numpy()
+    e.set_option(_lib.OPT_RAMP_PRODUCT, _lib.RAMP_I8X14)
+    assert np.array_equal(e.filter(to_dev(torch_cuda, case["prep"]), v0=0).cpu().numpy(), out)
+    assert rel_l2(out, fft) <= 1e-7
+    assert rel_l2(out, f64) <= 1.1 * rel_l2(fft, f64) + 1e-8, (rel_l2(out, f64), rel_l2(fft, f64))
 
 
 @pytest.mark.parametrize("exact", [True, False])

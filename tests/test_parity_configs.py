@@ -9,21 +9,20 @@ FilterCore + PreFilterWeightGenerator, BPCore, CTNumCore).
   bit for bit (BPCore.cpp:47-66), so the reference backprojects exactly the
   full volume's arithmetic there.
 
-Bars, as for the fixtures (test_gpu_parity.py):
+Bars:
   * preprocessing rel-L2 <= 1e-6 (GPU logf vs glibc);
-  * filter rel-L2 <= 1e-5 (dense Toeplitz product vs the FFT filter);
-  * EXACT-mode backprojection of the reference's filtered views: bit for bit,
-    and the set of voxels seen identical;
+  * filter rel-L2 <= 1e-6: the FP32 form's int8 product (exact integer
+    accumulation, rounded once) against the reference's float FFT filter,
+    both computing the same convolution of the same float pre-weighted rows;
+  * EXACT-mode backprojection of the reference's filtered views: bit for
+    bit, and the set of voxels seen identical;
   * default (fast) backprojection rel-L2 <= 1e-5;
   * CT numbers bit for bit given the same float volume;
   * the whole pipeline (the engine's own filter and backprojection) rel-L2 <=
-    1e-5 on the attenuation HU + 1000, in both backprojection modes, for c1.
-    For c2 the filter stage's 5e-6 (the dense product against the reference's
-    float FFT, both rounding the same exact convolution) grows to ~2.5e-5
-    through the backprojection's cancellations around the metal inserts, so
-    there the bar is that the engine is as close to the exact FDK (the FP64
-    oracle, tests/fp64_fdk.py) as the reference's own cores are -- its
-    rel-L2 to FP64 at most 1.25 x theirs -- and within 5e-5 of them.
+    1e-5 on the attenuation HU + 1000, in both backprojection modes.  For c2
+    the engine is also held against the exact FDK (the FP64 oracle,
+    tests/fp64_fdk.py): its rel-L2 to FP64 at most 1.1 x that of the
+    reference's own cores.
 The reference runs on all host cores, as its agents thread it
 (FilterAgent rows per thread, BPAgent slices per thread)."""
 import os
@@ -90,7 +89,7 @@ def check_config(torch, refcores, w, raw, fp64_oracle=None):
     res["prep"] = rel_l2_chunked(torch, raw_np, ref["prep"], lambda x, v0: exact.preprocess(x))
     res["filt"] = rel_l2_chunked(torch, ref["prep"], ref["filt"], lambda x, v0: exact.filter(x, v0=v0))
     assert res["prep"] <= 1e-6, res
-    assert res["filt"] <= 1e-5, res
+    assert res["filt"] <= 1e-6, res
     for name, e in (("exact", exact), ("fast", fast)):
         e.bp_reset()
         for v0 in range(0, w.geom.n_views, 50):
@@ -110,9 +109,9 @@ def check_config(torch, refcores, w, raw, fp64_oracle=None):
         res["recon_" + name] = rel_l2_seen(hus[name] + 1000.0, ref["hu"] + 1000.0)
     exact.close()
     fast.close()
+    for name in hus:
+        assert res["recon_" + name] <= 1e-5, res
     if fp64_oracle is None:
-        for name in hus:
-            assert res["recon_" + name] <= 1e-5, res
         return res
     from fp64_fdk import all_points, case_from_workload, fdk_f64, interior
     r = w.recon
@@ -126,8 +125,7 @@ def check_config(torch, refcores, w, raw, fp64_oracle=None):
     res["reference_vs_fp64"] = to_f64(ref["hu"].astype(np.float64))
     for name in hus:
         res[name + "_vs_fp64"] = to_f64(hus[name].astype(np.float64))
-        assert res[name + "_vs_fp64"] <= 1.25 * res["reference_vs_fp64"], res
-        assert res["recon_" + name] <= 5e-5, res
+        assert res[name + "_vs_fp64"] <= 1.1 * res["reference_vs_fp64"], res
     return res
 
 
