@@ -263,10 +263,20 @@ enum {
                                  JFDK_ERR_OOM, "CUDA failed to malloc ...".  Lets
                                  a caller sharing the GPU bound the engine, and
                                  choose the z-parts of jfdk_bp_set_slab ahead  */
-    JFDK_OPT_BP_TILE = 8      /* backprojection CTA width in x: 4 (4 x 32
+    JFDK_OPT_BP_TILE = 8,     /* backprojection CTA width in x: 4 (4 x 32
                                  threads), 8 (8 x 16) or 32 (32 x 4); 0
                                  (default): 4.  16-slice tiles are 4 wide.  The
                                  volume does not depend on it                  */
+    JFDK_OPT_BP_WEIGHTS = 9   /* FP32 form.  1 (default): a backprojection over
+                                 every view of the rotation (jfdk_reconstruct,
+                                 jfdk_reconstruct_host, jfdk_backproject_store)
+                                 divides by a volume of normalisation weights
+                                 computed once per geometry and backprojection
+                                 rounding (X*Y*Z floats, on first use) instead of
+                                 accumulating the taper per sample; the volume is
+                                 the same bit for bit.  Without room for it the
+                                 weights are accumulated per sample.  0: always
+                                 per sample                                     */
 };
 /* Ramp products (JFDK_OPT_RAMP_PRODUCT).  The split products run on the
  * tcgen05 tensor cores as hi*hi + hi*lo + lo*hi with FP32 accumulation; the

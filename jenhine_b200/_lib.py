@@ -30,6 +30,7 @@ OPT_FILTER_SIMT = 5
 OPT_RAMP_PRODUCT = 6
 OPT_DEVICE_MEMORY_LIMIT = 7
 OPT_BP_TILE = 8
+OPT_BP_WEIGHTS = 9
 AUTOTUNE_FORCE = 1
 BATCH_AUTOTUNE, BATCH_GRAPH, BATCH_PERSISTENT, BATCH_PIPELINED = 1, 2, 4, 8
 RAMP_DEFAULT, RAMP_TF32X3, RAMP_BF16X3, RAMP_FP16X3, RAMP_FP32_SIMT, RAMP_I8X14 = 0, 1, 2, 3, 4, 5

@@ -110,7 +110,8 @@ struct BatchTile {
 
 // The tile's (sum, weight) pairs: normalised, CT numbers, stored (FINALIZE),
 // or stored as accumulators.  The coordinates are asked for again here.
-template <int ZPT, bool FINALIZE, class Tile>
+// WV: the weights come from p.wvol (the whole volume, absolute slices).
+template <int ZPT, bool FINALIZE, class Tile, bool WV = false>
 __device__ __forceinline__ void epilogue(const BPParams& p, const Tile& tile, const float2 (&acc)[ZPT]) {
     const int x = tile.bx() * Tile::kX + threadIdx.x;
     const int y = tile.by() * Tile::kY + threadIdx.y;
@@ -120,7 +121,8 @@ __device__ __forceinline__ void epilogue(const BPParams& p, const Tile& tile, co
         if (zb + k >= p.z_end) break;
         if (FINALIZE) {
             const size_t idx = ((size_t)(zb + k - p.out_z0) * p.Y + y) * p.X + x;
-            float o = __fdiv_rn(acc[k].x, acc[k].y);   // BPCore::DoneSlice
+            const float wsum = WV ? __ldg(p.wvol + ((size_t)(zb + k) * p.Y + y) * p.X + x) : acc[k].y;
+            float o = __fdiv_rn(acc[k].x, wsum);   // BPCore::DoneSlice
             if (p.apply_ct) o = ct_number(o, p.ct_scale, p.ct_norm1);
             if (p.out) p.out[idx] = o;
             if (p.out16) p.out16[idx] = to_i16(o);
@@ -132,8 +134,12 @@ __device__ __forceinline__ void epilogue(const BPParams& p, const Tile& tile, co
     }
 }
 
-template <int ZPT, bool FINALIZE, bool EXACT, bool WZ, class Tile>
-__device__ __forceinline__ void bp_block(const BPParams& p, const Tile& tile) {
+// WV: the normalisation weights come from p.wvol (finalize over every view):
+// the view loop loads and accumulates only the projection samples.
+// WEIGHTS: the loop accumulates only the weights and stores them to out at
+// absolute slices (launch_bp_weights).
+template <int ZPT, bool FINALIZE, bool EXACT, bool WZ, class Tile, bool WV = false, bool WEIGHTS = false>
+__device__ __forceinline__ void bp_block(const BPParams& p, const Tile& tile, float* wout = nullptr) {
     const int x = tile.bx() * Tile::kX + threadIdx.x;
     const int y = tile.by() * Tile::kY + threadIdx.y;
     const int zb = p.z_begin + tile.bz() * ZPT;
@@ -177,27 +183,40 @@ __device__ __forceinline__ void bp_block(const BPParams& p, const Tile& tile) {
             const float2 fxy = psub(uv, psub(t, f2(kMagic, kMagic)));  // (u - fu, v - fv), exact
             const int ix = __float_as_int(t.x) - kMagicBits;
             const int idx = (__float_as_int(t.y) - kMagicBits) * p.U + ix;
-            const float4 Q = __ldg(q + idx);
-            const float2 w = __ldg(tw + ix);
-            const float2 lo = f2(Q.x, Q.y), d = f2(Q.z, Q.w);        // column ix, RN(column ix+1 - ix)
-            float val, c;
-            if (EXACT) {
-                const float t0 = __fadd_rn(lo.x, __fmul_rn(fxy.x, d.x));
-                const float t1 = __fadd_rn(lo.y, __fmul_rn(fxy.x, d.y));
-                val = __fadd_rn(t0, __fmul_rn(fxy.y, __fsub_rn(t1, t0)));
-                c = __fadd_rn(w.x, __fmul_rn(fxy.x, w.y));
-            } else {
-                const float2 t = pfma(f2(fxy.x, fxy.x), d, lo);
-                val = fmaf(fxy.y, t.y - t.x, t.x);
-                c = fmaf(fxy.x, w.y, w.x);
+            float val = 0.0f, c = 0.0f;
+            if constexpr (!WEIGHTS) {
+                const float4 Q = __ldg(q + idx);
+                const float2 lo = f2(Q.x, Q.y), d = f2(Q.z, Q.w);    // column ix, RN(column ix+1 - ix)
+                if (EXACT) {
+                    const float t0 = __fadd_rn(lo.x, __fmul_rn(fxy.x, d.x));
+                    const float t1 = __fadd_rn(lo.y, __fmul_rn(fxy.x, d.y));
+                    val = __fadd_rn(t0, __fmul_rn(fxy.y, __fsub_rn(t1, t0)));
+                } else {
+                    const float2 t = pfma(f2(fxy.x, fxy.x), d, lo);
+                    val = fmaf(fxy.y, t.y - t.x, t.x);
+                }
             }
-            if (in) acc[k] = padd(acc[k], f2(val, c));
+            if constexpr (!WV) {
+                const float2 w = __ldg(tw + ix);
+                c = EXACT ? __fadd_rn(w.x, __fmul_rn(fxy.x, w.y)) : fmaf(fxy.x, w.y, w.x);
+            }
+            if (in) {   // the same roundings as the packed add of (val, c)
+                if constexpr (WV) acc[k].x = __fadd_rn(acc[k].x, val);
+                else if constexpr (WEIGHTS) acc[k].y = __fadd_rn(acc[k].y, c);
+                else acc[k] = padd(acc[k], f2(val, c));
+            }
         }
     }
 
+    if constexpr (WEIGHTS) {
+#pragma unroll
+        for (int k = 0; k < ZPT; ++k)
+            if (zb + k < p.z_end) wout[((size_t)(zb + k) * p.Y + y) * p.X + x] = acc[k].y;
+        return;
+    }
     // The output index is formed here, not before the view loop, so that it
     // holds no registers across the loop.
-    epilogue<ZPT, FINALIZE>(p, tile, acc);
+    epilogue<ZPT, FINALIZE, Tile, WV>(p, tile, acc);
 }
 
 // ---- mixed precision ---------------------------------------------------------
@@ -307,9 +326,14 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& ti
 }
 
 // One CTA = one TX x (128 / TX) x ZPT voxel tile of one launch's grid.
-template <int ZPT, bool FINALIZE, bool EXACT, bool WZ, int TX>
+template <int ZPT, bool FINALIZE, bool EXACT, bool WZ, int TX, bool WV = false>
 __global__ void __launch_bounds__(kBPThreads, bp_fp32_min_blocks(ZPT)) bp_kernel(BPParams p) {
-    bp_block<ZPT, FINALIZE, EXACT, WZ>(p, GridTile<TX>{});
+    bp_block<ZPT, FINALIZE, EXACT, WZ, GridTile<TX>, WV>(p, GridTile<TX>{});
+}
+
+template <int ZPT, bool EXACT, bool WZ, int TX>
+__global__ void __launch_bounds__(kBPThreads, bp_fp32_min_blocks(ZPT)) bp_weights_kernel(BPParams p, float* out) {
+    bp_block<ZPT, true, EXACT, WZ, GridTile<TX>, false, true>(p, GridTile<TX>{}, out);
 }
 
 template <int ZPT, bool FINALIZE, bool WZ, int TX>
@@ -526,8 +550,39 @@ dim3 bp_grid(const BPParams& p, int zpt) {
 
 template <int ZPT, bool F, bool E, bool WZ, int TX>
 cudaError_t go(const BPParams& p, cudaStream_t s) {
+    if constexpr (F) {
+        if (p.wvol) {
+            bp_kernel<ZPT, F, E, WZ, TX, true><<<bp_grid<TX>(p, ZPT), dim3(TX, kBPThreads / TX), 0, s>>>(p);
+            return cudaGetLastError();
+        }
+    }
     bp_kernel<ZPT, F, E, WZ, TX><<<bp_grid<TX>(p, ZPT), dim3(TX, kBPThreads / TX), 0, s>>>(p);
     return cudaGetLastError();
+}
+
+template <int ZPT, bool E, bool WZ>
+cudaError_t go_weights(const BPParams& p, int tx, float* out, cudaStream_t s) {
+    if constexpr (ZPT != 16) {
+        if (tx == 8) {
+            bp_weights_kernel<ZPT, E, WZ, 8><<<bp_grid<8>(p, ZPT), dim3(8, kBPThreads / 8), 0, s>>>(p, out);
+            return cudaGetLastError();
+        }
+        if (tx == 32) {
+            bp_weights_kernel<ZPT, E, WZ, 32><<<bp_grid<32>(p, ZPT), dim3(32, kBPThreads / 32), 0, s>>>(p, out);
+            return cudaGetLastError();
+        }
+    }
+    bp_weights_kernel<ZPT, E, WZ, 4><<<bp_grid<4>(p, ZPT), dim3(4, kBPThreads / 4), 0, s>>>(p, out);
+    return cudaGetLastError();
+}
+
+template <bool E, bool WZ>
+cudaError_t go_weights2(const BPParams& p, int zpt, int tx, float* out, cudaStream_t s) {
+    switch (zpt) {
+        case 16: return go_weights<16, E, WZ>(p, tx, out, s);
+        case 8: return go_weights<8, E, WZ>(p, tx, out, s);
+        default: return go_weights<4, E, WZ>(p, tx, out, s);
+    }
 }
 
 // Tile widths 4, 8 and 32 for the tile depths the autotuner chooses between
@@ -588,6 +643,16 @@ cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depen
                      : go3<true, false>(p, w_depends_on_z, zpt, tile_x, s);
     return exact ? go3<false, true>(p, w_depends_on_z, zpt, tile_x, s)
                  : go3<false, false>(p, w_depends_on_z, zpt, tile_x, s);
+}
+
+cudaError_t launch_bp_weights(const BPParams& p, bool exact, bool w_depends_on_z, int zpt, int tile_x, float* out,
+                              cudaStream_t s) {
+    if (!out || p.v0 != 0) return cudaErrorInvalidValue;
+    if (exact)
+        return w_depends_on_z ? go_weights2<true, true>(p, zpt, tile_x, out, s)
+                              : go_weights2<true, false>(p, zpt, tile_x, out, s);
+    return w_depends_on_z ? go_weights2<false, true>(p, zpt, tile_x, out, s)
+                          : go_weights2<false, false>(p, zpt, tile_x, out, s);
 }
 
 cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, int tile_x,

@@ -274,7 +274,55 @@ jfdk_status pack_frames(jfdk_ctx* c, const float* plain, int nv, int view0, int 
     return JFDK_OK;
 }
 
+bool capturing(cudaStream_t s) {
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &st) != cudaSuccess) {
+        cudaGetLastError();
+        return true;   // the legacy stream while another stream captures
+    }
+    return st != cudaStreamCaptureStatusNone;
+}
+
+// The FP32 form's normalisation weights over every view (JFDK_OPT_BP_WEIGHTS),
+// computed once per geometry and rounding mode on the context's stream,
+// which is then synchronised, so later launches on any stream (and graph
+// captures) read finished weights with no event between them.  False
+// (nothing set) when the option is off, when a capture is under way and the
+// weights are not ready, or when the volume does not fit -- within
+// JFDK_OPT_DEVICE_MEMORY_LIMIT and the device -- and the weights are then
+// accumulated per sample.
+bool ensure_weights(jfdk_ctx* c, cudaStream_t s) {
+    if (mixed(c) || !c->opt_bp_weights) return false;
+    const int want = c->opt_bp_exact ? 2 : 1;
+    if (c->d_wvol && c->wvol_state == want) return true;
+    if (capturing(c->stream) || capturing(s)) return false;
+    if (!c->d_wvol) {
+        const size_t bytes = (size_t)c->X * c->Y * c->Z * sizeof(float);
+        if (c->mem_limit > 0 && c->dev_bytes + (long long)bytes > c->mem_limit) return false;
+        void* q = nullptr;
+        if (cudaMalloc(&q, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        c->alloc_bytes[q] = bytes;
+        c->dev_bytes += (long long)bytes;
+        c->d_wvol = static_cast<float*>(q);
+    }
+    BPParams b = bp_params(c);
+    b.view_base = 0; b.v0 = 0; b.nv = c->nviews;
+    c->wvol_state = 0;
+    if (launch_bp_weights(b, c->opt_bp_exact != 0, c->w_depends_on_z, bp_zpt(c), bp_tile(c), c->d_wvol, c->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    c->wvol_state = want;
+    return true;
+}
+
 jfdk_status run_bp_on(jfdk_ctx* c, BPParams b, bool finalize, cudaStream_t s) {
+    if (finalize && b.v0 == 0 && b.nv == c->nviews && ensure_weights(c, s)) b.wvol = c->d_wvol;
     if (mixed(c)) {
         b.qh = reinterpret_cast<const uint4*>(c->d_q4);
         b.qscale = c->d_qscale;
@@ -443,6 +491,7 @@ void jfdk_destroy(jfdk_ctx* c) {
     dev_free(c, c->d_sum); dev_free(c, c->d_cnt); dev_free(c, c->d_raw_stage); dev_free(c, c->d_hu_stage);
     dev_free(c, c->d_Tt); dev_free(c, c->d_rt); dev_free(c, c->d_qadj); dev_free(c, c->d_partial);
     dev_free(c, c->d_dptm);
+    dev_free(c, c->d_wvol);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     for (cudaStream_t s : {c->copy_stream, c->aux_stream}) {
@@ -673,6 +722,7 @@ jfdk_status jfdk_set_option(jfdk_ctx* c, int key, long long value) {
             c->opt_bp_tile = (int)value;
             return JFDK_OK;
         case JFDK_OPT_FILTER_SIMT: c->opt_ramp = value ? JFDK_RAMP_FP32_SIMT : JFDK_RAMP_DEFAULT; return JFDK_OK;
+        case JFDK_OPT_BP_WEIGHTS: c->opt_bp_weights = value ? 1 : 0; return JFDK_OK;
         case JFDK_OPT_RAMP_PRODUCT:
             if (value < JFDK_RAMP_DEFAULT || value > JFDK_RAMP_I8X14)
                 return fail(c, JFDK_ERR_INVALID, "unknown ramp product");
@@ -842,6 +892,7 @@ jfdk_status jfdk_reconstruct(jfdk_ctx* c, const uint16_t* d_raw, float* d_hu, in
     jfdk_status st = jfdk::reconstruct_filter_stage(c, d_raw, c->nviews);
     if (st) return st;
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[1], c->stream), "event");
+    ensure_weights(c, c->stream);   // once per geometry, outside the timed stages
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[2], c->stream), "event");
     if ((st = run_bp(c, jfdk::reconstruct_bp_params(c, d_hu, d_hu16), true))) return st;
     if (timing) JFDK_CUDA(c, cudaEventRecord(c->ev[3], c->stream), "event");
@@ -1080,6 +1131,7 @@ extern "C" {
 jfdk_status jfdk_set_bp_geometry(jfdk_ctx* c, const float* h_ptms) {
     if (!c || !h_ptms) return fail(c, JFDK_ERR_INVALID, "set_bp_geometry: bad argument");
     c->ptms.assign(h_ptms, h_ptms + (size_t)c->nviews * 12);
+    c->wvol_state = 0;   // the normalisation weights follow the geometry
     c->w_depends_on_z = false;
     for (int v = 0; v < c->nviews; ++v)
         if (c->ptms[(size_t)v * 12 + 10] != 0.0f) c->w_depends_on_z = true;
@@ -1262,6 +1314,7 @@ extern "C" jfdk_status jfdk_autotune(jfdk_ctx* c, int flags) {
     if ((st = dev_alloc(c, &slab, plane * nz, "the autotuner's slab"))) return st;
     int best_z = 8, best_x = kBPTileX;
     float best_t = 1e30f;
+    ensure_weights(c, c->stream);   // not inside the first candidate's time
     for (int zpt : {4, 8}) {
         for (int tx : {4, 8, 32}) {
             c->opt_bp_zpt = zpt;

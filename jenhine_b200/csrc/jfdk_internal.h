@@ -63,6 +63,10 @@ struct BPParams {
     int out_z0;
     int apply_ct;
     float ct_scale, ct_norm1;
+    // finalize over every view of the rotation, FP32 form: the normalisation
+    // weights of the whole volume [Z][Y][X] (launch_bp_weights), so the view
+    // loop accumulates the projections only; null: accumulated per sample
+    const float* wvol;
 };
 
 // One scan of a batched backprojection (bp_batch_kernel): its parameters
@@ -82,6 +86,13 @@ struct BatchScan {
 // (CTAs of 128 threads; other values and 16-slice tiles take 4).
 cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depends_on_z, int zpt, int tile_x,
                       cudaStream_t s);
+// The FP32 form's normalisation weights of every voxel of the volume over
+// every view of the rotation (p.v0 = 0, p.nv = all views, slices
+// [p.z_begin, p.z_end)), into out [Z][Y][X] at absolute slices: the weight
+// sums bp_kernel accumulates beside the projections, bit for bit (the same
+// coordinates, taper lerp and view order).
+cudaError_t launch_bp_weights(const BPParams& p, bool exact, bool w_depends_on_z, int zpt, int tile_x, float* out,
+                              cudaStream_t s);
 // A batched backprojection launch covers up to kBatchSlots scans that share
 // whether W depends on z (each with its own tile depth, 4 or 8 slices); their
 // parameters travel in the kernel's parameter space (16 slots: ~4.4 KB of the
@@ -319,6 +330,9 @@ struct jfdk_ctx {
     int opt_bp_zpt = 0;          // 0: default (bp_zpt() in jfdk_api.cpp)
     int opt_bp_tile = 0;         // tile width in x: 4, 8 or 32; 0: default (4)
     int opt_ramp = 0;            // JFDK_OPT_RAMP_PRODUCT (0: the form's default)
+    int opt_bp_weights = 1;      // JFDK_OPT_BP_WEIGHTS
+    float* d_wvol = nullptr;     // normalisation weights [Z][Y][X] (FP32 form)
+    int wvol_state = 0;          // 0: none, 1: valid for the fast rounding, 2: for EXACT
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // jfdk_reconstruct_host: a copy stream and a second compute stream, and
     // their events (created on first use)

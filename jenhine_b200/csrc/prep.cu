@@ -428,11 +428,11 @@ __global__ void __launch_bounds__(256) weight_kernel(PrepParams P, const float* 
 }
 
 // The int8 digit form with one warp per row: the row's values stay in
-// registers (width <= 32 * 4 * kI8WarpGroups), the scale's maximum is a
-// warp reduction; the same values, scale and digits as weight_kernel's
-// AOUT_I8X4 path.  No compositing (weight_kernel handles it).
+// registers (pitch <= 128 * G), the scale's maximum is a warp reduction;
+// the same values, scale and digits as weight_kernel's AOUT_I8X4 path.  No
+// compositing (weight_kernel handles it).
 constexpr int kI8WarpGroups = 16;
-template <bool FROM_RAW>
+template <bool FROM_RAW, int G>
 __global__ void __launch_bounds__(256) weight_i8_kernel(PrepParams P, const float* __restrict__ in, int width,
                                                         int rows, int v0, WeightParams W, AOperand A,
                                                         float* __restrict__ e) {
@@ -459,10 +459,10 @@ __global__ void __launch_bounds__(256) weight_i8_kernel(PrepParams P, const floa
                       (FROM_RAW ? ((reinterpret_cast<uintptr_t>(src) & 7) == 0)
                                 : ((reinterpret_cast<uintptr_t>(fin) & 15) == 0)) &&
                       (!pwrow || (reinterpret_cast<uintptr_t>(pwrow) & 15) == 0);
-    float v[kI8WarpGroups][4];
+    float v[G][4];
     float mx = 0.0f;
 #pragma unroll
-    for (int gi = 0; gi < kI8WarpGroups; ++gi) {
+    for (int gi = 0; gi < G; ++gi) {
         const int i4 = gi * 128 + lane * 4;
         if (gi * 128 >= width) break;
         if (vec4 && i4 < width) {
@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(256) weight_i8_kernel(PrepParams P, const floa
     int8_t* plane = static_cast<int8_t*>(A.hi);
     const size_t pstride = (size_t)(static_cast<int8_t*>(A.lo) - static_cast<int8_t*>(A.hi));
 #pragma unroll
-    for (int gi = 0; gi < kI8WarpGroups; ++gi) {
+    for (int gi = 0; gi < G; ++gi) {
         const int i4 = gi * 128 + lane * 4;
         if (gi * 128 >= A.pitch) break;
         if (i4 >= A.pitch) continue;
@@ -544,7 +544,13 @@ cudaError_t launch_weight_t(const PrepParams& p, const float* in, int nv, int v0
         case AOUT_I8X4:
             if (A.pitch % 4 != 0) return cudaErrorInvalidValue;
             if (!(FROM_RAW && w.comp.W > 0) && A.pitch <= 128 * kI8WarpGroups) {
-                weight_i8_kernel<FROM_RAW><<<dim3((rows + 7) / 8, nv), 256, 0, s>>>(p, in, width, rows, v0, w, A, e);
+                const dim3 g8((rows + 7) / 8, nv);
+                if (A.pitch <= 128 * 6)
+                    weight_i8_kernel<FROM_RAW, 6><<<g8, 256, 0, s>>>(p, in, width, rows, v0, w, A, e);
+                else if (A.pitch <= 128 * 8)
+                    weight_i8_kernel<FROM_RAW, 8><<<g8, 256, 0, s>>>(p, in, width, rows, v0, w, A, e);
+                else
+                    weight_i8_kernel<FROM_RAW, kI8WarpGroups><<<g8, 256, 0, s>>>(p, in, width, rows, v0, w, A, e);
                 break;
             }
             if (width > 12288) return cudaErrorInvalidValue;   // the row in 48 KB of shared memory

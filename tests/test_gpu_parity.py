@@ -131,6 +131,27 @@ def test_backprojection_in_chunks_equals_one_pass(torch_cuda, case):
     np.testing.assert_array_equal(e.finalize(apply_ctnum=False).cpu().numpy(), case["bp"])
 
 
+@pytest.mark.parametrize("exact", [True, False])
+def test_weight_volume_is_bit_identical(torch_cuda, case, exact):
+    """The FP32 form divides by a once-per-geometry volume of normalisation
+    weights (JFDK_OPT_BP_WEIGHTS, default on): the same volume bit for bit as
+    with the weights accumulated per sample, in both roundings, and again
+    after the geometry changes (the weights follow it)."""
+    torch = torch_cuda
+    from jenhine_b200 import _lib
+    raw = to_dev(torch, case["raw"])
+    on = engine_for(case, bp_exact=exact)
+    off = engine_for(case, bp_exact=exact)
+    off.set_option(_lib.OPT_BP_WEIGHTS, 0)
+    same = lambda a, b: torch.equal(torch.nan_to_num(a, 1e30), torch.nan_to_num(b, 1e30))
+    assert same(on.reconstruct(raw).clone(), off.reconstruct(raw).clone())
+    ptms = np.array(case["ptms"], np.float32).reshape(-1, 12).copy()
+    ptms[:, 3] += 0.25 * ptms[:, 11]          # shift the detector by a quarter pixel in u
+    on.set_bp_geometry(ptms)
+    off.set_bp_geometry(ptms)
+    assert same(on.reconstruct(raw).clone(), off.reconstruct(raw).clone())
+
+
 def test_ctnum_bit_exact(torch_cuda, case):
     e = engine_for(case)
     vol = to_dev(torch_cuda, case["bp"])
