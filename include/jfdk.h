@@ -231,8 +231,9 @@ jfdk_status jfdk_filter_raw(jfdk_ctx* ctx, const uint16_t* d_raw, int v0, int nv
  * (and, when compositing, of their conjugates) are read. */
 jfdk_status jfdk_filter_to_store(jfdk_ctx* ctx, const uint16_t* d_raw, int v0, int nv);
 /* Device address and size of the store's records of views [v0, v0+nv)
- * (contiguous, views in order) and, in the mixed form, of their per-view
- * scales (4 bytes a view; *d_scales = NULL in the FP32 form). */
+ * (contiguous, views in order; 16 bytes a pixel in the FP32 form, 8 in the
+ * mixed form) and, in the mixed form, of their per-view scales (4 bytes a
+ * view; *d_scales = NULL in the FP32 form). */
 jfdk_status jfdk_store_range(jfdk_ctx* ctx, int v0, int nv, void** d_records, size_t* record_bytes,
                              float** d_scales);
 /* The finalizing backprojection of every view in the store, with CT numbers,
@@ -267,7 +268,7 @@ enum {
                                  threads), 8 (8 x 16) or 32 (32 x 4); 0
                                  (default): 4.  16-slice tiles are 4 wide.  The
                                  volume does not depend on it                  */
-    JFDK_OPT_BP_WEIGHTS = 9   /* FP32 form.  1 (default): a backprojection over
+    JFDK_OPT_BP_WEIGHTS = 9   /* 1 (default): a backprojection over
                                  every view of the rotation (jfdk_reconstruct,
                                  jfdk_reconstruct_host, jfdk_backproject_store)
                                  divides by a volume of normalisation weights

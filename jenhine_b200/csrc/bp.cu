@@ -220,40 +220,59 @@ __device__ __forceinline__ void bp_block(const BPParams& p, const Tile& tile, fl
 }
 
 // ---- mixed precision ---------------------------------------------------------
-// Record per (slot, row r, column c), 16 bytes: the tapered footprint
-// p00 = p[r][c], p01 = p[r][c+1], p10 = p[r+1][c], p11 = p[r+1][c+1],
-// divided by the view's power-of-two scale s, as the coefficients of the
+// Record per (slot, row r, column c), 8 bytes, the tapered footprint
+// p00 = p[r][c], p01 = p[r][c+1], p10 = p[r+1][c], p11 = p[r+1][c+1] divided
+// by the view's power-of-two scale s, in FP16, as the coefficients of the
 // bilinear form  val = p00 + fx dx + fy (dy + fx dxy):
-//   .x  float p00 / s                  (exact)
-//   .y  half2 (dx = p01 - p00, dxy = p11 - p10 - p01 + p00) / s
-//   .z  half2 (dy = p10 - p00) / s, w[c+1] - w[c]   (the taper's step)
-//   .w  float w[c]                     the taper at c
-// so one 16-byte load per sample fetches everything the sample needs, and
-// the interpolation is three FP16 x FP16 + FP32 fused multiply-adds
-// (fma.rn.f32.f16, products exact in FP32; the FP32 addends p00 and w[c]
-// need no conversion) and one FP32 one.
+//   .x  half2 (p00, dx = p01 - p00)
+//   .y  half2 (dy = p10 - p00, dxy = p11 - p10 - p01 + p00)
+// each difference rounded against the already rounded coefficients, so every
+// corner the form reproduces carries the rounding of one coefficient only.
+// The records of the last row and the last column are zero: their samples
+// are not taken (below), and an index clamped onto them reads nothing.
+// The interpolation is two FP16 x FP16 + FP32 fused multiply-adds
+// (fma.rn.f32.f16, products exact in FP32) and one FP32 one.
 // The coordinates use an approximate reciprocal of W and fused
 // multiply-adds; when W does not depend on z the slices of a thread are
 // equally spaced on the detector and u, v advance by a constant per slice.
 // A sample is taken when floor(u) <= cols-2 and floor(v) <= rows-2 (the
 // same set as 0 <= u <= cols-1, 0 <= v <= rows-1 up to the measure-zero
-// points u = cols-1, v = rows-1), tested on the integer parts.  The lerps,
-// the rescale by s and the (sum, weight) accumulation are FP32.
+// points u = cols-1, v = rows-1) and W > 0.  The lerps, the rescale by s and
+// the (sum, weight) accumulation are FP32; the weight is the FP32 taper
+// pair's lerp at the sample's FP32 fraction.
+// WV: the weights come from p.wvol (finalize over every view), so the loop
+// clamps the index onto the zero records instead of testing the range and
+// loads one record per sample.  WEIGHTS: the loop accumulates only the
+// weights and stores them to out at absolute slices.
 __device__ __forceinline__ float rcp_approx(float x) {
     float r;
     asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
 
-template <int ZPT, bool FINALIZE, bool WZ, class Tile>
-__device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& tile) {
+// p00 + fx dx + fy (dy + fx dxy) of an 8-byte record (fx rounded to FP16).
+__device__ __forceinline__ float mixed_lerp(uint2 rec, float2 f) {
+    float v1, inner;
+    asm("{\n .reg .f16 p0, dx, dy, dxy, fh;\n .reg .f32 p0f, dyf;\n"
+        " mov.b32 {p0, dx}, %2;\n mov.b32 {dy, dxy}, %3;\n"
+        " cvt.rn.f16.f32 fh, %4;\n cvt.f32.f16 p0f, p0;\n cvt.f32.f16 dyf, dy;\n"
+        " fma.rn.f32.f16 %0, fh, dx, p0f;\n fma.rn.f32.f16 %1, fh, dxy, dyf;\n}"
+        : "=f"(v1), "=f"(inner)
+        : "r"(rec.x), "r"(rec.y), "f"(f.x));
+    return fmaf(f.y, inner, v1);
+}
+
+template <int ZPT, bool FINALIZE, bool WZ, class Tile, bool WV = false, bool WEIGHTS = false>
+__device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& tile, float* wout = nullptr) {
     const int x = tile.bx() * Tile::kX + threadIdx.x;
     const int y = tile.by() * Tile::kY + threadIdx.y;
     const int zb = p.z_begin + tile.bz() * ZPT;
     if (x >= p.X || y >= p.Y) return;
-    const float ax = (x - 0.5f * (p.X - 1)) * p.pxy;
-    const float ay = (y - 0.5f * (p.Y - 1)) * p.pxy;
-    const float az0 = (zb - 0.5f * (p.Z - 1)) * p.pz;
+    // every rounding explicit, so that each kernel built from this body
+    // (per-scan, batch, weights) forms the same coordinates
+    const float ax = __fmul_rn(__fadd_rn((float)x, -0.5f * (float)(p.X - 1)), p.pxy);
+    const float ay = __fmul_rn(__fadd_rn((float)y, -0.5f * (float)(p.Y - 1)), p.pxy);
+    const float az0 = __fmul_rn(__fadd_rn((float)zb, -0.5f * (float)(p.Z - 1)), p.pz);
     float2 acc[ZPT];  // (sum, weight)
 #pragma unroll
     for (int k = 0; k < ZPT; ++k) {
@@ -268,15 +287,17 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& ti
 
     const float4* P4 = reinterpret_cast<const float4*>(p.ptm + (size_t)p.v0 * 12);
     const float* sc = p.qscale + p.v0;
-    const uint4* __restrict__ q = p.qh + (size_t)(p.v0 - p.view_base) * p.q4_frame;
+    const uint2* __restrict__ q = p.qh + (size_t)(p.v0 - p.view_base) * p.q4_frame;
+    const float2* __restrict__ tw = p.tw + (size_t)p.v0 * p.U;
 #pragma unroll 1
-    for (int n = 0; n < p.nv; ++n, P4 += 3, ++sc, q += p.q4_frame) {
+    for (int n = 0; n < p.nv; ++n, P4 += 3, ++sc, q += p.q4_frame, tw += p.U) {
         const float4 r0 = __ldg(P4), r1 = __ldg(P4 + 1), r2 = __ldg(P4 + 2);
         const float2 P26 = f2(r0.z, r1.z);
         // U, V, W at slice zb
         const float2 UV0 = pfma(f2(az0, az0), P26,
                                 pfma(f2(ax, ax), f2(r0.x, r1.x), pfma(f2(ay, ay), f2(r0.y, r1.y), f2(r0.w, r1.w))));
         const float W0 = fmaf(az0, r2.z, fmaf(ax, r2.x, fmaf(ay, r2.y, r2.w)));
+        if (!WZ && !(W0 > 0.0f)) continue;   // a point at or behind the source plane samples nothing
         // !WZ: (u, v) itself steps from slice to slice.  WZ: U, V and W step
         // (one add each per slice, no per-slice offsets held through the loop)
         float2 uv = f2(0.f, 0.f), duv = f2(0.f, 0.f), UVk = UV0;
@@ -284,21 +305,25 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& ti
         if (!WZ) {
             const float r = rcp_approx(W0);
             uv = pfma(UV0, f2(r, r), f2(0.5f, 0.5f));
-            const float rz = r * p.pz;
-            duv = pmul(P26, f2(rz, rz));
+            const float rz = __fmul_rn(r, p.pz);
+            duv = f2(__fmul_rn(P26.x, rz), __fmul_rn(P26.y, rz));
         } else {
-            duv = pmul(P26, f2(p.pz, p.pz));
-            dW = p.pz * r2.z;
+            duv = f2(__fmul_rn(P26.x, p.pz), __fmul_rn(P26.y, p.pz));
+            dW = __fmul_rn(p.pz, r2.z);
         }
+        // (scalar products: a packed product feeding the packed adds below
+        // may be fused into them, differently in each kernel built from here)
         const float s = __ldg(sc);
 #pragma unroll
         for (int k = 0; k < ZPT; ++k) {
             float2 cuv;
+            bool front = true;
             if (WZ) {
                 const float r = rcp_approx(Wk);
+                front = Wk > 0.0f;
                 cuv = pfma(UVk, f2(r, r), f2(0.5f, 0.5f));
                 UVk = padd(UVk, duv);
-                Wk += dW;
+                Wk = __fadd_rn(Wk, dW);
             } else {
                 cuv = uv;              // slice k: uv0 + k duv, stepped
                 uv = padd(uv, duv);
@@ -307,22 +332,30 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& ti
             const float2 f = psub(cuv, psub(t, magic));               // fractions
             const unsigned iu = __float_as_uint(t.x) - (unsigned)kMagicBits;
             const unsigned iv = __float_as_uint(t.y) - (unsigned)kMagicBits;
-            const bool in = (iu < um1) & (iv < vm1);                  // negative / NaN wrap to large
-            const unsigned idx = in ? iv * uu + iu : 0u;
-            const uint4 rec = __ldg(q + idx);
-            float v1, inner, c;   // p00 + fx dx, dy + fx dxy, w + fx dw (fx rounded to FP16)
-            asm("{\n .reg .f16 dx, dxy, dy, dw, fh;\n .reg .f32 dyf;\n"
-                " mov.b32 {dx, dxy}, %4;\n mov.b32 {dy, dw}, %5;\n"
-                " cvt.rn.f16.f32 fh, %7;\n cvt.f32.f16 dyf, dy;\n"
-                " fma.rn.f32.f16 %0, fh, dx, %3;\n fma.rn.f32.f16 %1, fh, dxy, dyf;\n"
-                " fma.rn.f32.f16 %2, fh, dw, %6;\n}"
-                : "=f"(v1), "=f"(inner), "=f"(c)
-                : "f"(__uint_as_float(rec.x)), "r"(rec.y), "r"(rec.z), "f"(__uint_as_float(rec.w)), "f"(f.x));
-            const float val = fmaf(f.y, inner, v1);
-            if (in) acc[k] = pfma(f2(s, 1.0f), f2(val, c), acc[k]);
+            if constexpr (WV) {
+                // out of range (negative / NaN wrap to large): a zero record
+                const float val = mixed_lerp(__ldg(q + (min(iv, vm1) * uu + min(iu, um1))), f);
+                if (front) acc[k].x = fmaf(s, val, acc[k].x);
+            } else {
+                const bool in = (iu < um1) & (iv < vm1) & front;
+                const float2 w = __ldg(tw + (in ? iu : 0u));
+                const float c = fmaf(f.x, w.y, w.x);
+                if constexpr (WEIGHTS) {
+                    if (in) acc[k].y = __fadd_rn(acc[k].y, c);
+                } else {
+                    const float val = mixed_lerp(__ldg(q + (in ? iv * uu + iu : 0u)), f);
+                    if (in) acc[k] = pfma(f2(s, 1.0f), f2(val, c), acc[k]);   // (s val + sum, c + weight)
+                }
+            }
         }
     }
-    epilogue<ZPT, FINALIZE>(p, tile, acc);
+    if constexpr (WEIGHTS) {
+#pragma unroll
+        for (int k = 0; k < ZPT; ++k)
+            if (zb + k < p.z_end) wout[((size_t)(zb + k) * p.Y + y) * p.X + x] = acc[k].y;
+        return;
+    }
+    epilogue<ZPT, FINALIZE, Tile, WV>(p, tile, acc);
 }
 
 // One CTA = one TX x (128 / TX) x ZPT voxel tile of one launch's grid.
@@ -336,12 +369,17 @@ __global__ void __launch_bounds__(kBPThreads, bp_fp32_min_blocks(ZPT)) bp_weight
     bp_block<ZPT, true, EXACT, WZ, GridTile<TX>, false, true>(p, GridTile<TX>{}, out);
 }
 
-template <int ZPT, bool FINALIZE, bool WZ, int TX>
+template <int ZPT, bool FINALIZE, bool WZ, int TX, bool WV = false>
 __global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_mixed_kernel(BPParams p) {
     if constexpr (WZ)
-        bp_mixed_block<ZPT, FINALIZE, WZ>(p, GridTile<TX>{});
+        bp_mixed_block<ZPT, FINALIZE, WZ, GridTile<TX>, WV>(p, GridTile<TX>{});
     else
-        bp_mixed_block<ZPT, FINALIZE, WZ>(p, GridTileHeld<TX>{});
+        bp_mixed_block<ZPT, FINALIZE, WZ, GridTileHeld<TX>, WV>(p, GridTileHeld<TX>{});
+}
+
+template <int ZPT, bool WZ, int TX>
+__global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_mixed_weights_kernel(BPParams p, float* out) {
+    bp_mixed_block<ZPT, true, WZ, GridTile<TX>, false, true>(p, GridTile<TX>{}, out);
 }
 
 // Persistent backprojection over the tiles of up to kBatchSlots scans: each
@@ -433,7 +471,7 @@ __device__ __forceinline__ float view_scale(unsigned maxbits) {
 __global__ void __launch_bounds__(256) pack_mixed_kernel(const float* __restrict__ plain, long long plain_frame,
                                                          int rows, int U, const float2* __restrict__ tw, int view0,
                                                          int num_views, const unsigned* __restrict__ absmax,
-                                                         float* __restrict__ scale, uint4* __restrict__ qh,
+                                                         float* __restrict__ scale, uint2* __restrict__ qh,
                                                          long long q_frame, int slot0) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int r = blockIdx.y, f = blockIdx.z;
@@ -442,26 +480,21 @@ __global__ void __launch_bounds__(256) pack_mixed_kernel(const float* __restrict
     const float s = view_scale(absmax[f]);
     const float inv = __fdiv_rn(1.0f, s);
     if (r == 0 && c == 0) scale[view] = s;
-    const float* src = plain + (size_t)f * plain_frame + (size_t)r * U + c;
-    const bool right = c + 1 < U, down = r + 1 < rows;
-    const float2 w = tw[(size_t)view * U + c];                      // (w[c], RN(w[c+1] - w[c]))
-    const float w1 = right ? tw[(size_t)view * U + c + 1].x : 0.0f;
-    const float p00 = src[0] * w.x, p10 = down ? src[U] * w.x : 0.0f;
-    const float p01 = right ? src[1] * w1 : 0.0f, p11 = (right && down) ? src[U + 1] * w1 : 0.0f;
-    // p00 is kept in FP32; each difference is rounded against the already
-    // rounded ones, so every corner the form reproduces carries the rounding
-    // of one coefficient only: p01 that of dx (a difference, usually far
-    // smaller than the values), p10 that of dy, p11 that of dxy.
-    const float a = p00 * inv, b = p01 * inv, cc = p10 * inv, d = p11 * inv;   // exact: inv a power of two
-    const __half hdx = __float2half_rn(b - a), hdy = __float2half_rn(cc - a);
-    const __half hdxy = __float2half_rn(d - (a + __half2float(hdx) + __half2float(hdy)));
-    const __half2 d1 = __halves2half2(hdx, hdxy);
-    const __half2 d2 = __halves2half2(hdy, __float2half_rn(w.y));
-    uint4 rec;
-    rec.x = __float_as_uint(a);
-    rec.y = *reinterpret_cast<const unsigned*>(&d1);
-    rec.z = *reinterpret_cast<const unsigned*>(&d2);
-    rec.w = __float_as_uint(w.x);
+    uint2 rec = make_uint2(0u, 0u);   // the last row and column: samples not taken
+    if (c + 1 < U && r + 1 < rows) {
+        const float* src = plain + (size_t)f * plain_frame + (size_t)r * U + c;
+        const float w0 = tw[(size_t)view * U + c].x, w1 = tw[(size_t)view * U + c + 1].x;
+        // the tapered footprint over the view's scale (exact: inv a power of two)
+        const float a = (src[0] * w0) * inv, b = (src[1] * w1) * inv;
+        const float cc = (src[U] * w0) * inv, d = (src[U + 1] * w1) * inv;
+        const __half hp = __float2half_rn(a);
+        const float ap = __half2float(hp);
+        const __half hdx = __float2half_rn(b - ap), hdy = __float2half_rn(cc - ap);
+        const __half hdxy = __float2half_rn(d - (ap + __half2float(hdx) + __half2float(hdy)));
+        const __half2 h1 = __halves2half2(hp, hdx), h2 = __halves2half2(hdy, hdxy);
+        rec.x = *reinterpret_cast<const unsigned*>(&h1);
+        rec.y = *reinterpret_cast<const unsigned*>(&h2);
+    }
     qh[(size_t)(slot0 + f) * q_frame + (size_t)r * U + c] = rec;
 }
 
@@ -603,8 +636,39 @@ cudaError_t go2(const BPParams& p, bool wz, int tx, cudaStream_t s) {
 
 template <int ZPT, bool F, bool WZ, int TX>
 cudaError_t go_mixed(const BPParams& p, cudaStream_t s) {
+    if constexpr (F) {
+        if (p.wvol) {
+            bp_mixed_kernel<ZPT, F, WZ, TX, true><<<bp_grid<TX>(p, ZPT), dim3(TX, kBPThreads / TX), 0, s>>>(p);
+            return cudaGetLastError();
+        }
+    }
     bp_mixed_kernel<ZPT, F, WZ, TX><<<bp_grid<TX>(p, ZPT), dim3(TX, kBPThreads / TX), 0, s>>>(p);
     return cudaGetLastError();
+}
+
+template <int ZPT, bool WZ>
+cudaError_t go_mixed_weights(const BPParams& p, int tx, float* out, cudaStream_t s) {
+    if constexpr (ZPT != 16) {
+        if (tx == 8) {
+            bp_mixed_weights_kernel<ZPT, WZ, 8><<<bp_grid<8>(p, ZPT), dim3(8, kBPThreads / 8), 0, s>>>(p, out);
+            return cudaGetLastError();
+        }
+        if (tx == 32) {
+            bp_mixed_weights_kernel<ZPT, WZ, 32><<<bp_grid<32>(p, ZPT), dim3(32, kBPThreads / 32), 0, s>>>(p, out);
+            return cudaGetLastError();
+        }
+    }
+    bp_mixed_weights_kernel<ZPT, WZ, 4><<<bp_grid<4>(p, ZPT), dim3(4, kBPThreads / 4), 0, s>>>(p, out);
+    return cudaGetLastError();
+}
+
+template <bool WZ>
+cudaError_t go_mixed_weights2(const BPParams& p, int zpt, int tx, float* out, cudaStream_t s) {
+    switch (zpt) {
+        case 16: return go_mixed_weights<16, WZ>(p, tx, out, s);
+        case 8: return go_mixed_weights<8, WZ>(p, tx, out, s);
+        default: return go_mixed_weights<4, WZ>(p, tx, out, s);
+    }
 }
 
 template <int ZPT, bool F, bool WZ>
@@ -653,6 +717,13 @@ cudaError_t launch_bp_weights(const BPParams& p, bool exact, bool w_depends_on_z
                               : go_weights2<true, false>(p, zpt, tile_x, out, s);
     return w_depends_on_z ? go_weights2<false, true>(p, zpt, tile_x, out, s)
                           : go_weights2<false, false>(p, zpt, tile_x, out, s);
+}
+
+cudaError_t launch_bp_mixed_weights(const BPParams& p, bool w_depends_on_z, int zpt, int tile_x, float* out,
+                                    cudaStream_t s) {
+    if (!out || p.v0 != 0) return cudaErrorInvalidValue;
+    return w_depends_on_z ? go_mixed_weights2<true>(p, zpt, tile_x, out, s)
+                          : go_mixed_weights2<false>(p, zpt, tile_x, out, s);
 }
 
 cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, int tile_x,
@@ -711,7 +782,7 @@ cudaError_t launch_frame_absmax(const float* plain, long long frame, int nv, uns
 }
 
 cudaError_t launch_pack_mixed(const float* plain, long long plain_frame, int nv, int rows, int U, const float2* tw,
-                              int view0, int num_views, const unsigned* absmax, float* scale, uint4* qh,
+                              int view0, int num_views, const unsigned* absmax, float* scale, uint2* qh,
                               long long q_frame, int slot0, cudaStream_t s) {
     dim3 grid((U + 255) / 256, rows, nv);
     pack_mixed_kernel<<<grid, 256, 0, s>>>(plain, plain_frame, rows, U, tw, view0, num_views, absmax, scale, qh,

@@ -132,11 +132,16 @@ jfdk_status ensure_plain(jfdk_ctx* c, int views) {
     return JFDK_OK;
 }
 
+// Bytes of one record of the backprojection store: a 16-byte quad (FP32
+// form) or an 8-byte FP16 record (mixed form).
+size_t record_size(const jfdk_ctx* c) { return mixed(c) ? 8 : 16; }
+
 jfdk_status ensure_Q4(jfdk_ctx* c, int views) {
     if (c->q4_views >= views) return JFDK_OK;
     dev_free(c, c->d_q4);
     c->q4_views = 0;
-    jfdk_status st = dev_alloc(c, &c->d_q4, (size_t)views * frame_px(c), "the backprojection quad store");
+    const size_t bytes = (size_t)views * frame_px(c) * record_size(c);
+    jfdk_status st = dev_alloc(c, &c->d_q4, (bytes + 15) / 16, "the backprojection store");
     if (st) return st;
     c->q4_views = views;
     return JFDK_OK;
@@ -263,7 +268,7 @@ jfdk_status pack_frames(jfdk_ctx* c, const float* plain, int nv, int view0, int 
         if (!have_absmax)
             JFDK_LAUNCH(c, launch_frame_absmax(plain, frame_px(c), nv, c->d_absmax, c->stream), "per-view maxima");
         JFDK_LAUNCH(c, launch_pack_mixed(plain, frame_px(c), nv, c->rows, c->out_w, c->d_tw, view0, c->nviews,
-                                         c->d_absmax, c->d_qscale, reinterpret_cast<uint4*>(c->d_q4), frame_px(c),
+                                         c->d_absmax, c->d_qscale, reinterpret_cast<uint2*>(c->d_q4), frame_px(c),
                                          slot0, c->stream),
                     "packing projections");
         return JFDK_OK;
@@ -292,8 +297,10 @@ bool capturing(cudaStream_t s) {
 // JFDK_OPT_DEVICE_MEMORY_LIMIT and the device -- and the weights are then
 // accumulated per sample.
 bool ensure_weights(jfdk_ctx* c, cudaStream_t s) {
-    if (mixed(c) || !c->opt_bp_weights) return false;
-    const int want = c->opt_bp_exact ? 2 : 1;
+    if (!c->opt_bp_weights) return false;
+    // the mixed form's coordinates step from each thread's first slice, so
+    // its weights follow the tile depth too
+    const int want = mixed(c) ? 100 + bp_zpt(c) : c->opt_bp_exact ? 2 : 1;
     if (c->d_wvol && c->wvol_state == want) return true;
     if (capturing(c->stream) || capturing(s)) return false;
     if (!c->d_wvol) {
@@ -311,8 +318,11 @@ bool ensure_weights(jfdk_ctx* c, cudaStream_t s) {
     BPParams b = bp_params(c);
     b.view_base = 0; b.v0 = 0; b.nv = c->nviews;
     c->wvol_state = 0;
-    if (launch_bp_weights(b, c->opt_bp_exact != 0, c->w_depends_on_z, bp_zpt(c), bp_tile(c), c->d_wvol, c->stream) !=
-            cudaSuccess ||
+    const cudaError_t e =
+        mixed(c) ? launch_bp_mixed_weights(b, c->w_depends_on_z, bp_zpt(c), bp_tile(c), c->d_wvol, c->stream)
+                 : launch_bp_weights(b, c->opt_bp_exact != 0, c->w_depends_on_z, bp_zpt(c), bp_tile(c), c->d_wvol,
+                                     c->stream);
+    if (e != cudaSuccess ||
         cudaStreamSynchronize(c->stream) != cudaSuccess) {
         cudaGetLastError();
         return false;
@@ -324,7 +334,7 @@ bool ensure_weights(jfdk_ctx* c, cudaStream_t s) {
 jfdk_status run_bp_on(jfdk_ctx* c, BPParams b, bool finalize, cudaStream_t s) {
     if (finalize && b.v0 == 0 && b.nv == c->nviews && ensure_weights(c, s)) b.wvol = c->d_wvol;
     if (mixed(c)) {
-        b.qh = reinterpret_cast<const uint4*>(c->d_q4);
+        b.qh = reinterpret_cast<const uint2*>(c->d_q4);
         b.qscale = c->d_qscale;
         JFDK_LAUNCH(c, launch_bp_mixed(b, finalize, c->w_depends_on_z, bp_zpt(c), bp_tile(c), s), "backprojection");
         return JFDK_OK;
@@ -433,7 +443,7 @@ BPParams reconstruct_bp_params(const jfdk_ctx* c, float* d_hu, int16_t* d_hu16) 
     b.view_base = 0; b.v0 = 0; b.nv = c->nviews;
     b.out = d_hu; b.out16 = d_hu16; b.apply_ct = 1;
     if (mixed(c)) {
-        b.qh = reinterpret_cast<const uint4*>(c->d_q4);
+        b.qh = reinterpret_cast<const uint2*>(c->d_q4);
         b.qscale = c->d_qscale;
     }
     return b;
@@ -940,8 +950,8 @@ jfdk_status jfdk_store_range(jfdk_ctx* c, int v0, int nv, void** d_records, size
         return fail(c, JFDK_ERR_INVALID, "store_range: bad argument");
     jfdk_status st = ensure_Q4(c, c->nviews);
     if (st) return st;
-    *d_records = c->d_q4 + (size_t)v0 * frame_px(c);
-    *record_bytes = (size_t)nv * frame_px(c) * sizeof(float4);
+    *d_records = reinterpret_cast<char*>(c->d_q4) + (size_t)v0 * frame_px(c) * record_size(c);
+    *record_bytes = (size_t)nv * frame_px(c) * record_size(c);
     *d_scales = mixed(c) ? c->d_qscale + v0 : nullptr;
     return JFDK_OK;
 }

@@ -44,7 +44,7 @@ constexpr int kBPTileY = 32;
 struct BPParams {
     const float4* q4;        // quads, [slots][rows][U]: (p[r][c], p[r+1][c], p[r][c+1] - p[r][c], p[r+1][c+1] - p[r+1][c])
     const float2* tw;        // [views][U] taper pairs (w[c], RN(w[c+1] - w[c])), w[U] = 0
-    const uint4* qh;         // mixed precision: records [slots][rows][U] (bp.cu)
+    const uint2* qh;         // mixed precision: 8-byte records [slots][rows][U] (bp.cu)
     const float* qscale;     // mixed precision: [views] power-of-two scale of each view
     const float* ptm;        // [views][12]
     long long q4_frame;      // quads per slot (rows * U)
@@ -63,9 +63,10 @@ struct BPParams {
     int out_z0;
     int apply_ct;
     float ct_scale, ct_norm1;
-    // finalize over every view of the rotation, FP32 form: the normalisation
-    // weights of the whole volume [Z][Y][X] (launch_bp_weights), so the view
-    // loop accumulates the projections only; null: accumulated per sample
+    // finalize over every view of the rotation: the normalisation weights of
+    // the whole volume [Z][Y][X] (launch_bp_weights / launch_bp_mixed_weights),
+    // so the view loop accumulates the projections only; null: accumulated
+    // per sample
     const float* wvol;
 };
 
@@ -93,6 +94,9 @@ cudaError_t launch_bp(const BPParams& p, bool finalize, bool exact, bool w_depen
 // coordinates, taper lerp and view order).
 cudaError_t launch_bp_weights(const BPParams& p, bool exact, bool w_depends_on_z, int zpt, int tile_x, float* out,
                               cudaStream_t s);
+// The same for the mixed form (its coordinates, range test and FP32 taper lerp).
+cudaError_t launch_bp_mixed_weights(const BPParams& p, bool w_depends_on_z, int zpt, int tile_x, float* out,
+                                    cudaStream_t s);
 // A batched backprojection launch covers up to kBatchSlots scans that share
 // whether W depends on z (each with its own tile depth, 4 or 8 slices); their
 // parameters travel in the kernel's parameter space (16 slots: ~4.4 KB of the
@@ -115,7 +119,7 @@ cudaError_t launch_frame_absmax(const float* plain, long long frame, int nv, uns
 // Filtered frames -> mixed-precision records in slots [slot0, slot0 + nv);
 // writes the scale of rotation view (view0 + f) mod num_views to scale[].
 cudaError_t launch_pack_mixed(const float* plain, long long plain_frame, int nv, int rows, int U, const float2* tw,
-                              int view0, int num_views, const unsigned* absmax, float* scale, uint4* qh,
+                              int view0, int num_views, const unsigned* absmax, float* scale, uint2* qh,
                               long long q_frame, int slot0, cudaStream_t s);
 // Filtered frames [nv][rows][U] -> quads in slots [slot0, slot0 + nv), tapered
 // with the taper of rotation view (view0 + f) when apply_taper.
@@ -307,7 +311,7 @@ struct jfdk_ctx {
     float* d_arow = nullptr;                     // FP16X3: per-row factors
     float* d_e = nullptr;
     float* d_plain = nullptr; int plain_views = 0;  // filtered frames of one chunk
-    float4* d_q4 = nullptr; int q4_views = 0;       // quad store (mixed: uint4 records)
+    float4* d_q4 = nullptr; int q4_views = 0;       // quad store (mixed: 8-byte records)
     float* d_qscale = nullptr;                      // mixed: [views] scales
     unsigned* d_absmax = nullptr; int absmax_n = 0; // mixed: per-frame maxima
     float* d_sum = nullptr;                          // accumulators of the slab:
@@ -332,7 +336,7 @@ struct jfdk_ctx {
     int opt_ramp = 0;            // JFDK_OPT_RAMP_PRODUCT (0: the form's default)
     int opt_bp_weights = 1;      // JFDK_OPT_BP_WEIGHTS
     float* d_wvol = nullptr;     // normalisation weights [Z][Y][X] (FP32 form)
-    int wvol_state = 0;          // 0: none, 1: valid for the fast rounding, 2: for EXACT
+    int wvol_state = 0;          // 0: none; valid for 1: the fast rounding, 2: EXACT, 100 + tile depth: the mixed form
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // jfdk_reconstruct_host: a copy stream and a second compute stream, and
     // their events (created on first use)

@@ -131,17 +131,19 @@ def test_backprojection_in_chunks_equals_one_pass(torch_cuda, case):
     np.testing.assert_array_equal(e.finalize(apply_ctnum=False).cpu().numpy(), case["bp"])
 
 
-@pytest.mark.parametrize("exact", [True, False])
-def test_weight_volume_is_bit_identical(torch_cuda, case, exact):
-    """The FP32 form divides by a once-per-geometry volume of normalisation
-    weights (JFDK_OPT_BP_WEIGHTS, default on): the same volume bit for bit as
-    with the weights accumulated per sample, in both roundings, and again
-    after the geometry changes (the weights follow it)."""
+@pytest.mark.parametrize("form", ["exact", "fast", "mixed"])
+def test_weight_volume_is_bit_identical(torch_cuda, case, form):
+    """A backprojection over every view divides by a once-per-geometry volume
+    of normalisation weights (JFDK_OPT_BP_WEIGHTS, default on): the same
+    volume bit for bit as with the weights accumulated per sample, in both
+    roundings of the FP32 form and in the mixed form, and again after the
+    geometry changes (the weights follow it)."""
     torch = torch_cuda
     from jenhine_b200 import _lib
     raw = to_dev(torch, case["raw"])
-    on = engine_for(case, bp_exact=exact)
-    off = engine_for(case, bp_exact=exact)
+    kw = {"precision": "mixed"} if form == "mixed" else {"bp_exact": form == "exact"}
+    on = engine_for(case, **kw)
+    off = engine_for(case, **kw)
     off.set_option(_lib.OPT_BP_WEIGHTS, 0)
     same = lambda a, b: torch.equal(torch.nan_to_num(a, 1e30), torch.nan_to_num(b, 1e30))
     assert same(on.reconstruct(raw).clone(), off.reconstruct(raw).clone())

@@ -67,7 +67,7 @@ def test_store_range_describes_the_store(torch_cuda):
         e = engine_for(g, precision=precision)
         (p0, n0), sc0 = e.store_range(0, 4)
         (p1, n1), sc1 = e.store_range(4, 6)
-        frame = e.rows * e.filter_out_w * 16      # float4 quads / 16-byte records
+        frame = e.rows * e.filter_out_w * (8 if precision == "mixed" else 16)   # FP16 records / FP32 quads
         assert n0 == 4 * frame and n1 == 6 * frame and p1 == p0 + 4 * frame
         if precision == "mixed":
             assert sc0[1] == 16 and sc1[0] == sc0[0] + 16
