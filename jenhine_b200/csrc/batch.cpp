@@ -25,7 +25,7 @@ struct jfdk_batch {
     bool own_stream = false;
     struct Group {                      // one persistent launch
         BatchSlots slots;
-        int n, wz, ctas;
+        int n, wz, wv, ctas;            // wv: every scan divides by its weight volume
         unsigned total;
     };
     std::vector<Group> groups;
@@ -85,11 +85,18 @@ jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
         s.gx = (c->X + kBPTileX - 1) / kBPTileX;
         s.gy = (c->Y + kBPTileY - 1) / kBPTileY;
         s.gz = (c->Z + s.zpt - 1) / s.zpt;
-        if (b->groups.empty() || b->groups.back().n == kBatchSlots || b->groups.back().wz != s.wz) {
+        // the weights of the tile depth the launch runs (the mixed form's
+        // coordinates, and with them its weights, follow the depth)
+        const float* wvol = bp_slices_per_thread(c) == s.zpt ? bp_weight_volume(c) : nullptr;
+        s.p.wvol = wvol;
+        const int wv = wvol ? 1 : 0;
+        if (b->groups.empty() || b->groups.back().n == kBatchSlots || b->groups.back().wz != s.wz ||
+            b->groups.back().wv != wv) {
             jfdk_batch::Group g;
             std::memset(&g, 0, sizeof g);
             g.wz = s.wz;
-            BATCH_CUDA(b, bp_batch_ctas(b->mixed != 0, g.wz != 0, &g.ctas), "occupancy query");
+            g.wv = wv;
+            BATCH_CUDA(b, bp_batch_ctas(b->mixed != 0, g.wz != 0, g.wv != 0, &g.ctas), "occupancy query");
             b->groups.push_back(g);
         }
         jfdk_batch::Group& g = b->groups.back();
@@ -126,7 +133,7 @@ jfdk_status enqueue_persistent(jfdk_batch* b, const uint16_t* const* d_raw) {
     }
     for (size_t k = 0; k < b->groups.size(); ++k) {
         const jfdk_batch::Group& g = b->groups[k];
-        BATCH_CUDA(b, launch_bp_batch(g.slots, g.n, g.total, b->mixed != 0, g.wz != 0, b->d_counter + k, g.ctas,
+        BATCH_CUDA(b, launch_bp_batch(g.slots, g.n, g.total, b->mixed != 0, g.wz != 0, g.wv != 0, b->d_counter + k, g.ctas,
                                       b->stream),
                    "batched backprojection");
         ++b->launches;

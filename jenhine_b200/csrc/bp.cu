@@ -393,34 +393,35 @@ __global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_mixed_weigh
 // scan's own tile depth (4 or 8 slices, a uniform branch per tile), so scans
 // tuned to either depth share the launch.  The next tile's index is fetched
 // while the current one runs.
-template <int S, bool MIXED, bool WZ>
+// WV: every scan of the launch divides by its weight volume (p.wvol).
+template <int S, bool MIXED, bool WZ, bool WV>
 __device__ __forceinline__ void batch_slot_tile(const BatchSlots& t) {
     const BatchTile tile{t.s[S]};
     if (t.s[S].zpt == 8) {
         if (MIXED)
-            bp_mixed_block<8, true, WZ>(t.s[S].p, tile);
+            bp_mixed_block<8, true, WZ, BatchTile, WV>(t.s[S].p, tile);
         else
-            bp_block<8, true, false, WZ>(t.s[S].p, tile);
+            bp_block<8, true, false, WZ, BatchTile, WV>(t.s[S].p, tile);
     } else {
         if (MIXED)
-            bp_mixed_block<4, true, WZ>(t.s[S].p, tile);
+            bp_mixed_block<4, true, WZ, BatchTile, WV>(t.s[S].p, tile);
         else
-            bp_block<4, true, false, WZ>(t.s[S].p, tile);
+            bp_block<4, true, false, WZ, BatchTile, WV>(t.s[S].p, tile);
     }
 }
 
 // The tile of slot si (si < kBatchSlots): a compile-time slot per case.
-template <int S, bool MIXED, bool WZ>
+template <int S, bool MIXED, bool WZ, bool WV>
 __device__ __forceinline__ void batch_dispatch(const BatchSlots& t, int si) {
     if constexpr (S < kBatchSlots) {
         if (si == S)
-            batch_slot_tile<S, MIXED, WZ>(t);
+            batch_slot_tile<S, MIXED, WZ, WV>(t);
         else
-            batch_dispatch<S + 1, MIXED, WZ>(t, si);
+            batch_dispatch<S + 1, MIXED, WZ, WV>(t, si);
     }
 }
 
-template <bool MIXED, bool WZ>
+template <bool MIXED, bool WZ, bool WV>
 __global__ void __launch_bounds__(kBPThreads, MIXED ? bp_min_blocks(8) : bp_fp32_min_blocks(8))
     bp_batch_kernel(const __grid_constant__ BatchSlots t, int nscans, unsigned* __restrict__ counter,
                     unsigned total) {
@@ -434,7 +435,7 @@ __global__ void __launch_bounds__(kBPThreads, MIXED ? bp_min_blocks(8) : bp_fp32
         if (tid == 0) s_next = atomicAdd(counter, 1u);   // the next tile, while this one runs
         int si = 0;
         while (si + 1 < nscans && it >= t.s[si + 1].first_tile) ++si;
-        batch_dispatch<0, MIXED, WZ>(t, si);
+        batch_dispatch<0, MIXED, WZ, WV>(t, si);
         __syncthreads();   // every thread is done with the current tile
         if (tid == 0) g_batch_tile = s_next;
         __syncthreads();
@@ -735,40 +736,52 @@ cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_
 
 namespace {
 
-template <bool M, bool W>
+template <bool M, bool W, bool V>
 cudaError_t batch_go(const BatchSlots& t, int nscans, unsigned total, unsigned* counter, int ctas, cudaStream_t s) {
-    bp_batch_kernel<M, W><<<ctas, dim3(kBPTileX, kBPTileY), 0, s>>>(t, nscans, counter, total);
+    bp_batch_kernel<M, W, V><<<ctas, dim3(kBPTileX, kBPTileY), 0, s>>>(t, nscans, counter, total);
     return cudaGetLastError();
 }
 
-template <bool M, bool W>
+template <bool M, bool W, bool V>
 cudaError_t batch_occ(int* per) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, bp_batch_kernel<M, W>, kBPThreads, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, bp_batch_kernel<M, W, V>, kBPThreads, 0);
+}
+
+template <bool M, bool W>
+cudaError_t batch_go2(const BatchSlots& t, int nscans, unsigned total, unsigned* counter, int ctas, bool wv,
+                      cudaStream_t s) {
+    return wv ? batch_go<M, W, true>(t, nscans, total, counter, ctas, s)
+              : batch_go<M, W, false>(t, nscans, total, counter, ctas, s);
+}
+
+template <bool M, bool W>
+cudaError_t batch_occ2(bool wv, int* per) {
+    return wv ? batch_occ<M, W, true>(per) : batch_occ<M, W, false>(per);
 }
 
 }  // namespace
 
 cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tiles, bool mixed_form, bool wz,
-                            unsigned* counter, int ctas, cudaStream_t s) {
+                            bool wv, unsigned* counter, int ctas, cudaStream_t s) {
     if (nscans < 1 || nscans > kBatchSlots) return cudaErrorInvalidValue;
     for (int i = 0; i < nscans; ++i)
-        if (t.s[i].zpt != 4 && t.s[i].zpt != 8) return cudaErrorInvalidValue;
+        if ((t.s[i].zpt != 4 && t.s[i].zpt != 8) || (wv && !t.s[i].p.wvol)) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     if (mixed_form)
-        return wz ? batch_go<true, true>(t, nscans, total_tiles, counter, ctas, s)
-                  : batch_go<true, false>(t, nscans, total_tiles, counter, ctas, s);
-    return wz ? batch_go<false, true>(t, nscans, total_tiles, counter, ctas, s)
-              : batch_go<false, false>(t, nscans, total_tiles, counter, ctas, s);
+        return wz ? batch_go2<true, true>(t, nscans, total_tiles, counter, ctas, wv, s)
+                  : batch_go2<true, false>(t, nscans, total_tiles, counter, ctas, wv, s);
+    return wz ? batch_go2<false, true>(t, nscans, total_tiles, counter, ctas, wv, s)
+              : batch_go2<false, false>(t, nscans, total_tiles, counter, ctas, wv, s);
 }
 
-cudaError_t bp_batch_ctas(bool mixed_form, bool wz, int* ctas) {
+cudaError_t bp_batch_ctas(bool mixed_form, bool wz, bool wv, int* ctas) {
     int dev = 0, sms = 0, per = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-        e = mixed_form ? (wz ? batch_occ<true, true>(&per) : batch_occ<true, false>(&per))
-                       : (wz ? batch_occ<false, true>(&per) : batch_occ<false, false>(&per));
+        e = mixed_form ? (wz ? batch_occ2<true, true>(wv, &per) : batch_occ2<true, false>(wv, &per))
+                       : (wz ? batch_occ2<false, true>(wv, &per) : batch_occ2<false, false>(wv, &per));
     *ctas = sms * (per > 0 ? per : 1);
     return e;
 }

@@ -455,6 +455,7 @@ jfdk_status reconstruct_bp(jfdk_ctx* c, float* d_hu, cudaStream_t s) {
 
 int bp_slices_per_thread(const jfdk_ctx* c) { return bp_zpt(c); }
 bool mixed_form(const jfdk_ctx* c) { return mixed(c); }
+const float* bp_weight_volume(jfdk_ctx* c) { return ensure_weights(c, c->stream) ? c->d_wvol : nullptr; }
 
 }  // namespace jfdk
 

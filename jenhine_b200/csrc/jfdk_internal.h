@@ -108,9 +108,9 @@ struct BatchSlots {
 // All tiles of nscans scans in one persistent launch of `ctas` CTAs (the
 // SMs' resident CTAs); *counter is the work-list cursor (cleared here).
 cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tiles, bool mixed_form, bool wz,
-                            unsigned* counter, int ctas, cudaStream_t s);
+                            bool wv, unsigned* counter, int ctas, cudaStream_t s);
 // CTAs of a full persistent wave: SMs x resident CTAs per SM.
-cudaError_t bp_batch_ctas(bool mixed_form, bool wz, int* ctas);
+cudaError_t bp_batch_ctas(bool mixed_form, bool wz, bool wv, int* ctas);
 // Mixed-precision form: FP16 footprints with a per-view scale (qh, qscale).
 cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, int tile_x,
                             cudaStream_t s);
@@ -365,4 +365,9 @@ BPParams reconstruct_bp_params(const jfdk_ctx* c, float* d_hu, int16_t* d_hu16);
 jfdk_status reconstruct_bp(jfdk_ctx* c, float* d_hu, cudaStream_t s);
 int bp_slices_per_thread(const jfdk_ctx* c);
 bool mixed_form(const jfdk_ctx* c);
+// The context's normalisation-weight volume for a backprojection over every
+// view with its current options (computed now if needed, the context's
+// stream synchronised), or null when it has none (JFDK_OPT_BP_WEIGHTS off,
+// no room, or a capture under way).
+const float* bp_weight_volume(jfdk_ctx* c);
 }  // namespace jfdk
