@@ -427,13 +427,14 @@ __global__ void __launch_bounds__(256) weight_kernel(PrepParams P, const float* 
     }
 }
 
-// The int8 digit form with one warp per row: the row's values stay in
-// registers (pitch <= 128 * G), the scale's maximum is a warp reduction;
-// the same values, scale and digits as weight_kernel's AOUT_I8X4 path.  No
-// compositing (weight_kernel handles it).
+// One warp per row, for the int8 digit form and the BF16 pairs: the row's
+// values stay in registers (pitch <= 128 * G); for the digits the scale's
+// maximum is a warp reduction.  The same values, scale and digits as
+// weight_kernel's AOUT_I8X4 / AOUT_BF16X2 paths.  No compositing
+// (weight_kernel handles it).
 constexpr int kI8WarpGroups = 16;
-template <bool FROM_RAW, int G>
-__global__ void __launch_bounds__(256) weight_i8_kernel(PrepParams P, const float* __restrict__ in, int width,
+template <bool FROM_RAW, int G, int OUT>
+__global__ void __launch_bounds__(256) weight_warp_kernel(PrepParams P, const float* __restrict__ in, int width,
                                                         int rows, int v0, WeightParams W, AOperand A,
                                                         float* __restrict__ e) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -491,6 +492,18 @@ __global__ void __launch_bounds__(256) weight_i8_kernel(PrepParams P, const floa
 #pragma unroll
         for (int k = 0; k < 4; ++k) mx = fmaxf(mx, fabsf(v[gi][k]));
     }
+    if constexpr (OUT == AOUT_BF16X2) {
+#pragma unroll
+        for (int gi = 0; gi < G; ++gi) {
+            const int i4 = gi * 128 + lane * 4;
+            if (gi * 128 >= A.pitch) break;
+            if (i4 >= A.pitch) continue;
+            float o[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) o[k] = gi * 128 < width ? v[gi][k] : 0.0f;
+            store4<AOUT_BF16X2>(A.hi, A.lo, a0 + i4, o);
+        }
+    } else {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     int E = 0;
@@ -524,12 +537,26 @@ __global__ void __launch_bounds__(256) weight_i8_kernel(PrepParams P, const floa
         for (int s2 = 0; s2 < kI8RowDigits; ++s2)
             *reinterpret_cast<char4*>(plane + s2 * pstride + a0 + i4) = make_char4(d[s2][0], d[s2][1], d[s2][2], d[s2][3]);
     }
+    }
     if (lane == 0) {
         // FilterCore.cpp:203-214 -- mean of the three outermost unweighted samples
         const float edge = W.mirror ? __fdiv_rn(__fadd_rn(__fadd_rn(pix(width - 1), pix(width - 2)), pix(width - 3)), 3.0f)
                                     : __fdiv_rn(__fadd_rn(__fadd_rn(pix(0), pix(1)), pix(2)), 3.0f);
         e[m] = edge;
     }
+}
+
+template <bool FROM_RAW, int OUT>
+cudaError_t launch_weight_warp(const PrepParams& p, const float* in, int nv, int v0, int width, int rows,
+                               const WeightParams& w, const AOperand& A, float* e, cudaStream_t s) {
+    const dim3 g8((rows + 7) / 8, nv);
+    if (A.pitch <= 128 * 6)
+        weight_warp_kernel<FROM_RAW, 6, OUT><<<g8, 256, 0, s>>>(p, in, width, rows, v0, w, A, e);
+    else if (A.pitch <= 128 * 8)
+        weight_warp_kernel<FROM_RAW, 8, OUT><<<g8, 256, 0, s>>>(p, in, width, rows, v0, w, A, e);
+    else
+        weight_warp_kernel<FROM_RAW, kI8WarpGroups, OUT><<<g8, 256, 0, s>>>(p, in, width, rows, v0, w, A, e);
+    return cudaGetLastError();
 }
 
 template <bool FROM_RAW>
@@ -539,20 +566,16 @@ cudaError_t launch_weight_t(const PrepParams& p, const float* in, int nv, int v0
     switch (A.kind) {
         case AOUT_F32: weight_kernel<FROM_RAW, AOUT_F32><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e); break;
         case AOUT_TF32X2: weight_kernel<FROM_RAW, AOUT_TF32X2><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e); break;
-        case AOUT_BF16X2: weight_kernel<FROM_RAW, AOUT_BF16X2><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e); break;
+        case AOUT_BF16X2:
+            if (!(FROM_RAW && w.comp.W > 0) && A.pitch <= 128 * kI8WarpGroups && (A.pitch & 3) == 0)
+                return launch_weight_warp<FROM_RAW, AOUT_BF16X2>(p, in, nv, v0, width, rows, w, A, e, s);
+            weight_kernel<FROM_RAW, AOUT_BF16X2><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e);
+            break;
         case AOUT_FP16X2: weight_kernel<FROM_RAW, AOUT_FP16X2><<<grid, threads, 0, s>>>(p, in, width, rows, v0, w, A, e); break;
         case AOUT_I8X4:
             if (A.pitch % 4 != 0) return cudaErrorInvalidValue;
-            if (!(FROM_RAW && w.comp.W > 0) && A.pitch <= 128 * kI8WarpGroups) {
-                const dim3 g8((rows + 7) / 8, nv);
-                if (A.pitch <= 128 * 6)
-                    weight_i8_kernel<FROM_RAW, 6><<<g8, 256, 0, s>>>(p, in, width, rows, v0, w, A, e);
-                else if (A.pitch <= 128 * 8)
-                    weight_i8_kernel<FROM_RAW, 8><<<g8, 256, 0, s>>>(p, in, width, rows, v0, w, A, e);
-                else
-                    weight_i8_kernel<FROM_RAW, kI8WarpGroups><<<g8, 256, 0, s>>>(p, in, width, rows, v0, w, A, e);
-                break;
-            }
+            if (!(FROM_RAW && w.comp.W > 0) && A.pitch <= 128 * kI8WarpGroups)
+                return launch_weight_warp<FROM_RAW, AOUT_I8X4>(p, in, nv, v0, width, rows, w, A, e, s);
             if (width > 12288) return cudaErrorInvalidValue;   // the row in 48 KB of shared memory
             weight_kernel<FROM_RAW, AOUT_I8X4><<<grid, threads, sizeof(float) * width, s>>>(p, in, width, rows, v0, w, A, e);
             break;
