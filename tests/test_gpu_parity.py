@@ -154,6 +154,40 @@ def test_weight_volume_is_bit_identical(torch_cuda, case, form):
     assert same(on.reconstruct(raw).clone(), off.reconstruct(raw).clone())
 
 
+def test_weight_volume_follows_the_rounding_and_the_memory_bound(torch_cuda, case):
+    """One context switched between the roundings recomputes its weights
+    (fast and EXACT weights differ), and under a device-memory bound that
+    leaves no room for the weight volume a reconstruction falls back to the
+    per-sample weights -- the same volume either way."""
+    torch = torch_cuda
+    from jenhine_b200 import _lib
+    raw = to_dev(torch, case["raw"])
+    same = lambda a, b: torch.equal(torch.nan_to_num(a, 1e30), torch.nan_to_num(b, 1e30))
+    ref = {}
+    for exact in (False, True):
+        off = engine_for(case, bp_exact=exact)
+        off.set_option(_lib.OPT_BP_WEIGHTS, 0)
+        ref[exact] = off.reconstruct(raw).clone()
+    e = engine_for(case)
+    assert same(e.reconstruct(raw).clone(), ref[False])
+    e.set_option(_lib.OPT_BP_EXACT, 1)
+    assert same(e.reconstruct(raw).clone(), ref[True])
+    e.set_option(_lib.OPT_BP_EXACT, 0)
+    assert same(e.reconstruct(raw).clone(), ref[False])
+    tight = engine_for(case)
+    tight.reconstruct(raw)                     # allocates the stores (and the weights)
+    X, Y, Z = (int(v) for v in case["vol"])
+    fresh = engine_for(case)
+    fresh.set_option(_lib.OPT_BP_WEIGHTS, 0)
+    fresh.reconstruct(raw)
+    without = fresh.device_bytes               # everything a reconstruction holds but the weights
+    assert tight.device_bytes >= without + X * Y * Z * 4
+    bound = engine_for(case)
+    bound.set_option(_lib.OPT_DEVICE_MEMORY_LIMIT, without + X * Y * Z * 4 - 1)
+    assert same(bound.reconstruct(raw).clone(), ref[False])
+    assert bound.device_bytes <= without + X * Y * Z * 4 - 1
+
+
 def test_ctnum_bit_exact(torch_cuda, case):
     e = engine_for(case)
     vol = to_dev(torch_cuda, case["bp"])
