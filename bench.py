@@ -364,7 +364,7 @@ def time_zslab(a, w, raw, ptms, precision, dist, rank, world, local):
     from jenhine_b200.zslab import reconstruct_zslab, slab_ranges
     eng = FDKEngine(w.scan, w.recon, ptms, precision=precision, bp_exact=a.exact)
     r = w.recon
-    z0, nz = slab_ranges(r.num_pixels_z, world)[rank]
+    z0, nz = slab_ranges(r.num_pixels_z, world, eng.tile_depth)[rank]
     out = torch.empty((max(nz, 1), r.num_pixels_y, r.num_pixels_x), dtype=torch.float32, device="cuda")
     frames = torch.empty((w.geom.n_views, eng.rows, eng.filter_out_w), dtype=torch.float32, device="cuda")
     for _ in range(a.warmup):
@@ -483,7 +483,7 @@ def time_form(a, w, raw, ptms, precision, dist, world, local):
     out = {"value": w.updates * world / (ms / 1000.0) / 1e9, "ms_per_step": ms, "s_per_volume": ms / 1000.0,
            "stages_ms": {"preprocess_weight_filter": statistics.mean(s[0] for s in stage_ms),
                          "backprojection_hu": statistics.mean(s[2] for s in stage_ms)},
-           "gpu_launches": launches, "clocks": clk, "_sample": sample}
+           "gpu_launches": launches, "clocks": clk, "tile_depth": eng.tile_depth, "_sample": sample}
 
     # end to end through the host-buffer call, pinned memory
     if not a.no_e2e:
@@ -548,7 +548,8 @@ def roofline(w, bp_ms, form, clocks):
     # volume: a 16-byte FP32 quad, or an 8-byte FP16 record (mixed)
     rec = 16 if form == "fp32" else 8
     per_req = profile_figure(f"{kernel}_c2_chunks", "records_per_request") or 6.0
-    gather = gather_ceiling(rec, False, max(1, min(32, int(round(per_req)))))
+    warps = int(profile_figure(f"{kernel}_c2_chunks", "warps_per_sm") or 32)
+    gather = gather_ceiling(rec, False, max(1, min(32, int(round(per_req)))), warps)
     peak, peak_kind = measured_peaks()
     # projections once (4 / 2 bytes a pixel), the weights read and the volume written once
     alg = g.n_views * g.det_v * g.det_u * (4 if form == "fp32" else 2) + 2 * r.num_pixels_x * r.num_pixels_y * \
@@ -566,7 +567,7 @@ def roofline(w, bp_ms, form, clocks):
     out["gather"] = {"peak": gather / 1e9 if gather else None, "achieved": gups,
                      "frac": gups / (gather / 1e9) if gather else None, "unit": "G samples/s",
                      "pattern": f"one {rec}-byte record per sample, {per_req:g} records per warp request, "
-                                f"32 warps per SM, L1-resident (jfdk_measure_gather_rate, this run)"}
+                                f"{warps} warps per SM, L1-resident (jfdk_measure_gather_rate, this run)"}
     out["hbm"] = {"achieved": hbm, "peak": peak, "frac": hbm / peak, "unit": "GB/s",
                   "peak_source": f"{peak_kind} hbm_gbs ({'of measured' if peak_kind == 'measured' else 'of fallback'})",
                   "algorithmic_bytes_per_launch": alg, "traffic": profile_traffic(prof)}

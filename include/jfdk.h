@@ -214,7 +214,7 @@ jfdk_status jfdk_reconstruct_host(jfdk_ctx* ctx, const uint16_t* h_raw, float* h
  * counterpart in the reference), and each GPU backprojects its own slab of
  * slices from every view (jfdk_backproject_store).  Results equal
  * jfdk_reconstruct's bit for bit when the slabs start at multiples of the
- * tile depth (JFDK_OPT_BP_ZPT; 8 by default). */
+ * tile depth (jfdk_get_option(JFDK_OPT_BP_ZPT)). */
 /* The filter stage of jfdk_reconstruct for views [v0, v0+nv) of the
  * rotation -- preprocessing (and compositing), pre-weight, ramp filter,
  * z-filter -- into caller-owned filtered frames: d_raw the rotation's frames
@@ -253,7 +253,11 @@ enum {
     JFDK_OPT_STAGE_TIMING = 3,/* 1: jfdk_reconstruct records CUDA events on its
                                  stream around each stage                        */
     JFDK_OPT_BP_ZPT = 4,      /* slices each backprojection thread keeps in
-                                 registers: 4, 8 or 16; 0 (default): 8         */
+                                 registers: 4, 8 or 16; 0 (default): 16 in the
+                                 mixed form when W does not depend on z, else 8.
+                                 The FP32 form's volume does not depend on it;
+                                 the mixed form's coordinates step from each
+                                 tile's first slice, so its volume does      */
     JFDK_OPT_FILTER_SIMT = 5, /* 1: ramp product on FP32 CUDA cores (same as
                                  JFDK_OPT_RAMP_PRODUCT = JFDK_RAMP_FP32_SIMT);
                                  0: the form's default                          */
@@ -298,6 +302,11 @@ typedef enum {
                                  the tiling (the FP32 form's default)            */
 } jfdk_ramp_product;
 jfdk_status jfdk_set_option(jfdk_ctx* ctx, int key, long long value);
+/* The value an option has in effect: the set value, or the default the
+ * context resolves it to (JFDK_OPT_BP_ZPT: the tile depth its
+ * backprojection runs with; JFDK_OPT_BP_TILE: its tile width;
+ * JFDK_OPT_RAMP_PRODUCT: the product its filter runs). */
+jfdk_status jfdk_get_option(jfdk_ctx* ctx, int key, long long* value);
 /* Stage times (ms) of the last jfdk_reconstruct with JFDK_OPT_STAGE_TIMING:
  * [0] preprocess + pre-weight + ramp filter (+ z-filter) + packing for the
  * backprojector, [1] reserved (0), [2] backprojection with normalisation and
@@ -336,7 +345,8 @@ jfdk_status jfdk_geometry_gradient(jfdk_ctx* ctx, const float* d_q, int v0, int 
 /* ---- autotuner and batches (no counterpart in the reference) -------------- */
 
 /* Pick the backprojection's voxel tile (JFDK_OPT_BP_ZPT: 4 or 8 slices per
- * thread; JFDK_OPT_BP_TILE: 4, 8 or 32 threads wide in x, 128 per CTA) and
+ * thread, and 16 in the mixed form; JFDK_OPT_BP_TILE: 4, 8 or 32 threads wide
+ * in x, 128 per CTA, 16-slice tiles 4 wide) and
  * the filter stage's views per chunk (JFDK_OPT_VIEW_CHUNK: 16, 32 or 64) for
  * this context's shape by timing the candidates on the device (a 32-slice
  * slab, the first 128 views of zero frames).  Results are cached per shape in the process and, when

@@ -77,6 +77,7 @@ _SIGS = {
     "jfdk_sync": ([_P], C.c_int),
     "jfdk_get_dims": ([_P, _P, _P, _P, _P], C.c_int),
     "jfdk_set_option": ([_P, C.c_int, C.c_longlong], C.c_int),
+    "jfdk_get_option": ([_P, C.c_int, C.POINTER(C.c_longlong)], C.c_int),
     "jfdk_stage_times": ([_P, _P], C.c_int),
     "jfdk_preprocess_frames": ([_P, _P, C.c_int, _P], C.c_int),
     "jfdk_filter_frames": ([_P, _P, C.c_int, C.c_int, _P], C.c_int),

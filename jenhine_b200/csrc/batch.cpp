@@ -25,7 +25,7 @@ struct jfdk_batch {
     bool own_stream = false;
     struct Group {                      // one persistent launch
         BatchSlots slots;
-        int n, wz, wv, ctas;            // wv: every scan divides by its weight volume
+        int n, wz, wv, deep, ctas;      // wv: every scan divides by its weight volume; deep: 16-slice tiles
         unsigned total;
     };
     std::vector<Group> groups;
@@ -71,8 +71,9 @@ void drop_graph(jfdk_batch* b) {
 
 // Scan descriptors for the given outputs: each scan's finalizing BP params,
 // its grid of kBPTileX x kBPTileY x ZPT tiles and its first tile in its group's
-// work list; consecutive scans with the same W(z) share a group of up to
-// kBatchSlots.
+// work list; consecutive scans with the same W(z), weight-volume use and
+// tile-depth class (16 slices, the mixed form's default, or 4 / 8) share a
+// group of up to kBatchSlots.
 jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
     b->groups.clear();
     for (size_t i = 0; i < b->ctx.size(); ++i) {
@@ -80,7 +81,8 @@ jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
         BatchScan s;
         std::memset(&s, 0, sizeof s);
         s.p = reconstruct_bp_params(c, d_hu[i], nullptr);
-        s.zpt = bp_slices_per_thread(c) == 4 ? 4 : 8;
+        const int zpt = bp_slices_per_thread(c);
+        s.zpt = zpt == 4 ? 4 : (zpt == 16 && b->mixed) ? 16 : 8;
         s.wz = c->w_depends_on_z ? 1 : 0;
         s.gx = (c->X + kBPTileX - 1) / kBPTileX;
         s.gy = (c->Y + kBPTileY - 1) / kBPTileY;
@@ -89,14 +91,16 @@ jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
         // coordinates, and with them its weights, follow the depth)
         const float* wvol = bp_slices_per_thread(c) == s.zpt ? bp_weight_volume(c) : nullptr;
         s.p.wvol = wvol;
-        const int wv = wvol ? 1 : 0;
+        const int wv = wvol ? 1 : 0, deep = s.zpt == 16 ? 1 : 0;
         if (b->groups.empty() || b->groups.back().n == kBatchSlots || b->groups.back().wz != s.wz ||
-            b->groups.back().wv != wv) {
+            b->groups.back().wv != wv || b->groups.back().deep != deep) {
             jfdk_batch::Group g;
             std::memset(&g, 0, sizeof g);
             g.wz = s.wz;
             g.wv = wv;
-            BATCH_CUDA(b, bp_batch_ctas(b->mixed != 0, g.wz != 0, g.wv != 0, &g.ctas), "occupancy query");
+            g.deep = deep;
+            BATCH_CUDA(b, bp_batch_ctas(b->mixed != 0, g.wz != 0, g.wv != 0, g.deep != 0, &g.ctas),
+                       "occupancy query");
             b->groups.push_back(g);
         }
         jfdk_batch::Group& g = b->groups.back();

@@ -57,8 +57,11 @@ constexpr int kBPThreads = kBPTileX * kBPTileY;
 // faster than 8-warp ones: a finishing CTA leaves fewer warps idle while the
 // SM waits for the next.  Each warp covers 4 x 8 voxels in (x, y) rather than
 // a row of 32: its sample points spread less on the detector (1.5-1.7 %
-// faster than 32 x 1 in both forms).
-constexpr int bp_min_blocks(int zpt) { return zpt == 8 ? 1024 / kBPThreads : 1; }
+// faster than 32 x 1 in both forms).  The mixed form with 16 slices per
+// thread (its default tile when W does not depend on z) halves the per-view
+// work per sample and fits 96 registers at 20 warps per SM: 88.0 ms on c2
+// against 88.9 at 80 registers and 24 warps and 93.6 with 8 slices.
+constexpr int bp_min_blocks(int zpt) { return zpt == 8 ? 1024 / kBPThreads : zpt == 16 ? 5 : 1; }
 constexpr int bp_fp32_min_blocks(int zpt) { return zpt == 8 ? 6 : 1; }
 
 // Where a CTA's tile lies: the launch grid's block index for the per-scan
@@ -377,8 +380,11 @@ __global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_mixed_kerne
         bp_mixed_block<ZPT, FINALIZE, WZ, GridTileHeld<TX>, WV>(p, GridTileHeld<TX>{});
 }
 
+// (once per geometry; with 16 slices at 128 registers, which the weights'
+// taper lerps fill without spilling)
 template <int ZPT, bool WZ, int TX>
-__global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_mixed_weights_kernel(BPParams p, float* out) {
+__global__ void __launch_bounds__(kBPThreads, ZPT == 16 ? 4 : bp_min_blocks(ZPT))
+    bp_mixed_weights_kernel(BPParams p, float* out) {
     bp_mixed_block<ZPT, true, WZ, GridTile<TX>, false, true>(p, GridTile<TX>{}, out);
 }
 
@@ -391,13 +397,18 @@ __global__ void __launch_bounds__(kBPThreads, bp_min_blocks(ZPT)) bp_mixed_weigh
 // exactly as the single-scan kernels do; a shared-memory or indexed copy of
 // them measured 16-27 % slower at the 64-register bound.  Each slot holds its
 // scan's own tile depth (4 or 8 slices, a uniform branch per tile), so scans
-// tuned to either depth share the launch.  The next tile's index is fetched
+// tuned to either depth share the launch.  DEEP: a launch of the mixed
+// form's 16-slice tiles only, at that body's register bound (96 registers;
+// the 4- and 8-slice bodies run at 64).  The next tile's index is fetched
 // while the current one runs.
 // WV: every scan of the launch divides by its weight volume (p.wvol).
-template <int S, bool MIXED, bool WZ, bool WV>
+template <int S, bool MIXED, bool WZ, bool WV, bool DEEP>
 __device__ __forceinline__ void batch_slot_tile(const BatchSlots& t) {
     const BatchTile tile{t.s[S]};
-    if (t.s[S].zpt == 8) {
+    if constexpr (DEEP) {
+        static_assert(MIXED, "16-slice batch tiles are the mixed form's");
+        bp_mixed_block<16, true, WZ, BatchTile, WV>(t.s[S].p, tile);
+    } else if (t.s[S].zpt == 8) {
         if (MIXED)
             bp_mixed_block<8, true, WZ, BatchTile, WV>(t.s[S].p, tile);
         else
@@ -411,18 +422,20 @@ __device__ __forceinline__ void batch_slot_tile(const BatchSlots& t) {
 }
 
 // The tile of slot si (si < kBatchSlots): a compile-time slot per case.
-template <int S, bool MIXED, bool WZ, bool WV>
+template <int S, bool MIXED, bool WZ, bool WV, bool DEEP>
 __device__ __forceinline__ void batch_dispatch(const BatchSlots& t, int si) {
     if constexpr (S < kBatchSlots) {
         if (si == S)
-            batch_slot_tile<S, MIXED, WZ, WV>(t);
+            batch_slot_tile<S, MIXED, WZ, WV, DEEP>(t);
         else
-            batch_dispatch<S + 1, MIXED, WZ, WV>(t, si);
+            batch_dispatch<S + 1, MIXED, WZ, WV, DEEP>(t, si);
     }
 }
 
-template <bool MIXED, bool WZ, bool WV>
-__global__ void __launch_bounds__(kBPThreads, MIXED ? bp_min_blocks(8) : bp_fp32_min_blocks(8))
+template <bool MIXED, bool WZ, bool WV, bool DEEP>
+__global__ void __launch_bounds__(kBPThreads, DEEP    ? bp_min_blocks(16)
+                                              : MIXED ? bp_min_blocks(8)
+                                                      : bp_fp32_min_blocks(8))
     bp_batch_kernel(const __grid_constant__ BatchSlots t, int nscans, unsigned* __restrict__ counter,
                     unsigned total) {
     __shared__ unsigned s_next;
@@ -435,7 +448,7 @@ __global__ void __launch_bounds__(kBPThreads, MIXED ? bp_min_blocks(8) : bp_fp32
         if (tid == 0) s_next = atomicAdd(counter, 1u);   // the next tile, while this one runs
         int si = 0;
         while (si + 1 < nscans && it >= t.s[si + 1].first_tile) ++si;
-        batch_dispatch<0, MIXED, WZ, WV>(t, si);
+        batch_dispatch<0, MIXED, WZ, WV, DEEP>(t, si);
         __syncthreads();   // every thread is done with the current tile
         if (tid == 0) g_batch_tile = s_next;
         __syncthreads();
@@ -736,27 +749,36 @@ cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_
 
 namespace {
 
-template <bool M, bool W, bool V>
+template <bool M, bool W, bool V, bool D>
 cudaError_t batch_go(const BatchSlots& t, int nscans, unsigned total, unsigned* counter, int ctas, cudaStream_t s) {
-    bp_batch_kernel<M, W, V><<<ctas, dim3(kBPTileX, kBPTileY), 0, s>>>(t, nscans, counter, total);
+    bp_batch_kernel<M, W, V, D><<<ctas, dim3(kBPTileX, kBPTileY), 0, s>>>(t, nscans, counter, total);
     return cudaGetLastError();
 }
 
-template <bool M, bool W, bool V>
+template <bool M, bool W, bool V, bool D>
 cudaError_t batch_occ(int* per) {
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, bp_batch_kernel<M, W, V>, kBPThreads, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per, bp_batch_kernel<M, W, V, D>, kBPThreads, 0);
 }
 
+// deep: 16-slice tiles (the mixed form only)
 template <bool M, bool W>
 cudaError_t batch_go2(const BatchSlots& t, int nscans, unsigned total, unsigned* counter, int ctas, bool wv,
-                      cudaStream_t s) {
-    return wv ? batch_go<M, W, true>(t, nscans, total, counter, ctas, s)
-              : batch_go<M, W, false>(t, nscans, total, counter, ctas, s);
+                      bool deep, cudaStream_t s) {
+    if constexpr (M) {
+        if (deep)
+            return wv ? batch_go<M, W, true, true>(t, nscans, total, counter, ctas, s)
+                      : batch_go<M, W, false, true>(t, nscans, total, counter, ctas, s);
+    }
+    return wv ? batch_go<M, W, true, false>(t, nscans, total, counter, ctas, s)
+              : batch_go<M, W, false, false>(t, nscans, total, counter, ctas, s);
 }
 
 template <bool M, bool W>
-cudaError_t batch_occ2(bool wv, int* per) {
-    return wv ? batch_occ<M, W, true>(per) : batch_occ<M, W, false>(per);
+cudaError_t batch_occ2(bool wv, bool deep, int* per) {
+    if constexpr (M) {
+        if (deep) return wv ? batch_occ<M, W, true, true>(per) : batch_occ<M, W, false, true>(per);
+    }
+    return wv ? batch_occ<M, W, true, false>(per) : batch_occ<M, W, false, false>(per);
 }
 
 }  // namespace
@@ -764,24 +786,28 @@ cudaError_t batch_occ2(bool wv, int* per) {
 cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tiles, bool mixed_form, bool wz,
                             bool wv, unsigned* counter, int ctas, cudaStream_t s) {
     if (nscans < 1 || nscans > kBatchSlots) return cudaErrorInvalidValue;
-    for (int i = 0; i < nscans; ++i)
-        if ((t.s[i].zpt != 4 && t.s[i].zpt != 8) || (wv && !t.s[i].p.wvol)) return cudaErrorInvalidValue;
+    const bool deep = t.s[0].zpt == 16;   // a launch of 16-slice tiles holds those only
+    if (deep && !mixed_form) return cudaErrorInvalidValue;
+    for (int i = 0; i < nscans; ++i) {
+        const int z = t.s[i].zpt;
+        if ((deep ? z != 16 : (z != 4 && z != 8)) || (wv && !t.s[i].p.wvol)) return cudaErrorInvalidValue;
+    }
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     if (mixed_form)
-        return wz ? batch_go2<true, true>(t, nscans, total_tiles, counter, ctas, wv, s)
-                  : batch_go2<true, false>(t, nscans, total_tiles, counter, ctas, wv, s);
-    return wz ? batch_go2<false, true>(t, nscans, total_tiles, counter, ctas, wv, s)
-              : batch_go2<false, false>(t, nscans, total_tiles, counter, ctas, wv, s);
+        return wz ? batch_go2<true, true>(t, nscans, total_tiles, counter, ctas, wv, deep, s)
+                  : batch_go2<true, false>(t, nscans, total_tiles, counter, ctas, wv, deep, s);
+    return wz ? batch_go2<false, true>(t, nscans, total_tiles, counter, ctas, wv, false, s)
+              : batch_go2<false, false>(t, nscans, total_tiles, counter, ctas, wv, false, s);
 }
 
-cudaError_t bp_batch_ctas(bool mixed_form, bool wz, bool wv, int* ctas) {
+cudaError_t bp_batch_ctas(bool mixed_form, bool wz, bool wv, bool deep, int* ctas) {
     int dev = 0, sms = 0, per = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess)
-        e = mixed_form ? (wz ? batch_occ2<true, true>(wv, &per) : batch_occ2<true, false>(wv, &per))
-                       : (wz ? batch_occ2<false, true>(wv, &per) : batch_occ2<false, false>(wv, &per));
+        e = mixed_form ? (wz ? batch_occ2<true, true>(wv, deep, &per) : batch_occ2<true, false>(wv, deep, &per))
+                       : (wz ? batch_occ2<false, true>(wv, false, &per) : batch_occ2<false, false>(wv, false, &per));
     *ctas = sms * (per > 0 ? per : 1);
     return e;
 }

@@ -251,8 +251,14 @@ BPParams bp_params(const jfdk_ctx* c) {
     return b;
 }
 
-// Slices per thread: the option, else 8 (measured fastest in both forms).
-int bp_zpt(const jfdk_ctx* c) { return c->opt_bp_zpt ? c->opt_bp_zpt : 8; }
+// Slices per thread: the option, else 16 in the mixed form when W does not
+// depend on z (88.0 against 93.6 ms on c2), 8 otherwise (the FP32 form
+// measured 139 ms with 16 against 128 with 8: its per-slice coordinates
+// leave no per-view work to amortise and 16 slices need 96 registers).
+int bp_zpt(const jfdk_ctx* c) {
+    if (c->opt_bp_zpt) return c->opt_bp_zpt;
+    return mixed(c) && !c->w_depends_on_z ? 16 : 8;
+}
 
 // CTA width in x: the option, else 4 (4 x 32 threads).
 int bp_tile(const jfdk_ctx* c) { return c->opt_bp_tile ? c->opt_bp_tile : kBPTileX; }
@@ -748,6 +754,22 @@ jfdk_status jfdk_set_option(jfdk_ctx* c, int key, long long value) {
             if (value < 0) return fail(c, JFDK_ERR_INVALID, "negative memory limit");
             c->mem_limit = value;
             return JFDK_OK;
+        default: return fail(c, JFDK_ERR_INVALID, "unknown option");
+    }
+}
+
+jfdk_status jfdk_get_option(jfdk_ctx* c, int key, long long* value) {
+    if (!c || !value) return JFDK_ERR_INVALID;
+    switch (key) {
+        case JFDK_OPT_BP_EXACT: *value = c->opt_bp_exact; return JFDK_OK;
+        case JFDK_OPT_VIEW_CHUNK: *value = c->opt_view_chunk; return JFDK_OK;
+        case JFDK_OPT_STAGE_TIMING: *value = c->opt_stage_timing; return JFDK_OK;
+        case JFDK_OPT_BP_ZPT: *value = bp_zpt(c); return JFDK_OK;
+        case JFDK_OPT_BP_TILE: *value = bp_zpt(c) == 16 ? kBPTileX : bp_tile(c); return JFDK_OK;
+        case JFDK_OPT_FILTER_SIMT: *value = ramp_kind(c) == JFDK_RAMP_FP32_SIMT ? 1 : 0; return JFDK_OK;
+        case JFDK_OPT_RAMP_PRODUCT: *value = ramp_kind(c); return JFDK_OK;
+        case JFDK_OPT_DEVICE_MEMORY_LIMIT: *value = c->mem_limit; return JFDK_OK;
+        case JFDK_OPT_BP_WEIGHTS: *value = c->opt_bp_weights; return JFDK_OK;
         default: return fail(c, JFDK_ERR_INVALID, "unknown option");
     }
 }
@@ -1258,7 +1280,7 @@ void tune_file_load() {
     while (std::fgets(line, sizeof line, f)) {
         int z = 0, ch = 0, tx = kBPTileX;
         if (std::sscanf(line, "%255s %d %d %d", key, &z, &ch, &tx) < 3) continue;
-        if ((z == 4 || z == 8) && (ch == 16 || ch == 32 || ch == 64) && (tx == 4 || tx == 8 || tx == 32))
+        if ((z == 4 || z == 8 || z == 16) && (ch == 16 || ch == 32 || ch == 64) && (tx == 4 || tx == 8 || tx == 32))
             g_tune_cache[key] = {z, ch, tx};
     }
     std::fclose(f);
@@ -1326,8 +1348,10 @@ extern "C" jfdk_status jfdk_autotune(jfdk_ctx* c, int flags) {
     int best_z = 8, best_x = kBPTileX;
     float best_t = 1e30f;
     ensure_weights(c, c->stream);   // not inside the first candidate's time
-    for (int zpt : {4, 8}) {
+    for (int zpt : {4, 8, 16}) {
+        if (zpt == 16 && !mixed(c)) continue;   // the FP32 form: 139 against 128 ms on c2
         for (int tx : {4, 8, 32}) {
+            if (zpt == 16 && tx != kBPTileX) continue;   // 16-slice tiles are 4 wide
             c->opt_bp_zpt = zpt;
             c->opt_bp_tile = tx;
             BPParams b = jfdk::reconstruct_bp_params(c, slab - (ptrdiff_t)(z0 * plane), nullptr);

@@ -77,7 +77,7 @@ struct BatchScan {
     BPParams p;
     unsigned first_tile;
     int gx, gy, gz;
-    int zpt;                 // 4 or 8
+    int zpt;                 // 4 or 8; 16 (mixed form) in a launch of 16-slice tiles only
     int wz;                  // W depends on z
     int pad[2];
 };
@@ -98,7 +98,8 @@ cudaError_t launch_bp_weights(const BPParams& p, bool exact, bool w_depends_on_z
 cudaError_t launch_bp_mixed_weights(const BPParams& p, bool w_depends_on_z, int zpt, int tile_x, float* out,
                                     cudaStream_t s);
 // A batched backprojection launch covers up to kBatchSlots scans that share
-// whether W depends on z (each with its own tile depth, 4 or 8 slices); their
+// whether W depends on z (each with its own tile depth, 4 or 8 slices, or
+// all of them the mixed form's 16); their
 // parameters travel in the kernel's parameter space (16 slots: ~4.4 KB of the
 // 32 KB a launch may carry).
 constexpr int kBatchSlots = 16;
@@ -110,7 +111,7 @@ struct BatchSlots {
 cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tiles, bool mixed_form, bool wz,
                             bool wv, unsigned* counter, int ctas, cudaStream_t s);
 // CTAs of a full persistent wave: SMs x resident CTAs per SM.
-cudaError_t bp_batch_ctas(bool mixed_form, bool wz, bool wv, int* ctas);
+cudaError_t bp_batch_ctas(bool mixed_form, bool wz, bool wv, bool deep, int* ctas);
 // Mixed-precision form: FP16 footprints with a per-view scale (qh, qscale).
 cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, int tile_x,
                             cudaStream_t s);

@@ -167,6 +167,18 @@ class FDKEngine:
     def set_option(self, key: int, value: int):
         self._check(self.lib.jfdk_set_option(self.ctx, key, int(value)))
 
+    def get_option(self, key: int) -> int:
+        """The option's value in effect (defaults resolved, jfdk_get_option)."""
+        v = C.c_longlong(0)
+        self._check(self.lib.jfdk_get_option(self.ctx, key, C.byref(v)))
+        return int(v.value)
+
+    @property
+    def tile_depth(self) -> int:
+        """Slices per backprojection thread in effect: z-slabs that start at
+        multiples of it reproduce the whole volume bit for bit."""
+        return self.get_option(_lib.OPT_BP_ZPT)
+
     def stage_times(self):
         """ms of [prep + filter, z-filter, backprojection] of the last
         reconstruct (needs set_option(OPT_STAGE_TIMING, 1))."""

@@ -70,15 +70,19 @@ def exchange(parts, rank: int, group=None) -> None:
             dist.broadcast(t, src=src, group=group)
 
 
-def reconstruct_zslab(engine, raw, rank: int, world: int, group=None, out=None, tile_depth: int = 8, frames=None):
+def reconstruct_zslab(engine, raw, rank: int, world: int, group=None, out=None, tile_depth: Optional[int] = None,
+                      frames=None):
     """This rank's slab of the HU volume: (z0, tensor of nz x Y x X, or None
     when the rank has no slices).  raw: the rotation's frames on this rank's
     GPU (only this rank's views -- and their conjugates when compositing --
     are read); frames: an optional (views, rows, filter_out_w) float32 device
-    buffer for the filtered frames of every view."""
+    buffer for the filtered frames of every view; tile_depth: the slabs'
+    granularity (default: the engine's backprojection tile depth)."""
     import torch
     V = engine.scan.num_views
     views = view_ranges(V, world)
+    if tile_depth is None:
+        tile_depth = engine.tile_depth
     slabs = slab_ranges(engine.recon.num_pixels_z, world, tile_depth)
     if frames is None:
         frames = torch.empty((V, engine.rows, engine.filter_out_w), dtype=torch.float32, device=raw.device)

@@ -102,3 +102,26 @@ def test_sixteen_uneven_scans_in_one_persistent_launch(torch_cuda):
         assert batch.launches - n0 == 1
         assert all(same(torch, o, r) for o, r in zip(outs, refs))
         batch.close()
+
+
+def test_mixed_scans_of_sixteen_slice_tiles_in_one_launch(torch_cuda):
+    """The mixed form's default tile (16 slices per thread) runs in a launch
+    of its own kind: scans of the default tile share one persistent launch;
+    a scan tuned to 8 slices between them starts another."""
+    torch = torch_cuda
+    from jenhine_b200 import _lib
+    from jenhine_b200.fdk import FDKBatch
+    for depths, launches in (((16, 16, 16, 16), 1), ((16, 8, 16, 16), 3)):
+        scans = make_scans("mixed")
+        for d, (_, e, _) in zip(depths, scans):
+            e.set_option(_lib.OPT_BP_ZPT, 0 if d == 16 else d)
+            assert e.tile_depth == d
+        refs = [e.reconstruct(raw).clone() for _, e, raw in scans]
+        batch = FDKBatch([e for _, e, _ in scans], autotune=False, graph=False, schedule="persistent")
+        outs = [torch.full_like(r, -7.0) for r in refs]
+        n0 = batch.launches
+        batch.run([raw for _, _, raw in scans], outs)
+        torch.cuda.synchronize()
+        assert batch.launches - n0 == launches
+        assert all(same(torch, o, r) for o, r in zip(outs, refs))
+        batch.close()

@@ -234,8 +234,9 @@ def test_reconstruct_int16_output(torch_cuda, case, oracle):
 @pytest.mark.parametrize("precision", ["fp32", "mixed"])
 def test_voxel_tiles_give_the_same_volume(torch_cuda, case, precision):
     """Every backprojection tile the autotuner chooses between (4, 8 or 32
-    threads wide in x; 4 or 8 slices per thread) computes each voxel the same
-    way: the volume equals the default tile's bit for bit, in chunks too."""
+    threads wide in x; 4, 8 or 16 slices per thread, 16-slice tiles 4 wide)
+    computes each voxel the same way: the volume equals the default tile's
+    bit for bit, in chunks too."""
     from jenhine_b200 import _lib
     raw = to_dev(torch_cuda, case["raw"])
     filt = to_dev(torch_cuda, case["filt"])
@@ -253,7 +254,7 @@ def test_voxel_tiles_give_the_same_volume(torch_cuda, case, precision):
     def same(a, b):
         return torch_cuda.equal(torch_cuda.nan_to_num(a, 1e30), torch_cuda.nan_to_num(b, 1e30))
 
-    for zpt in (4, 8):
+    for zpt in (4, 8, 16):
         # the mixed form steps z from each thread's first slice: compare
         # within one tile depth; the FP32 volume does not depend on it either
         want = run(zpt, 4) if precision == "mixed" or zpt == 4 else want
@@ -269,6 +270,27 @@ def test_voxel_tile_option_is_checked(torch_cuda, case):
     e = engine_for(case)
     with pytest.raises(_lib.JfdkError):
         e.set_option(_lib.OPT_BP_TILE, 16)
+    with pytest.raises(_lib.JfdkError):
+        e.set_option(_lib.OPT_BP_ZPT, 32)
+
+
+def test_tile_depth_in_effect(torch_cuda):
+    """jfdk_get_option resolves the defaults: 16 slices per thread in the
+    mixed form when W does not depend on z, else 8; a set value as set."""
+    from jenhine_b200 import _lib
+    for name, precision, want in (("mini_c2", "fp32", 8), ("mini_c2", "mixed", 16), ("mini_tilt", "mixed", 8)):
+        e = engine_for(load_golden(name), precision=precision)
+        assert e.tile_depth == want, (name, precision)
+        assert e.get_option(_lib.OPT_BP_TILE) == 4
+        e.set_option(_lib.OPT_BP_ZPT, 4)
+        assert e.tile_depth == 4
+        e.set_option(_lib.OPT_BP_ZPT, 0)
+        assert e.tile_depth == want
+    e = engine_for(load_golden("mini_c2"))
+    assert e.get_option(_lib.OPT_RAMP_PRODUCT) == _lib.RAMP_I8X14
+    assert e.get_option(_lib.OPT_BP_WEIGHTS) == 1
+    with pytest.raises(_lib.JfdkError):
+        e.get_option(999)
 
 
 def test_zfilter_matches_reference_order(torch_cuda, case):

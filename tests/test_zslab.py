@@ -40,7 +40,7 @@ def test_emulated_ranks_equal_reconstruct(torch_cuda, name, precision, world):
     for v0, nv in views:              # each rank filters its views
         e.filter_raw(raw, v0, nv, out=frames[v0:v0 + nv])
     parts = []
-    for z0, nz in slab_ranges(Z, world):
+    for z0, nz in slab_ranges(Z, world, e.tile_depth):
         if not nz:
             continue
         e.bp_set_slab(z0, nz)         # each rank backprojects every view into its slab
@@ -55,7 +55,7 @@ def test_emulated_ranks_equal_reconstruct(torch_cuda, name, precision, world):
     e.bp_set_slab(0, Z)
     for v0, nv in views:
         e.filter_to_store(raw, v0, nv)
-    got = torch.cat([e.backproject_store(z0, nz) for z0, nz in slab_ranges(Z, world) if nz])
+    got = torch.cat([e.backproject_store(z0, nz) for z0, nz in slab_ranges(Z, world, e.tile_depth) if nz])
     torch.cuda.synchronize()
     assert torch.equal(torch.nan_to_num(got, 1e30), torch.nan_to_num(whole, 1e30))
 
