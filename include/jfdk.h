@@ -254,7 +254,9 @@ enum {
                                  stream around each stage                        */
     JFDK_OPT_BP_ZPT = 4,      /* slices each backprojection thread keeps in
                                  registers: 4, 8 or 16; 0 (default): 16 in the
-                                 mixed form when W does not depend on z, else 8.
+                                 mixed form when W does not depend on z and the
+                                 volume holds at least 8 waves of 16-slice
+                                 tiles (c2 does, c1 does not), else 8.
                                  The FP32 form's volume does not depend on it;
                                  the mixed form's coordinates step from each
                                  tile's first slice, so its volume does      */

@@ -72,7 +72,8 @@ void drop_graph(jfdk_batch* b) {
 // Scan descriptors for the given outputs: each scan's finalizing BP params,
 // its grid of kBPTileX x kBPTileY x ZPT tiles and its first tile in its group's
 // work list; consecutive scans with the same W(z), weight-volume use and
-// tile-depth class (16 slices, the mixed form's default, or 4 / 8) share a
+// tile-depth class (16 slices, the mixed form's default on large volumes,
+// or 4 / 8) share a
 // group of up to kBatchSlots.
 jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
     b->groups.clear();

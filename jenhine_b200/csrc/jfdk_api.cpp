@@ -252,12 +252,18 @@ BPParams bp_params(const jfdk_ctx* c) {
 }
 
 // Slices per thread: the option, else 16 in the mixed form when W does not
-// depend on z (88.0 against 93.6 ms on c2), 8 otherwise (the FP32 form
-// measured 139 ms with 16 against 128 with 8: its per-slice coordinates
-// leave no per-view work to amortise and 16 slices need 96 registers).
+// depend on z and the volume holds at least 8 waves of 16-slice tiles (5
+// CTAs per SM), 8 otherwise.  16 slices halve the mixed loop's per-view work
+// (87.8 against 93.6 ms on c2, 130 waves), but a small volume then fills the
+// GPU in few waves (c1, 128^3: 1.4 waves, 1.39 against 1.22 ms with 8); the
+// FP32 form measured 139 ms with 16 against 128 with 8 (its per-slice
+// coordinates leave no per-view work to amortise).
 int bp_zpt(const jfdk_ctx* c) {
     if (c->opt_bp_zpt) return c->opt_bp_zpt;
-    return mixed(c) && !c->w_depends_on_z ? 16 : 8;
+    if (!mixed(c) || c->w_depends_on_z) return 8;
+    const long long tiles = (long long)((c->X + kBPTileX - 1) / kBPTileX) * ((c->Y + kBPTileY - 1) / kBPTileY) *
+                            ((c->Z + 15) / 16);
+    return tiles >= 8LL * 5 * c->sms ? 16 : 8;
 }
 
 // CTA width in x: the option, else 4 (4 x 32 threads).
@@ -576,6 +582,7 @@ jfdk_status jfdk_create(jfdk_ctx** out, const jfdk_scan_params* scan, const jfdk
     JFDK_CUDA(c, cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
     if (prop.major != 10) return bail(fail(c, JFDK_ERR_NO_DEVICE, "libjfdk needs an sm_100 (B200) device"));
     c->device = dev;
+    c->sms = prop.multiProcessorCount;
     // NULL selects the legacy default stream, so the context's work is
     // ordered with every other default-stream operation of the process.
     c->stream = static_cast<cudaStream_t>(cuda_stream);

@@ -267,6 +267,7 @@ struct jfdk_ctx {
     std::vector<float> adj_pts, adj_db;
     int precision = 0;
     int device = 0;
+    int sms = 148;                // the device's SMs
     cudaStream_t stream = nullptr;
     bool own_stream = false;
 

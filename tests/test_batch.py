@@ -105,16 +105,16 @@ def test_sixteen_uneven_scans_in_one_persistent_launch(torch_cuda):
 
 
 def test_mixed_scans_of_sixteen_slice_tiles_in_one_launch(torch_cuda):
-    """The mixed form's default tile (16 slices per thread) runs in a launch
-    of its own kind: scans of the default tile share one persistent launch;
-    a scan tuned to 8 slices between them starts another."""
+    """The mixed form's 16-slice tiles (its default on large volumes) run in
+    launches of their own kind: scans of 16-slice tiles share one persistent
+    launch; a scan of 8-slice tiles between them starts another."""
     torch = torch_cuda
     from jenhine_b200 import _lib
     from jenhine_b200.fdk import FDKBatch
     for depths, launches in (((16, 16, 16, 16), 1), ((16, 8, 16, 16), 3)):
         scans = make_scans("mixed")
         for d, (_, e, _) in zip(depths, scans):
-            e.set_option(_lib.OPT_BP_ZPT, 0 if d == 16 else d)
+            e.set_option(_lib.OPT_BP_ZPT, d)
             assert e.tile_depth == d
         refs = [e.reconstruct(raw).clone() for _, e, raw in scans]
         batch = FDKBatch([e for _, e, _ in scans], autotune=False, graph=False, schedule="persistent")

@@ -276,16 +276,25 @@ def test_voxel_tile_option_is_checked(torch_cuda, case):
 
 def test_tile_depth_in_effect(torch_cuda):
     """jfdk_get_option resolves the defaults: 16 slices per thread in the
-    mixed form when W does not depend on z, else 8; a set value as set."""
+    mixed form when W does not depend on z and the volume holds at least 8
+    waves of 16-slice tiles (c2), else 8 (the small fixtures, a tilted orbit,
+    the FP32 form); a set value as set."""
     from jenhine_b200 import _lib
-    for name, precision, want in (("mini_c2", "fp32", 8), ("mini_c2", "mixed", 16), ("mini_tilt", "mixed", 8)):
+    from jenhine_b200.fdk import FDKEngine
+    from jenhine_b200.workloads import c2
+    w = c2()
+    for precision, want in (("fp32", 8), ("mixed", 16)):
+        e = FDKEngine(w.scan, w.recon, w.geom.ptms(), precision=precision)
+        assert e.tile_depth == want, precision
+        e.close()
+    for name, precision in (("mini_c2", "fp32"), ("mini_c2", "mixed"), ("mini_tilt", "mixed")):
         e = engine_for(load_golden(name), precision=precision)
-        assert e.tile_depth == want, (name, precision)
+        assert e.tile_depth == 8, (name, precision)
         assert e.get_option(_lib.OPT_BP_TILE) == 4
-        e.set_option(_lib.OPT_BP_ZPT, 4)
-        assert e.tile_depth == 4
+        e.set_option(_lib.OPT_BP_ZPT, 16)
+        assert e.tile_depth == 16 and e.get_option(_lib.OPT_BP_TILE) == 4
         e.set_option(_lib.OPT_BP_ZPT, 0)
-        assert e.tile_depth == want
+        assert e.tile_depth == 8
     e = engine_for(load_golden("mini_c2"))
     assert e.get_option(_lib.OPT_RAMP_PRODUCT) == _lib.RAMP_I8X14
     assert e.get_option(_lib.OPT_BP_WEIGHTS) == 1
