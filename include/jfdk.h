@@ -363,8 +363,9 @@ jfdk_status jfdk_autotune(jfdk_ctx* ctx, int flags);
  *    streams, so small scans' stages run side by side), then ONE persistent
  *    backprojection launch over the tiles of up to 16 scans (scans in order;
  *    a CTA takes the next tile when it finishes one, so scans of uneven size
- *    leave no tail; each scan keeps its own tile depth; consecutive scans
- *    whose W does not depend on z the same way start a new launch);
+ *    leave no tail; each scan keeps its own tile depth; scans whose W depends
+ *    on z differently, and the mixed form's 16-slice scans, share launches of
+ *    their own kind);
  *  - pipelined: each scan's own backprojection launch, the filter stage of
  *    the next scan running beside it on a second stream.
  * JFDK_BATCH_AUTOTUNE tunes each context (jfdk_autotune) and, on the first

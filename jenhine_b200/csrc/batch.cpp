@@ -71,10 +71,12 @@ void drop_graph(jfdk_batch* b) {
 
 // Scan descriptors for the given outputs: each scan's finalizing BP params,
 // its grid of kBPTileX x kBPTileY x ZPT tiles and its first tile in its group's
-// work list; consecutive scans with the same W(z), weight-volume use and
-// tile-depth class (16 slices, the mixed form's default on large volumes,
-// or 4 / 8) share a
-// group of up to kBatchSlots.
+// work list.  Scans with the same W(z), weight-volume use and tile-depth
+// class (16 slices, the mixed form's default on large volumes, or 4 / 8)
+// share a group of up to kBatchSlots, in scan order, whatever lies between
+// them: a batch whose scans were tuned to 16 and to 8 slices is two launches,
+// not one per change of depth (8 launches for the 16-scan workload, whose
+// mixed-form persistent schedule then ran 2.7 % behind the pipelined one).
 jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
     b->groups.clear();
     for (size_t i = 0; i < b->ctx.size(); ++i) {
@@ -93,8 +95,12 @@ jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
         const float* wvol = bp_slices_per_thread(c) == s.zpt ? bp_weight_volume(c) : nullptr;
         s.p.wvol = wvol;
         const int wv = wvol ? 1 : 0, deep = s.zpt == 16 ? 1 : 0;
-        if (b->groups.empty() || b->groups.back().n == kBatchSlots || b->groups.back().wz != s.wz ||
-            b->groups.back().wv != wv || b->groups.back().deep != deep) {
+        size_t gi = b->groups.size();
+        for (size_t k = 0; k < b->groups.size(); ++k) {
+            const jfdk_batch::Group& o = b->groups[k];
+            if (o.n < kBatchSlots && o.wz == s.wz && o.wv == wv && o.deep == deep) gi = k;
+        }
+        if (gi == b->groups.size()) {
             jfdk_batch::Group g;
             std::memset(&g, 0, sizeof g);
             g.wz = s.wz;
@@ -104,7 +110,7 @@ jfdk_status plan_groups(jfdk_batch* b, float* const* d_hu) {
                        "occupancy query");
             b->groups.push_back(g);
         }
-        jfdk_batch::Group& g = b->groups.back();
+        jfdk_batch::Group& g = b->groups[gi];
         s.first_tile = g.total;
         g.total += (unsigned)s.gx * s.gy * s.gz;
         g.slots.s[g.n++] = s;
