@@ -40,7 +40,6 @@
 
 #include <algorithm>
 #include <cstdint>
-#include <type_traits>
 
 #include "bp_common.cuh"
 #include "jfdk_internal.h"
@@ -288,7 +287,6 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& ti
         }
     }
     const unsigned um1 = (unsigned)(p.U - 1), vm1 = (unsigned)(p.V - 1), uu = (unsigned)p.U;
-    const float ulim = (float)(p.U - 2), vlim = (float)(p.V - 2);   // a pixel inside the last sampled column / row
     const float2 magic = f2(kMagic, kMagic);
 
     const float4* P4 = reinterpret_cast<const float4*>(p.ptm + (size_t)p.v0 * 12);
@@ -320,62 +318,39 @@ __device__ __forceinline__ void bp_mixed_block(const BPParams& p, const Tile& ti
         // (scalar products: a packed product feeding the packed adds below
         // may be fused into them, differently in each kernel built from here)
         const float s = __ldg(sc);
-        // The slices of one view.  CLAMP (WV): the record index is clamped
-        // onto the zero records; without it every sample is known to lie on
-        // the detector and its index is formed as it is.
-        auto slices = [&](auto clamp) {
-            [[maybe_unused]] constexpr bool CLAMP = decltype(clamp)::value;
 #pragma unroll
-            for (int k = 0; k < ZPT; ++k) {
-                float2 cuv;
-                bool front = true;
-                if (WZ) {
-                    const float r = rcp_approx(Wk);
-                    front = Wk > 0.0f;
-                    cuv = pfma(UVk, f2(r, r), f2(0.5f, 0.5f));
-                    UVk = padd(UVk, duv);
-                    Wk = __fadd_rn(Wk, dW);
+        for (int k = 0; k < ZPT; ++k) {
+            float2 cuv;
+            bool front = true;
+            if (WZ) {
+                const float r = rcp_approx(Wk);
+                front = Wk > 0.0f;
+                cuv = pfma(UVk, f2(r, r), f2(0.5f, 0.5f));
+                UVk = padd(UVk, duv);
+                Wk = __fadd_rn(Wk, dW);
+            } else {
+                cuv = uv;              // slice k: uv0 + k duv, stepped
+                uv = padd(uv, duv);
+            }
+            const float2 t = padd_rm(cuv, magic);                     // 2^23 + floor(uv)
+            const float2 f = psub(cuv, psub(t, magic));               // fractions
+            const unsigned iu = __float_as_uint(t.x) - (unsigned)kMagicBits;
+            const unsigned iv = __float_as_uint(t.y) - (unsigned)kMagicBits;
+            if constexpr (WV) {
+                // out of range (negative / NaN wrap to large): a zero record
+                const float val = mixed_lerp(__ldg(q + (min(iv, vm1) * uu + min(iu, um1))), f);
+                if (front) acc[k].x = fmaf(s, val, acc[k].x);
+            } else {
+                const bool in = (iu < um1) & (iv < vm1) & front;
+                const float2 w = __ldg(tw + (in ? iu : 0u));
+                const float c = fmaf(f.x, w.y, w.x);
+                if constexpr (WEIGHTS) {
+                    if (in) acc[k].y = __fadd_rn(acc[k].y, c);
                 } else {
-                    cuv = uv;              // slice k: uv0 + k duv, stepped
-                    uv = padd(uv, duv);
-                }
-                const float2 t = padd_rm(cuv, magic);                     // 2^23 + floor(uv)
-                const float2 f = psub(cuv, psub(t, magic));               // fractions
-                const unsigned iu = __float_as_uint(t.x) - (unsigned)kMagicBits;
-                const unsigned iv = __float_as_uint(t.y) - (unsigned)kMagicBits;
-                if constexpr (WV) {
-                    // out of range (negative / NaN wrap to large): a zero record
-                    const unsigned ri = CLAMP ? min(iv, vm1) * uu + min(iu, um1) : iv * uu + iu;
-                    const float val = mixed_lerp(__ldg(q + ri), f);
-                    if (front) acc[k].x = fmaf(s, val, acc[k].x);
-                } else {
-                    const bool in = (iu < um1) & (iv < vm1) & front;
-                    const float2 w = __ldg(tw + (in ? iu : 0u));
-                    const float c = fmaf(f.x, w.y, w.x);
-                    if constexpr (WEIGHTS) {
-                        if (in) acc[k].y = __fadd_rn(acc[k].y, c);
-                    } else {
-                        const float val = mixed_lerp(__ldg(q + (in ? iv * uu + iu : 0u)), f);
-                        if (in) acc[k] = pfma(f2(s, 1.0f), f2(val, c), acc[k]);   // (s val + sum, c + weight)
-                    }
+                    const float val = mixed_lerp(__ldg(q + (in ? iv * uu + iu : 0u)), f);
+                    if (in) acc[k] = pfma(f2(s, 1.0f), f2(val, c), acc[k]);   // (s val + sum, c + weight)
                 }
             }
-        };
-        if constexpr (WV && !WZ) {
-            // The stepped (u, v) are monotone in k (each step adds the same
-            // duv, rounded) and within ~ZPT ulps of uv + k duv, so when both
-            // ends of the thread's slices lie a pixel inside [0, cols-1) x
-            // [0, rows-1) every slice samples and no index needs clamping.
-            // NaN fails the comparisons.
-            const float2 last = pfma(duv, f2((float)(ZPT - 1), (float)(ZPT - 1)), uv);
-            const bool inside = (uv.x >= 1.0f) & (last.x >= 1.0f) & (uv.x <= ulim) & (last.x <= ulim) &
-                                (uv.y >= 1.0f) & (last.y >= 1.0f) & (uv.y <= vlim) & (last.y <= vlim);
-            if (inside)
-                slices(std::false_type{});
-            else
-                slices(std::true_type{});
-        } else {
-            slices(std::true_type{});
         }
     }
     if constexpr (WEIGHTS) {
