@@ -295,8 +295,15 @@ jfdk_status jfdk_batch_run(jfdk_batch* b, const uint16_t* const* d_raw, float* c
         return JFDK_OK;
     }
     drop_graph(b);
-    jfdk_status st = plan_groups(b, d_hu);
-    if (st) return st;
+    // the stores first: the persistent launches' parameters name them, and a
+    // context that has not reconstructed yet (or whose shape the autotuner
+    // answered from its cache) would otherwise get its store from the filter
+    // stage after those parameters were taken
+    jfdk_status st = JFDK_OK;
+    for (size_t i = 0; i < n; ++i)
+        if ((st = ensure_store(b->ctx[i])))
+            return berr(b, st, std::string("scan ") + std::to_string(i) + ": " + b->ctx[i]->err);
+    if ((st = plan_groups(b, d_hu))) return st;
     b->hu.assign(d_hu, d_hu + n);
     // run directly (allocates whatever the contexts still need; picks the
     // schedule on the first run)

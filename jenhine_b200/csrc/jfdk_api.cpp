@@ -450,6 +450,11 @@ jfdk_status filter_stage_range(jfdk_ctx* c, const uint16_t* d_raw, int vbeg, int
 
 // The finalizing backprojection of every view into d_hu / d_hu16 with CT
 // numbers (the store filled by reconstruct_filter_stage).
+// The backprojection store of every view, allocated now, so that parameters
+// taken before a filter stage (the batch's persistent launches) name the
+// buffer that filter stage fills.
+jfdk_status ensure_store(jfdk_ctx* c) { return ensure_Q4(c, c->nviews); }
+
 BPParams reconstruct_bp_params(const jfdk_ctx* c, float* d_hu, int16_t* d_hu16) {
     BPParams b = bp_params(c);
     b.view_base = 0; b.v0 = 0; b.nv = c->nviews;

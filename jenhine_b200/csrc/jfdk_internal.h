@@ -112,6 +112,8 @@ cudaError_t launch_bp_batch(const BatchSlots& t, int nscans, unsigned total_tile
                             bool wv, unsigned* counter, int ctas, cudaStream_t s);
 // CTAs of a full persistent wave: SMs x resident CTAs per SM.
 cudaError_t bp_batch_ctas(bool mixed_form, bool wz, bool wv, bool deep, int* ctas);
+// The context's backprojection store for every view (allocated if missing).
+jfdk_status ensure_store(jfdk_ctx* c);
 // Mixed-precision form: FP16 footprints with a per-view scale (qh, qscale).
 cudaError_t launch_bp_mixed(const BPParams& p, bool finalize, bool w_depends_on_z, int zpt, int tile_x,
                             cudaStream_t s);

@@ -125,3 +125,23 @@ def test_mixed_scans_of_sixteen_slice_tiles_in_one_launch(torch_cuda):
         assert batch.launches - n0 == launches
         assert all(same(torch, o, r) for o, r in zip(outs, refs))
         batch.close()
+
+
+def test_batch_on_contexts_that_have_not_reconstructed(torch_cuda):
+    """Contexts straight from creation, two of one shape (the autotuner
+    answers the second from its cache): the batch allocates their
+    backprojection stores before it plans its persistent launches, whose
+    parameters name them, and every volume equals the scan's own
+    reconstruction taken afterwards."""
+    torch = torch_cuda
+    from jenhine_b200.fdk import FDKBatch
+    for precision in ("fp32", "mixed"):
+        scans = make_scans(precision, [SHAPES[0], SHAPES[1], SHAPES[0]])
+        batch = FDKBatch([e for _, e, _ in scans], autotune=True, graph=False, schedule="persistent")
+        outs = [torch.full((w.recon.num_pixels_z, w.recon.num_pixels_y, w.recon.num_pixels_x), -7.0, device="cuda")
+                for w, _, _ in scans]
+        batch.run([raw for _, _, raw in scans], outs)
+        torch.cuda.synchronize()
+        refs = [e.reconstruct(raw).clone() for _, e, raw in scans]
+        assert all(same(torch, o, r) for o, r in zip(outs, refs))
+        batch.close()
