@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--zpt", type=int, default=0, help="slices per backprojection thread (0: form default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the default c2 line's batch key (the 16-scan batch, mixed form)")
     ap.add_argument("--no-gpu-baseline", action="store_true",
                     help="skip timing the reference's own GPU backprojector (baseline/_ref)")
     ap.add_argument("--split", default="scans", choices=["scans", "zslab"],
@@ -685,6 +687,46 @@ def run_batch(a, rank, world, local):
         dist.destroy_process_group()
 
 
+def batch_summary(local, form: str = "mixed", steps: int = 3, warmup: int = 3):
+    """The 16-scan batch workload in one form, autotuned and graph-replayed
+    (the schedule the autotuner keeps), for the default line's `batch` key;
+    the comparison of schedules is `--workload batch`."""
+    import torch
+    from jenhine_b200.fdk import FDKBatch, FDKEngine
+    from jenhine_b200.workloads import batch
+    scans = batch()
+    updates = sum(w.updates for w in scans)
+    raws = [w.raw_torch() for w in scans]
+    engines = [FDKEngine(w.scan, w.recon, w.geom.ptms(), precision=form) for w in scans]
+    outs = [torch.empty((w.recon.num_pixels_z, w.recon.num_pixels_y, w.recon.num_pixels_x), device="cuda")
+            for w in scans]
+    b = FDKBatch(engines, autotune=True, graph=True)
+    try:
+        for _ in range(warmup):   # the first run times both schedules and records the graph
+            b.run(raws, outs)
+        torch.cuda.synchronize()
+        clocks = ClockSampler(local)
+        clocks.start()
+        time.sleep(0.5)
+        l0 = b.launches
+        s1, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s1.record()
+        for _ in range(steps):
+            b.run(raws, outs)
+        e1.record()
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        ms = s1.elapsed_time(e1) / steps
+        return {"value": updates / (ms / 1000.0) / 1e9, "unit": "GUPS", "ms_per_step": ms, "steps": steps,
+                "warmup": warmup, "precision": form, "schedule": b.schedule, "gpu_launches": b.launches - l0,
+                "clocks": clk, "updates_per_step": updates,
+                "workload": "16 seeded scans of uneven size (bench.py --workload batch), one graph-replayed batch"}
+    finally:
+        b.close()
+        for e in engines:
+            e.close()
+
+
 def run_grad(a, rank, world, local):
     """--workload grad: the differentiation case (c3: 256^3 at 0.4 mm from 360
     views of 512^2).  One step = the loss ||FDK(p; theta) - V_target||^2 and
@@ -841,6 +883,11 @@ def main():
             gb = gpu_baseline(w, raw, ptms, local)
             if gb is not None:
                 line["gpu_baseline"] = gb
+        if not a.no_batch and world == 1 and a.workload == "c2" and "mixed" in forms:
+            try:
+                line["batch"] = batch_summary(local)
+            except Exception as ex:   # the extra key must not cost the line
+                line["batch"] = {"unavailable": f"{type(ex).__name__}: {ex}"}
         if not a.no_cpu_baseline and world == 1 and not w.composite:
             # the CPU leg (rank 0, one GPU): the reference Cores timed on the
             # host, and each form's error against the FP64 oracle
